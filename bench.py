@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 SolTrace trace.
+
+Metric: ray-stage intersections/s on one B200 for the central-receiver heliostat
+field -- 2,000 flat 10x10 m heliostats on a radial-staggered field 100-1000 m north
+of a 150 m tower, Buie CSR 0.1 sunshape at 45 deg elevation / 180 deg azimuth,
+1.5 mrad slope error, an 8 m x 10 m external cylindrical receiver -- traced to
+1e8 first-stage hits per step, in mixed FP32/FP64 precision, with the FP64 device
+trace and the flux-map L2 error between them reported beside it.
+
+A step is one st_sim_run of that scene through the C ABI (coretrace_api.so).  A
+ray-stage intersection is one generated sun ray or one ray entering a later stage.
+`value` divides the units of the K timed steps by their device time (CUDA events on
+the library's stream, first launch to last completion); `e2e` divides them by the
+wall time of the st_sim_run calls themselves (scene upload from host memory,
+kernels, flux and counter readback into host arrays).
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun (N > 1) every rank traces its own 1e8 hits with its own seed
+(weak scaling) and the receiver flux maps are summed with one NCCL all-reduce.
+`--impl reference` times the reference coretrace (built from its sources into
+oracle/_ref/) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from soltrace_b200 import flops_model as fm  # noqa: E402
+from soltrace_b200 import scenes  # noqa: E402
+
+METRIC = "ray-stage intersections/s on 1 B200, mixed vs FP64, at <=0.5% flux-map L2 error"
+UNIT = "ray-stage intersections/s"
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "coretrace_ref.so")
+FLUX_MAP = (2, 1, 1, 100, 100, 0.0, 4.0, -5.0, 5.0, 1)  # receiver: 100 x 100 angle x axial, absorbed
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--hits", type=int, default=100_000_000)
+    p.add_argument("--helios", type=int, default=2000)
+    p.add_argument("--seed", type=int, default=3)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload(args):
+    return {"workload": f"heliostat field: {args.helios} flat 10x10 m heliostats, Buie CSR 0.1, "
+                        f"8 m x 10 m cylindrical receiver, {args.hits:.0e} first-stage hits per step",
+            "heliostats": args.helios, "hits_per_step": args.hits, "receiver_flux_map": "100x100",
+            "l2": "per-step working set > L2 (hit lists of up to 0.5 GB per sun-ray batch); "
+                  "scene tables (~1 MB) stay L2-resident by design",
+            "parallelism": f"dp{args.gpus} (independent rays per GPU)"}
+
+
+# ---------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------
+# reference (CPU) timing
+# ---------------------------------------------------------------------------------------
+def reference_sample(sc, seconds: float, seed: int):
+    """The reference coretrace on all host cores: one context per thread, raycount/threads
+    hits each, seeds seed + i*123 (the GUI's multi-thread convention).  Times st_sim_run only."""
+    from soltrace_b200.capi import StApi
+    if not os.path.exists(REF_SO):
+        raise FileNotFoundError(REF_SO)
+    ref = StApi(REF_SO)
+    ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+    def one(hits, s, out, idx, barrier=None):
+        ctx = ref.st_create_context()
+        local = dataclasses.replace(sc, raycount=hits, raymax=2_000_000_000 - 1)
+        scenes.push(ref, ctx, local)
+        if barrier:
+            barrier.wait()
+        t0 = time.perf_counter()
+        n = ref.run(ctx, s)
+        dt = time.perf_counter() - t0
+        ss = ref.sun_stats(ctx)
+        rec = ref.records(ctx)
+        ref.st_free_context(ctx)
+        entries2 = len(np.unique(rec["raynum"][rec["stage"] == 2])) if n > 0 else 0
+        out[idx] = (dt, ss["nsunrays"] + entries2, n)
+
+    # calibrate the per-core rate on a small run
+    probe = [None]
+    one(2000, seed, probe, 0)
+    rate = probe[0][1] / max(probe[0][0], 1e-6)  # units per second per core
+    units_per_hit = probe[0][1] / 2000.0
+    hits_per_thread = max(2000, int(rate * seconds / units_per_hit))
+    res = [None] * ncores
+    bar = threading.Barrier(ncores)
+    th = [threading.Thread(target=one, args=(hits_per_thread, seed + i * 123, res, i, bar)) for i in range(ncores)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    wall = max(r[0] for r in res)
+    units = sum(r[1] for r in res)
+    return {"value": units / wall, "unit": UNIT, "cores": ncores, "kind": "reference",
+            "sample": f"{ncores} threads x {hits_per_thread} hits ({units} ray-stage units, "
+                      f"{wall:.1f} s wall, st_sim_run only, polar receiver hash on)"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sc = scenes.field_scene(args.helios, args.hits)
+    if not os.path.exists(REF_SO):
+        print(json.dumps({"impl": "reference", "unavailable": "reference library oracle/_ref/coretrace_ref.so not built"}))
+        return
+    per_step = max(2.0, min(args.cpu_seconds, 20.0))
+    vals = []
+    for k in range(args.warmup + args.steps):
+        r = reference_sample(sc, per_step, args.seed + k)
+        if k >= args.warmup:
+            vals.append(r)
+    value = statistics.median([v["value"] for v in vals])
+    cb = dict(vals[-1])
+    cb["value"] = value
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload(args),
+            "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import torch
+
+    from soltrace_b200.lib import load
+    api = load()
+    sc = scenes.field_scene(args.helios, args.hits)
+    ctx = api.st_create_context()
+    scenes.push(api, ctx, sc)
+    api.st_b200_set_device(ctx, local if world > 1 else 0)
+    api.st_b200_set_records(ctx, 0)
+    api.st_b200_add_flux_map(ctx, *FLUX_MAP)
+
+    def step(prec, seed):
+        api.st_b200_set_precision(ctx, prec)
+        t0 = time.perf_counter()
+        rc = api.run(ctx, seed)
+        wall = time.perf_counter() - t0
+        if rc < 0:
+            raise RuntimeError("st_sim_run failed: " + "; ".join(api.messages(ctx)))
+        st = api.stats(ctx)
+        st["wall_ms"] = wall * 1e3
+        st["flux"] = api.flux(ctx, 0, FLUX_MAP[3], FLUX_MAP[4])
+        return st
+
+    seed0 = args.seed + 1000 * rank
+    for k in range(args.warmup):
+        step(1, seed0 + k)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    runs = []
+    with ClockSampler(local) as clk:
+        barrier()
+        for k in range(args.steps):
+            runs.append(step(1, seed0 + 100 + k))
+        barrier()
+    units = sum(r["ray_stage_units"] for r in runs)
+    dev_ms = sum(r["kernel_ms"] for r in runs)
+    wall_ms = sum(r["wall_ms"] for r in runs)
+    probe_ms = sum(r["probe_ms"] for r in runs)
+    trace_ms = sum(r["trace_ms"] for r in runs)
+    launches = sum(r["gpu_launches"] for r in runs)
+
+    # FP64 device trace of the same steps: throughput and the flux-map L2 error
+    n64 = max(1, min(args.steps, 2))
+    runs64 = [step(0, seed0 + 100 + k) for k in range(n64)]
+    units64 = sum(r["ray_stage_units"] for r in runs64)
+    dev64 = sum(r["kernel_ms"] for r in runs64)
+    l2 = [float(np.linalg.norm(runs[k]["flux"].astype(float) - runs64[k]["flux"].astype(float)) /
+                max(np.linalg.norm(runs64[k]["flux"].astype(float)), 1e-30)) for k in range(n64)]
+
+    flux_sum = runs[-1]["flux"].astype(np.int64)
+    if dist:
+        t = torch.tensor([units, wall_ms], dtype=torch.float64, device="cuda")
+        tmax = torch.tensor([dev_ms, wall_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        units, dev_ms, wall_ms = t[0].item(), tmax[0].item(), tmax[1].item()
+        fx = torch.from_numpy(flux_sum).cuda()
+        dist.all_reduce(fx, op=dist.ReduceOp.SUM)  # combined receiver map of all ranks
+        flux_sum = fx.cpu().numpy()
+    if rank != 0:
+        api.st_free_context(ctx)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    value = units / (dev_ms / 1e3)
+    e2e = units / (wall_ms / 1e3)
+    last = runs[-1]
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    sun_rays = sum(r["sun_rays"] for r in runs)
+    hits = sum(r["ray_hits"] for r in runs)
+    rec_entries = sum(r["stage_entries"][1] for r in runs)
+    pf, tf = fm.probe_flops(sun_rays), fm.trace_flops(hits, rec_entries)
+    probe_tflops = pf / (probe_ms / 1e3) / 1e12
+    trace_tflops = tf / (trace_ms / 1e3) / 1e12
+    dominant = "k_probe" if probe_ms >= trace_ms else "k_trace"
+    traffic = None
+    try:
+        traffic = json.load(open(os.path.join(ROOT, "profiles", "traffic.json"))).get(dominant)
+    except (OSError, ValueError):
+        pass
+    if dominant == "k_probe":
+        ach, pk = probe_tflops, fm.NOMINAL_FP64_TFLOPS
+        hbm_ach = fm.probe_bytes(sun_rays, hits) / (probe_ms / 1e3) / 1e9
+    else:
+        ach, pk = trace_tflops, fm.NOMINAL_FP64_TFLOPS
+        hbm_ach = fm.trace_bytes(hits) / (trace_ms / 1e3) / 1e9
+    roofline = {"bound": "fp64", "kernel": dominant, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                "frac": ach / pk, "peak_source": "nominal (148 SMs x 64 FP64 lanes x 2 x 1965 MHz); "
+                                                 "no measured FP64 vector peak on this pool",
+                "traffic": traffic,
+                "hbm": {"achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_ach / hbm_peak,
+                        "peak_source": "of measured" if "hbm_gbs" in peaks else "of fallback"},
+                "split_ms_per_step": {"k_probe+compact": probe_ms / len(runs), "k_trace": trace_ms / len(runs)},
+                "probe_tflops": probe_tflops, "trace_tflops": trace_tflops}
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = reference_sample(scenes.field_scene(args.helios, args.hits), args.cpu_seconds, args.seed)
+        except Exception as ex:  # noqa: BLE001
+            cpu = {"value": None, "unavailable": str(ex)}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_ms / len(runs), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32+fp64 (mixed)", "data": "synthetic (seeded heliostat layout and aim jitter)",
+        "config": workload(args),
+        "fp64": {"value": units64 / (dev64 / 1e3), "ms_per_step": dev64 / n64,
+                 "mixed_speedup": value / (units64 / (dev64 / 1e3)), "flux_l2_mixed_vs_fp64": max(l2)},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(last["h2d_bytes"]),
+                "d2h_bytes_per_step": int(last["d2h_bytes"]), "ms_per_step": wall_ms / len(runs)},
+        "gpu_launches": int(launches),
+        "units_per_step": units / len(runs), "sun_rays_per_step": sun_rays / len(runs),
+        "roofline": roofline, "clocks": clk.summary(), "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+    api.st_free_context(ctx)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,81 @@
+/*
+ * B200 extensions to the SolTrace C API (coretrace_api.so).
+ *
+ * These entry points have no counterpart in the reference's stapi.h; they
+ * expose controls and results of the CUDA trace that a caller of st_sim_run
+ * may want without changing the reference-compatible calls in stapi.h.
+ * All return 1 (or a non-negative count/index) on success and -1 on a bad
+ * context or argument, with the reason in st_message().
+ */
+#ifndef SOLTRACE_B200_EXT_H
+#define SOLTRACE_B200_EXT_H
+
+#include "stapi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Arithmetic of the per-ray work.
+ *   ST_B200_FP64  (default): every ray computation in double precision.
+ *   ST_B200_MIXED: element-local intersection, interaction and error sampling in
+ *                  float; global/stage/element transforms, the torus quartic, the
+ *                  Newton refinement of file-defined surfaces and all counters in
+ *                  double/64-bit integers. */
+#define ST_B200_FP64 0
+#define ST_B200_MIXED 1
+int st_b200_set_precision(st_context_t pcxt, int mode);
+
+/* 1 (default): build the per-intersection records that st_locations & co. read
+ * back, in the reference's order.  0: keep only counters and flux maps (the
+ * records are then never materialised in device or host memory). */
+int st_b200_set_records(st_context_t pcxt, int on);
+
+/* CUDA device ordinal used by st_sim_run (default 0). */
+int st_b200_set_device(st_context_t pcxt, int device);
+
+/* Deterministic input: trace these n rays (global position/direction, 3 doubles
+ * each) into the first stage instead of sampling sun rays; every supplied ray is
+ * traced once and rays that hit the first stage are numbered in input order.
+ * n = 0 returns to sun-ray sampling. */
+int st_b200_explicit_rays(st_context_t pcxt, st_uint_t n, const double *pos, const double *cos);
+
+/* Flux maps binned on the device at every intersection with (stage, element)
+ * (1-based, as in the records).  kind 0: element-local x in [x0,x1) by y in [y0,y1);
+ * kind 1: cylinder, angle atan2(x, z - x1) + pi over [0, 2 pi) (x1 is the
+ * radius) by axial y in [y0,y1).  absorbed_only selects absorbed intersections.
+ * Returns the map index. */
+int st_b200_add_flux_map(st_context_t pcxt, int stage, int element, int kind, int nx, int ny, double x0, double x1,
+                         double y0, double y1, int absorbed_only);
+int st_b200_clear_flux_maps(st_context_t pcxt);
+/* nx*ny counts, row-major [iy][ix], of the last run. */
+int st_b200_flux_counts(st_context_t pcxt, int map, unsigned long long *counts);
+
+typedef struct st_b200_stats {
+    unsigned long long sun_rays;          /* generated sun rays (64-bit SunRayCount) */
+    unsigned long long ray_hits;          /* rays numbered by a first-stage hit */
+    unsigned long long stage_entries[16]; /* rays entering stage i (i < 16) */
+    unsigned long long ray_stage_units;   /* sun_rays + sum over stages >= 2 of stage_entries */
+    unsigned long long records;           /* intersection records produced */
+    double kernel_ms;                     /* device time of the trace kernels */
+    double probe_ms, trace_ms;            /* split of kernel_ms */
+    double setup_ms, readback_ms;         /* host-side scene upload / result download */
+    int batches;                          /* sun-ray batches launched */
+    int gpu_launches;                     /* kernels launched by the run */
+    unsigned long long h2d_bytes;         /* host -> device bytes copied by the run */
+    unsigned long long d2h_bytes;         /* device -> host bytes copied by the run */
+} st_b200_stats;
+int st_b200_run_stats(st_context_t pcxt, st_b200_stats *out);
+
+/* Per-element ray accounting of the last run for a stage (1-based): first_hits[e]
+ * counts rays whose first intersection in that stage was element e+1; absorbed[e]
+ * counts intersections with element e+1 that were absorbed; delivered[e] counts
+ * rays whose first stage-1 element was e+1 and that were absorbed in the last
+ * stage (the per-heliostat intercept numerator; only filled for stage 1). */
+int st_b200_element_counts(st_context_t pcxt, int stage, unsigned long long *first_hits,
+                           unsigned long long *absorbed, unsigned long long *delivered);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

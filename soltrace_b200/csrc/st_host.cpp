@@ -1,0 +1,1587 @@
+// Host side of coretrace_api.so: the SolTrace context and its C API
+// (coretrace/stapi.h:68-176), geometry set-up, acceleration structures and
+// the assembly of the records the device returns into the reference's order.
+//
+// The scene model follows coretrace/types.h:85-343; set-up follows
+// coretrace/input.cpp (InitGeometries 153-286, TranslateSurfaceParams 288-366,
+// ReadSurfaceFile 368-573, CheckInputs 87-150), coretrace/apertureplane.cpp
+// and coretrace/suntoprimarystage.cpp, and then flattens everything into the
+// device tables of st_scene.h.
+#include <algorithm>
+#include <cctype>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <strings.h>
+#include <vector>
+
+#include "../../include/st_b200.h"
+#include "st_host.h"
+
+namespace {
+
+using namespace stb;
+constexpr double kDegToRad = 0.017453292519943295;
+constexpr double kPi = 3.141592653589793238462643;
+
+struct Face {
+    char dist = 'g';
+    int optnum = 1, apgr = 0, order = 0;
+    double refl = 0, trans = 0, slope = 0, spec = 0;
+    double n[4] = {0, 0, 0, 0};
+    double ab12[4] = {0, 0, 0, 0};
+    std::vector<double> refl_tab, trans_tab;  // (angle, value) pairs
+    bool use_refl = false, use_trans = false;
+};
+struct OpticSet {
+    std::string name;
+    Face front, back;
+};
+struct Elem {
+    bool enabled = true;
+    double origin[3] = {0, 0, 0}, aim[3] = {0, 0, 0}, zrot = 0;
+    char shape = ' ';
+    double p[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    char surface = ' ';
+    int stype = 0;
+    double kappa = 0, alpha[5] = {0, 0, 0, 0, 0}, vcx = 0, vcy = 0, ra = 0, rs = 0, cone = 0, curv = 0;
+    int fit_order = 0;
+    std::vector<double> bcoef, poly, spl_x, spl_y, spl_y2, vshot;
+    int vshot_rows = 0;
+    bool fe_surface = false;
+    int interaction = 0;
+    std::string optic;
+    // derived
+    double R[9] = {0}, area = 0, zap = 0;
+    int optic_idx = -1;
+};
+struct StageM {
+    bool multihit = true, virt = false, tracethrough = false;
+    double origin[3] = {0, 0, 0}, aim[3] = {0, 0, 0}, zrot = 0;
+    double R[9] = {0};
+    std::vector<Elem> elems;
+};
+struct SunM {
+    char shape = ' ';
+    double sigma = 0;
+    bool point_source = false;
+    std::vector<double> ang, inten;  // mirrored table
+    double max_angle = 0, max_intensity = 0;
+    double origin[3] = {0, 0, 0};
+    double xmin = 0, xmax = 0, ymin = 0, ymax = 0;
+};
+struct FluxMap {
+    FluxMapReq req;
+    std::vector<unsigned long long> counts;
+};
+
+struct Context {
+    SunM sun;
+    std::vector<OpticSet> optics;
+    std::vector<StageM> stages;
+    int raycount = 1000, raymax = 100000;
+    bool dyn = false, err_sun = true, err_opt = true;
+    std::vector<std::string> messages;
+    // results
+    std::vector<RecordDev> records;  // reference order
+    uint64_t sun_rays = 0;
+    int precision = ST_B200_FP64;
+    bool want_records = true;
+    int device = 0;
+    std::vector<double> ex_pos, ex_cos;
+    std::vector<FluxMap> flux;
+    st_b200_stats stats;
+    std::vector<std::vector<unsigned long long>> elem_first, elem_absorbed, elem_delivered;
+    int (*cb)(unsigned long, unsigned long, unsigned long, unsigned long, unsigned long, void *) = nullptr;
+    void *cbdata = nullptr;
+    double last_hit_rate = 0.0;  // batch planning hint carried between runs of a context
+    Context() { memset(&stats, 0, sizeof stats); }
+    void log(const char *fmt, ...) {
+        char buf[513];
+        va_list a;
+        va_start(a, fmt);
+        vsnprintf(buf, 512, fmt, a);
+        va_end(a);
+        messages.push_back(buf);
+    }
+};
+
+// ---------------- math (mathproc.cpp:175-217, input.cpp:160-176) ----------------
+void rot_from_euler(const double e[3], double R[9]) {
+    const double ca = cos(e[0]), cb = cos(e[1]), cg = cos(e[2]);
+    const double sa = sin(e[0]), sb = sin(e[1]), sg = sin(e[2]);
+    R[0] = ca * cg + sa * sb * sg;
+    R[1] = -cb * sg;
+    R[2] = -sa * cg + ca * sb * sg;
+    R[3] = ca * sg - sa * sb * cg;
+    R[4] = cb * cg;
+    R[5] = -sa * sg - ca * sb * cg;
+    R[6] = sa * cb;
+    R[7] = sb;
+    R[8] = ca * cb;
+}
+bool euler_of(const double o[3], const double a[3], double zrot, double e[3]) {
+    double dx = a[0] - o[0], dy = a[1] - o[1], dz = a[2] - o[2];
+    const double d = sqrt(dx * dx + dy * dy + dz * dz);
+    if (d == 0.0) return false;
+    dx = dx / d;
+    dy = dy / d;
+    dz = dz / d;
+    e[0] = atan2(dx, dz);
+    e[1] = asin(dy);
+    e[2] = zrot * kDegToRad;
+    return true;
+}
+void mulv(const double R[9], const double v[3], double o[3]) {
+    o[0] = R[0] * v[0] + R[1] * v[1] + R[2] * v[2];
+    o[1] = R[3] * v[0] + R[4] * v[1] + R[5] * v[2];
+    o[2] = R[6] * v[0] + R[7] * v[1] + R[8] * v[2];
+}
+void mulvt(const double R[9], const double v[3], double o[3]) {
+    o[0] = R[0] * v[0] + R[3] * v[1] + R[6] * v[2];
+    o[1] = R[1] * v[0] + R[4] * v[1] + R[7] * v[2];
+    o[2] = R[2] * v[0] + R[5] * v[1] + R[8] * v[2];
+}
+inline double sq(double x) { return x * x; }
+
+double mono_at(const Elem &e, double x, double y) {
+    const int w = e.fit_order + 1;
+    double z = 0.0;
+    for (int i = 0; i <= e.fit_order; ++i)
+        for (int j = 0; j <= i; ++j) {
+            const double xx = (j == 0) ? 1.0 : pow(x, j);
+            const double yy = (i - j == 0) ? 1.0 : pow(y, i - j);
+            z = z + e.bcoef[i * w + j] * xx * yy;
+        }
+    return z;
+}
+double poly_at(const Elem &e, double r) {
+    double z = 0.0;
+    for (int i = 0; i <= e.fit_order; ++i) z = z + e.poly[i] * pow(r, i);
+    return z;
+}
+
+// natural / end-slope cubic spline second derivatives (tridiagonal sweep)
+void spline_y2(const std::vector<double> &x, const std::vector<double> &y, double yp1, double ypn,
+               std::vector<double> &y2) {
+    const int n = int(x.size());
+    std::vector<double> u(n, 0.0);
+    y2.assign(n, 0.0);
+    if (n < 2) return;
+    if (yp1 > 0.99e30) {
+        y2[0] = 0.0;
+        u[0] = 0.0;
+    } else {
+        y2[0] = -0.5;
+        u[0] = (3.0 / (x[1] - x[0])) * ((y[1] - y[0]) / (x[1] - x[0]) - yp1);
+    }
+    for (int i = 1; i < n - 1; ++i) {
+        const double sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1]);
+        const double p = sig * y2[i - 1] + 2.0;
+        y2[i] = (sig - 1.0) / p;
+        u[i] = (y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1]);
+        u[i] = (6.0 * u[i] / (x[i + 1] - x[i - 1]) - sig * u[i - 1]) / p;
+    }
+    double qn = 0.0, un = 0.0;
+    if (!(ypn > 0.99e30)) {
+        qn = 0.5;
+        un = (3.0 / (x[n - 1] - x[n - 2])) * (ypn - (y[n - 1] - y[n - 2]) / (x[n - 1] - x[n - 2]));
+    }
+    y2[n - 1] = (un - qn * u[n - 2]) / (qn * y2[n - 2] + 1.0);
+    for (int k = n - 2; k >= 0; --k) y2[k] = y2[k] * y2[k + 1] + u[k];
+}
+
+// ---------------- surface translation (input.cpp:288-366) ----------------
+bool translate_surface(Context *cx, Elem &e, const double p[8]) {
+    const bool line = (e.shape == 'l' || e.shape == 'L');
+    switch (e.surface) {
+        case 's':
+        case 'S':
+            e.vcx = p[0];
+            e.vcy = line ? 0.0 : e.vcx;
+            e.kappa = 1.0;
+            e.stype = (e.vcy == 0.0) ? 7 : 1;
+            return true;
+        case 'p':
+        case 'P':
+            e.vcx = p[0];
+            e.vcy = p[1];
+            e.kappa = 0.0;
+            e.stype = (e.vcy == 0.0) ? 7 : 1;
+            return true;
+        case 'o':
+        case 'O':
+            e.vcx = p[0];
+            e.vcy = p[0];
+            e.kappa = p[1];
+            e.stype = (e.vcy == 0.0) ? 7 : 1;
+            return true;
+        case 'g':
+        case 'G':
+            e.vcx = p[0];
+            e.vcy = p[1];
+            e.kappa = p[2];
+            for (int i = 0; i < 5; ++i) e.alpha[i] = p[3 + i];
+            e.stype = (e.vcy == 0.0) ? 7 : 1;
+            return true;
+        case 'f':
+        case 'F':
+            e.alpha[0] = 0;
+            e.alpha[1] = 0;
+            e.alpha[2] = 1;
+            e.alpha[3] = 0;
+            e.alpha[4] = 0;
+            e.stype = 3;
+            return true;
+        case 'c':
+        case 'C':
+            e.cone = p[0];
+            e.stype = 1;
+            return true;
+        case 't':
+        case 'T':
+            if (!line || e.p[0] != 0.0 || e.p[1] != 0.0) {
+                cx->log("Bad aperture or parameters of element not consistent with cylindrical surface\n");
+                return false;
+            }
+            e.curv = p[0];
+            e.vcx = e.curv;
+            e.stype = 2;
+            return true;
+        case 'd':
+        case 'D':
+            if ((e.shape != 'a' && e.shape != 'A') || e.p[0] != 0.0 || e.p[1] != 0.0) {
+                cx->log("Bad aperture or parameters of element not consistent with toroidal surface\n");
+                return false;
+            }
+            e.ra = p[0];
+            e.rs = p[1];
+            e.stype = 10;
+            return true;
+        default:
+            cx->log("invalid surface index: %c\n", e.surface);
+            return false;
+    }
+}
+
+// ---------------- ZAperture (apertureplane.cpp:57-491) ----------------
+void aperture_plane(Elem &e) {
+    const char sh = char(tolower(e.shape));
+    double maxr = 0.0;
+    if (sh == 'i' || sh == 'q') {
+        maxr = sqrt(sq(e.p[0]) + sq(e.p[1]));
+        maxr = std::max(maxr, sqrt(sq(e.p[2]) + sq(e.p[3])));
+        maxr = std::max(maxr, sqrt(sq(e.p[4]) + sq(e.p[5])));
+        if (sh == 'q') maxr = std::max(maxr, sqrt(sq(e.p[6]) + sq(e.p[7])));
+    }
+    // family: 1 circle/hexagon/triangle, 2 rectangle, 3 annulus/line, 4 irregular
+    int fam = 0;
+    double r2 = 0.0;
+    if (sh == 'c' || sh == 'h' || sh == 't') {
+        fam = 1;
+        r2 = sq(e.p[0] / 2.0);
+    } else if (sh == 'r') {
+        fam = 2;
+        r2 = sq(e.p[0] / 2.0) + sq(e.p[1] / 2.0);
+    } else if (sh == 'a' || sh == 'l') {
+        fam = 3;
+        r2 = (fabs(e.p[1]) >= fabs(e.p[0])) ? sq(e.p[1]) : sq(e.p[0]);
+    } else if (sh == 'i' || sh == 'q') {
+        fam = 4;
+        r2 = sq(maxr);
+    }
+    switch (tolower(e.surface)) {
+        case 'g': {
+            if (!fam) break;
+            double sum = 0.0;
+            if (fam == 1) {
+                double rho = 1.0;
+                for (int i = 0; i < 5; ++i) {
+                    rho = rho * r2;
+                    sum += e.alpha[i] * rho;
+                }
+                e.zap = e.vcx * r2 / (1 + sqrt(1 - e.kappa * e.vcx * e.vcx * r2)) + sum;
+            } else {
+                if (fam != 4)
+                    for (int i = 0; i < 5; ++i) sum += e.alpha[i] * pow(r2, (int)(i + 1));
+                e.zap = e.vcx * r2 / (1 + sqrt(1 - e.kappa * sq(e.vcx) * r2)) + sum;
+            }
+            break;
+        }
+        case 's':
+            if (fam) {
+                const double f = 1.0 / (2.0 * e.vcx);
+                e.zap = 2.0 * f - sqrt(sq(2.0 * f) - r2);
+            }
+            break;
+        case 'p':
+            if (fam) e.zap = r2 / (4.0 * (1.0 / (2.0 * e.vcx)));
+            break;
+        case 'm':
+            if (fam && e.fit_order >= 2) {
+                const int w = e.fit_order + 1;
+                const double f = (1.0 / (4.0 * e.bcoef[2 * w + 0]) + 1.0 / (4.0 * e.bcoef[2 * w + 2])) / 2.0;
+                e.zap = r2 / (4.0 * f);
+            }
+            break;
+        case 'f':
+            e.zap = 0.0;
+            break;
+        case 'o':
+            if (fam) e.zap = (1 - sqrt(1 - e.kappa * sq(e.vcx) * r2)) / (e.kappa * e.vcx);
+            break;
+        case 'c': {
+            const double t = tan(e.cone * kDegToRad);
+            if (fam == 1)
+                e.zap = e.p[0] / (2.0 * t);
+            else if (fam == 2 || fam == 4)
+                e.zap = sqrt(r2) / (2.0 * t);
+            else if (sh == 'a')
+                e.zap = e.p[1] / t;
+            break;
+        }
+        case 't':
+            e.zap = 2.0 / e.curv;
+            break;
+        case 'd':
+            e.zap = 2.0 * e.rs;
+            break;
+        case 'r':
+            if (fam) e.zap = poly_at(e, fam == 1 ? e.p[0] / 2.0 : sqrt(r2));
+            break;
+        case 'i':
+            if (!e.spl_y.empty()) e.zap = e.spl_y.back();
+            break;
+        case 'v': {
+            double z = 0.0;
+            for (int i = 0; i < e.vshot_rows; ++i) z = std::max(z, mono_at(e, e.vshot[5 * i], e.vshot[5 * i + 1]));
+            e.zap = z;
+            break;
+        }
+        case 'e': {
+            double z = 0.0;  // the reference scans the nodes' second coordinate
+            for (size_t i = 0; i + 2 < e.vshot.size(); i += 3) z = std::max(z, e.vshot[i + 1]);
+            e.zap = z;
+            break;
+        }
+        default:
+            break;
+    }
+}
+
+bool check_inputs(Context *cx) {  // input.cpp:87-150
+    for (size_t i = 0; i < cx->stages.size(); ++i)
+        for (size_t j = 0; j < cx->stages[i].elems.size(); ++j) {
+            const Elem &e = cx->stages[i].elems[j];
+            const bool pp = e.surface == 'p' || e.surface == 'P', ss = e.surface == 's' || e.surface == 'S';
+            const bool line = e.shape == 'l' || e.shape == 'L';
+            if (pp && line && e.vcy != 0.0) {
+                cx->log("Parabolic surface combined with single axis curvature section aperture must have Cy = 0.  Element %d Stage %d.",
+                        int(j + 1), int(i + 1));
+                return false;
+            }
+            if (ss && e.vcx == 0.0) {
+                cx->log("Spherical surface must have a curvature greater than 0.0.  Consider using a flat surface instead. Element %d, Stage %d.",
+                        int(j + 1), int(i + 1));
+                return false;
+            }
+            if (ss && e.vcy != 0.0 && e.vcy != e.vcx) {
+                cx->log("Spherical surface must have Cy=0 or Cy=Cx.  Currently, Cy=%lg for Element %d, Stage %d", e.vcy,
+                        int(j + 1), int(i + 1));
+                return false;
+            }
+            if ((e.surface == 'o' || e.surface == 'O') && (e.kappa == 1.0 || e.kappa == 0.0)) {
+                cx->log("Kappa = 0.0 or 1.0 defines either a parabola or a sphere.  Use the specific surface definition for either of those cases. Element %d, Stage %d.",
+                        int(j + 1), int(i + 1));
+                return false;
+            }
+        }
+    return true;
+}
+
+bool init_geometries(Context *cx) {  // input.cpp:153-286
+    for (size_t i = 0; i < cx->stages.size(); ++i) {
+        StageM &st = cx->stages[i];
+        double eu[3];
+        if (!euler_of(st.origin, st.aim, st.zrot, eu)) {
+            cx->log("Stage %d geometry as defined not possible.\n", int(i));
+            return false;
+        }
+        rot_from_euler(eu, st.R);
+        for (size_t j = 0; j < st.elems.size(); ++j) {
+            Elem &e = st.elems[j];
+            if (!euler_of(e.origin, e.aim, e.zrot, eu)) {
+                cx->log("Stage %d element %d geometry as defined not possible.\n", int(i), int(j));
+                return false;
+            }
+            rot_from_euler(eu, e.R);
+            const double *p = e.p;
+            switch (e.shape) {
+                case 'c':
+                case 'C':
+                    e.area = kPi * sq(p[0] / 2);
+                    break;
+                case 'h':
+                case 'H':
+                    e.area = 5.0 * sq(p[0] / 2.0) * cos(30.0 * kDegToRad) * sin(30.0 * kDegToRad);
+                    break;
+                case 'r':
+                case 'R':
+                    e.area = p[0] * p[1];
+                    break;
+                case 't':
+                case 'T':
+                    e.area = 0.25 * sq(p[0] * cos(30.0 * kDegToRad)) * sqrt(3.0);
+                    break;
+                case 'a':
+                case 'A':
+                    e.area = p[2] * kDegToRad * (p[1] - p[0]);
+                    break;
+                case 'l':
+                case 'L':
+                    e.area = (p[1] - p[0]) * p[2];
+                    break;
+                case 'i':
+                case 'I': {
+                    const double v11 = p[0] - p[2], v12 = p[1] - p[3], v21 = p[4] - p[2], v22 = p[5] - p[3];
+                    const double a = sqrt(v11 * v11 + v12 * v12), b = sqrt(v21 * v21 + v22 * v22);
+                    e.area = 0.5 * a * b * sin(acos((v11 * v21 + v12 * v22) / (a * b)));
+                    break;
+                }
+                case 'q':
+                case 'Q': {
+                    const double v11 = p[0] - p[2], v12 = p[1] - p[3], v21 = p[4] - p[2], v22 = p[5] - p[3];
+                    const double v31 = p[4] - p[6], v32 = p[5] - p[7], v41 = p[0] - p[6], v42 = p[1] - p[7];
+                    const double a = sqrt(v11 * v11 + v12 * v12), b = sqrt(v21 * v21 + v22 * v22);
+                    const double c = sqrt(v31 * v31 + v32 * v32), d = sqrt(v41 * v41 + v42 * v42);
+                    e.area = 0.5 * (a * b * sin(acos((v11 * v21 + v12 * v22) / (a * b))) +
+                                    c * d * sin(acos((v31 * v41 + v32 * v42) / (c * d))));
+                    break;
+                }
+                default:
+                    cx->log("invalid shape '%c' for aperture, element %d\n", e.shape, int(j));
+                    return false;
+            }
+            if (!st.virt) {
+                int found = -1;
+                for (size_t k = 0; k < cx->optics.size(); ++k)
+                    if (strcasecmp(cx->optics[k].name.c_str(), e.optic.c_str()) == 0) found = int(k);
+                if (found < 0) {
+                    cx->log("Stage %d element %d invalid optical property set name: '%s'\n", int(i), int(j),
+                            e.optic.c_str());
+                    return false;
+                }
+                e.optic_idx = found;
+                OpticSet &set = cx->optics[found];
+                set.front.n[2] = set.back.n[0];
+                set.front.n[3] = set.back.n[1];
+                set.back.n[2] = set.front.n[0];
+                set.back.n[3] = set.front.n[1];
+            } else {
+                e.optic_idx = -1;
+            }
+            aperture_plane(e);
+        }
+    }
+    return check_inputs(cx);
+}
+
+// Radius about the element origin that contains every hit the trace can accept,
+// or -1 when no finite bound is known for the surface (those elements are tested
+// for every ray).  Used to build the sun-plane grid and the stage BVHs.
+double accept_radius(const Elem &e) {
+    const char sh = char(tolower(e.shape));
+    double rap;
+    switch (sh) {
+        case 'c':
+        case 'h':
+            rap = e.p[0] / 2.0;
+            break;
+        case 't':
+            rap = e.p[0] / 2.0;
+            break;
+        case 'r':
+            rap = 0.5 * sqrt(sq(e.p[0]) + sq(e.p[1]));
+            break;
+        case 'a':
+            rap = std::max(fabs(e.p[0]), fabs(e.p[1]));
+            break;
+        case 'l':
+            rap = sqrt(sq(std::max(fabs(e.p[0]), fabs(e.p[1]))) + sq(e.p[2] / 2.0));
+            break;
+        case 'i':
+        case 'q': {
+            rap = 0;
+            for (int k = 0; k < (sh == 'q' ? 8 : 6); k += 2) rap = std::max(rap, sqrt(sq(e.p[k]) + sq(e.p[k + 1])));
+            break;
+        }
+        default:
+            return -1.0;
+    }
+    const int s = tolower(e.surface);
+    double zext;
+    if (e.stype == 3) {
+        zext = 0.0;
+    } else if (s == 'p' && e.stype != 2) {
+        // z = (Cx x^2 + Cy y^2)/2 on the surface, for (x, y) inside the aperture
+        zext = 0.5 * std::max(fabs(e.vcx), fabs(e.vcy)) * rap * rap;
+    } else if (e.stype == 2) {
+        // cylinder about the local y axis through (0, y, r): |x| <= r, 0 <= z <= 2r
+        const double r = fabs(1.0 / e.curv);
+        return sqrt(sq(r) + sq(e.p[2] / 2.0) + sq(2.0 * r)) * (1.0 + 1e-9) + 1e-6;
+    } else if (e.stype == 10) {
+        return sqrt(sq(fabs(e.ra) + fabs(e.rs)) + sq(2.0 * fabs(e.rs))) * (1.0 + 1e-9) + 1e-6;
+    } else if (s == 's' && e.vcx > 0.0) {
+        // accepted hits satisfy z <= ZAperture on the lower cap (0 <= z)
+        zext = std::max(fabs(e.zap), 0.0);
+    } else {
+        return -1.0;
+    }
+    return sqrt(rap * rap + zext * zext) * (1.0 + 1e-9) + 1e-6;
+}
+
+// Median-split BVH over element bounding spheres (stage coordinates).
+void build_bvh(const std::vector<Elem> &els, std::vector<BvhNode> &nodes, std::vector<int> &items) {
+    struct Item {
+        int j;
+        double c[3], r;
+    };
+    std::vector<Item> its;
+    for (size_t j = 0; j < els.size(); ++j) {
+        const double r = accept_radius(els[j]);
+        Item it;
+        it.j = int(j);
+        for (int q = 0; q < 3; ++q) it.c[q] = els[j].origin[q];
+        it.r = (r < 0) ? 1e30 : r;  // unbounded elements get an all-space box
+        its.push_back(it);
+    }
+    const size_t base = nodes.size();
+    (void)base;
+    struct Task {
+        int node, lo, hi;
+    };
+    auto box = [&](int lo, int hi, BvhNode &nd) {
+        double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+        for (int k = lo; k < hi; ++k)
+            for (int q = 0; q < 3; ++q) {
+                mn[q] = std::min(mn[q], its[k].c[q] - its[k].r);
+                mx[q] = std::max(mx[q], its[k].c[q] + its[k].r);
+            }
+        for (int q = 0; q < 3; ++q) {
+            // pad for the float traversal: 1 mm plus 1e-6 of the coordinate
+            const double pl = 1e-3 + 1e-6 * fabs(mn[q]), ph = 1e-3 + 1e-6 * fabs(mx[q]);
+            nd.lo[q] = float(std::max(mn[q] - pl, -3.0e38));
+            nd.hi[q] = float(std::min(mx[q] + ph, 3.0e38));
+            nd.lo[q] = std::nextafter(nd.lo[q], -INFINITY);
+            nd.hi[q] = std::nextafter(nd.hi[q], INFINITY);
+        }
+    };
+    std::vector<BvhNode> out(1);
+    std::vector<Task> todo{{0, 0, int(its.size())}};
+    while (!todo.empty()) {
+        Task t = todo.back();
+        todo.pop_back();
+        BvhNode nd;
+        box(t.lo, t.hi, nd);
+        if (t.hi - t.lo <= 4) {
+            nd.first = t.lo;
+            nd.count = t.hi - t.lo;
+            out[t.node] = nd;
+            continue;
+        }
+        double cmn[3] = {1e300, 1e300, 1e300}, cmx[3] = {-1e300, -1e300, -1e300};
+        for (int k = t.lo; k < t.hi; ++k)
+            for (int q = 0; q < 3; ++q) {
+                cmn[q] = std::min(cmn[q], its[k].c[q]);
+                cmx[q] = std::max(cmx[q], its[k].c[q]);
+            }
+        int ax = 0;
+        for (int q = 1; q < 3; ++q)
+            if (cmx[q] - cmn[q] > cmx[ax] - cmn[ax]) ax = q;
+        const int mid = (t.lo + t.hi) / 2;
+        std::nth_element(its.begin() + t.lo, its.begin() + mid, its.begin() + t.hi,
+                         [ax](const Item &a, const Item &b) { return a.c[ax] < b.c[ax]; });
+        const int left = int(out.size());
+        out.push_back(BvhNode());
+        out.push_back(BvhNode());
+        nd.first = left;
+        nd.count = 0;
+        out[t.node] = nd;
+        todo.push_back({left + 1, mid, t.hi});
+        todo.push_back({left, t.lo, mid});
+    }
+    nodes.insert(nodes.end(), out.begin(), out.end());
+    for (auto &it : its) items.push_back(it.j);
+}
+
+// ---------------- the sun frame and sun box (suntoprimarystage.cpp:59-293) ----------------
+bool sun_setup(Context *cx, HostScene &hs) {
+    StageM &st = cx->stages[0];
+    SunM &sun = cx->sun;
+    const double dx = 0.0 - sun.origin[0], dy = 0.0 - sun.origin[1], dz = 0.0 - sun.origin[2];
+    const double dt = sqrt(dx * dx + dy * dy + dz * dz);
+    if (dt == 0.0) {
+        cx->log("error calculating sun position in primary stage, dtot = 0.0\n");
+        return false;
+    }
+    const double cg[3] = {dx / dt, dy / dt, dz / dt};
+    double cs[3];
+    mulv(st.R, cg, cs);
+    const double se[3] = {atan2(cs[0], cs[2]), asin(cs[1]), 0.0};
+    double Rs[9];
+    rot_from_euler(se, Rs);
+    sun.xmax = -1.0e20;
+    sun.xmin = 1.0e20;
+    sun.ymax = -1.0e20;
+    sun.ymin = 1.0e20;
+    const double cd[3] = {0, 0, 1};
+    (void)cd;
+    size_t n = 0;
+    for (const Elem &e : st.elems) {
+        if (!e.enabled) continue;
+        double pl[3];
+        mulv(Rs, e.origin, pl);
+        double ext = 0.0;
+        const double *p = e.p;
+        switch (e.shape) {
+            case 'c':
+            case 'C':
+            case 'h':
+            case 'H':
+                ext = p[0] / 2.0;
+                break;
+            case 'r':
+            case 'R':
+                ext = sqrt((p[0] * p[0] + p[1] * p[1]) / 4.0);
+                break;
+            case 't':
+            case 'T':
+                ext = p[0] / (2.0 * cos(30.0 * kDegToRad));
+                break;
+            case 'a':
+            case 'A':
+                ext = p[1];
+                break;
+            case 'l':
+            case 'L': {
+                const double leg = (fabs(p[1]) >= fabs(p[0])) ? p[1] : p[0];
+                ext = sqrt(leg * leg + 0.25 * p[2] * p[2]);
+                break;
+            }
+            case 'i':
+            case 'I':
+            case 'q':
+            case 'Q': {
+                double m = sqrt(p[0] * p[0] + p[1] * p[1]);
+                m = std::max(m, sqrt(p[2] * p[2] + p[3] * p[3]));
+                m = std::max(m, sqrt(p[4] * p[4] + p[5] * p[5]));
+                if (e.shape == 'q' || e.shape == 'Q') m = std::max(m, sqrt(p[6] * p[6] + p[7] * p[7]));
+                ext = m;
+                break;
+            }
+            default:
+                break;
+        }
+        if (pl[0] - ext < sun.xmin) sun.xmin = pl[0] - ext;
+        if (pl[0] + ext > sun.xmax) sun.xmax = pl[0] + ext;
+        if (pl[1] - ext < sun.ymin) sun.ymin = pl[1] - ext;
+        if (pl[1] + ext > sun.ymax) sun.ymax = pl[1] + ext;
+        n++;
+    }
+    if (n == 0) {
+        cx->log("error calculating sun position in primary stage because no elements were enabled");
+        return false;
+    }
+    SunDev &sd = hs.dev.sun;
+    sd.xmin = sun.xmin;
+    sd.xmax = sun.xmax;
+    sd.ymin = sun.ymin;
+    sd.ymax = sun.ymax;
+    for (int k = 0; k < 9; ++k) sd.Rsun[k] = Rs[k];
+    for (int k = 0; k < 3; ++k) {
+        sd.pos_sun_stage[k] = 0.0;  // the sun frame is centred on the first stage's origin
+        sd.origin[k] = sun.origin[k];
+    }
+    sd.shape = sun.shape;
+    sd.point_source = sun.point_source ? 1 : 0;
+    sd.sigma = sun.sigma;
+
+    // inverse CDF of theta * I(theta) on [0, MaxAngle] for table sunshapes
+    hs.cdf_theta.clear();
+    hs.cdf.clear();
+    if (sun.ang.size() >= 3 && sun.max_angle > 0) {
+        auto intensity = [&](double th) {
+            size_t i = 0;
+            while (i < sun.ang.size() - 1 && sun.ang[i] < th) i++;
+            if (i == 0) return sun.inten[0];
+            return sun.inten[i - 1] + (sun.inten[i] - sun.inten[i - 1]) * (th - sun.ang[i - 1]) / (sun.ang[i] - sun.ang[i - 1]);
+        };
+        const int K = kSunCdfCells;
+        hs.cdf_theta.assign(K + 1, 0.0);
+        hs.cdf.assign(K + 1, 0.0);
+        const double dth = sun.max_angle / K;
+        double prev = 0.0;
+        for (int j = 0; j <= K; ++j) {
+            const double th = dth * j;
+            const double pdf = th * intensity(th);
+            hs.cdf_theta[j] = th;
+            if (j > 0) hs.cdf[j] = hs.cdf[j - 1] + 0.5 * (prev + pdf) * dth;
+            prev = pdf;
+        }
+        const double tot = hs.cdf[K];
+        for (int j = 0; j <= K; ++j) hs.cdf[j] = tot > 0 ? hs.cdf[j] / tot : 0.0;
+    }
+
+    // sun-plane grid over the first stage: every element whose bounding disc (centre
+    // = projected origin, radius = accept radius) overlaps a cell is listed there
+    sd.grid_on = 0;
+    hs.cell_start.assign(2, 0);
+    hs.cell_items.clear();
+    if (!sun.point_source && st.elems.size() >= 4) {
+        bool bounded = true;
+        double rmax = 0;
+        std::vector<double> rad(st.elems.size()), cx_(st.elems.size()), cy_(st.elems.size());
+        for (size_t j = 0; j < st.elems.size(); ++j) {
+            const double r = accept_radius(st.elems[j]);
+            if (r < 0) {
+                bounded = false;
+                break;
+            }
+            double pl[3];
+            mulv(Rs, st.elems[j].origin, pl);
+            rad[j] = r;
+            cx_[j] = pl[0];
+            cy_[j] = pl[1];
+            rmax = std::max(rmax, r);
+        }
+        if (bounded && rmax > 0) {
+            const double W = sun.xmax - sun.xmin, H = sun.ymax - sun.ymin;
+            double cell = std::max(rmax * 0.5, 1e-6);
+            // keep the grid within ~4M cells
+            while ((W / cell + 1) * (H / cell + 1) > 4.0e6) cell *= 1.5;
+            const int nx = std::max(1, int(ceil(W / cell))), ny = std::max(1, int(ceil(H / cell)));
+            std::vector<std::vector<int>> cells(size_t(nx) * ny);
+            for (size_t j = 0; j < st.elems.size(); ++j) {
+                const double pad = rad[j] * (1.0 + 1e-9) + 1e-6 * (1.0 + fabs(cx_[j]) + fabs(cy_[j]));
+                const int x0 = std::max(0, int(floor((cx_[j] - pad - sun.xmin) / cell)));
+                const int x1 = std::min(nx - 1, int(floor((cx_[j] + pad - sun.xmin) / cell)));
+                const int y0 = std::max(0, int(floor((cy_[j] - pad - sun.ymin) / cell)));
+                const int y1 = std::min(ny - 1, int(floor((cy_[j] + pad - sun.ymin) / cell)));
+                for (int gy = y0; gy <= y1; ++gy)
+                    for (int gx = x0; gx <= x1; ++gx) {
+                        // distance from the disc centre to the cell rectangle
+                        const double ax = sun.xmin + gx * cell, bx = ax + cell;
+                        const double ay = sun.ymin + gy * cell, by = ay + cell;
+                        const double ddx = std::max(std::max(ax - cx_[j], 0.0), cx_[j] - bx);
+                        const double ddy = std::max(std::max(ay - cy_[j], 0.0), cy_[j] - by);
+                        if (ddx * ddx + ddy * ddy <= pad * pad) cells[size_t(gy) * nx + gx].push_back(int(j));
+                    }
+            }
+            hs.cell_start.assign(size_t(nx) * ny + 1, 0);
+            for (size_t c = 0; c < cells.size(); ++c) {
+                hs.cell_start[c + 1] = hs.cell_start[c] + int(cells[c].size());
+                hs.cell_items.insert(hs.cell_items.end(), cells[c].begin(), cells[c].end());
+            }
+            sd.grid_on = 1;
+            sd.gnx = nx;
+            sd.gny = ny;
+            sd.gx0 = sun.xmin;
+            sd.gy0 = sun.ymin;
+            sd.ginv = 1.0 / cell;
+        }
+    }
+    return true;
+}
+
+bool flatten(Context *cx, HostScene &hs) {
+    hs = HostScene();
+    memset(&hs.dev, 0, sizeof hs.dev);
+    if (cx->stages.size() > size_t(kMaxStages)) {
+        cx->log("at most %d stages are supported", kMaxStages);
+        return false;
+    }
+    // optics: two OpticRec per set (front, back)
+    for (const OpticSet &os : cx->optics) {
+        for (int fb = 0; fb < 2; ++fb) {
+            const Face &f = fb ? os.back : os.front;
+            OpticRec r;
+            memset(&r, 0, sizeof r);
+            r.refl = f.refl;
+            r.trans = f.trans;
+            r.slope = f.slope;
+            r.spec = f.spec;
+            r.n_in = f.n[0];
+            r.n_out = f.n[2];
+            r.dist = f.dist;
+            r.refl_tab_off = int(hs.tables.size());
+            r.refl_tab_n = f.use_refl ? int(f.refl_tab.size() / 2) : 0;
+            if (f.use_refl) hs.tables.insert(hs.tables.end(), f.refl_tab.begin(), f.refl_tab.end());
+            r.trans_tab_off = int(hs.tables.size());
+            r.trans_tab_n = f.use_trans ? int(f.trans_tab.size() / 2) : 0;
+            if (f.use_trans) hs.tables.insert(hs.tables.end(), f.trans_tab.begin(), f.trans_tab.end());
+            hs.optics.push_back(r);
+        }
+    }
+    hs.dev.n_stages = int(cx->stages.size());
+    for (size_t si = 0; si < cx->stages.size(); ++si) {
+        const StageM &st = cx->stages[si];
+        StageRec &sr = hs.dev.stages[si];
+        for (int k = 0; k < 9; ++k) sr.R[k] = st.R[k];
+        for (int k = 0; k < 3; ++k) sr.o[k] = st.origin[k];
+        sr.first_elem = int(hs.elems.size());
+        sr.n_elem = int(st.elems.size());
+        sr.virt = st.virt;
+        sr.multihit = st.multihit;
+        sr.tracethrough = st.tracethrough;
+        sr.bvh_off = -1;
+        for (const Elem &e : st.elems) {
+            if (e.fe_surface) {
+                cx->log("finite-element surface files (.fed) are not supported by the B200 trace");
+                return false;
+            }
+            ElemRec r;
+            memset(&r, 0, sizeof r);
+            for (int k = 0; k < 9; ++k) r.R[k] = e.R[k];
+            for (int k = 0; k < 3; ++k) r.o[k] = e.origin[k];
+            for (int k = 0; k < 8; ++k) r.ap[k] = e.p[k];
+            r.zap = e.zap;
+            r.kappa = e.kappa;
+            r.vcx = e.vcx;
+            r.vcy = e.vcy;
+            r.curv_rev = e.curv;
+            r.cone_deg = e.cone;
+            r.ra = e.ra;
+            r.rs = e.rs;
+            r.area = e.area;
+            r.bound_r = accept_radius(e);
+            r.shape = tolower(e.shape);
+            r.surf = e.surface;
+            r.stype = e.stype;
+            r.interaction = e.interaction;
+            r.opt_front = e.optic_idx >= 0 ? 2 * e.optic_idx : -1;
+            r.opt_back = e.optic_idx >= 0 ? 2 * e.optic_idx + 1 : -1;
+            r.enabled = e.enabled;
+            r.fit_order = e.fit_order;
+            r.data_off = int(hs.surf_data.size());
+            switch (e.stype) {
+                case kSurfZernike:
+                    hs.surf_data.insert(hs.surf_data.end(), e.bcoef.begin(), e.bcoef.end());
+                    break;
+                case kSurfVshot:
+                    hs.surf_data.insert(hs.surf_data.end(), e.bcoef.begin(), e.bcoef.end());
+                    hs.surf_data.insert(hs.surf_data.end(), e.vshot.begin(), e.vshot.end());
+                    r.data_n = e.vshot_rows;
+                    break;
+                case kSurfPoly:
+                    hs.surf_data.insert(hs.surf_data.end(), e.poly.begin(), e.poly.end());
+                    break;
+                case kSurfSpline:
+                    hs.surf_data.insert(hs.surf_data.end(), e.spl_x.begin(), e.spl_x.end());
+                    hs.surf_data.insert(hs.surf_data.end(), e.spl_y.begin(), e.spl_y.end());
+                    hs.surf_data.insert(hs.surf_data.end(), e.spl_y2.begin(), e.spl_y2.end());
+                    r.spl_n = int(e.spl_x.size());
+                    break;
+                default:
+                    break;
+            }
+            hs.elems.push_back(r);
+        }
+        if (st.elems.size() >= 16) {
+            sr.bvh_off = int(hs.bvh.size());
+            sr.bvh_items_off = int(hs.bvh_items.size());
+            build_bvh(st.elems, hs.bvh, hs.bvh_items);
+            // child indices are relative to the stage's first node
+        }
+    }
+    if (!sun_setup(cx, hs)) return false;
+    hs.dev.sunshape_on = cx->err_sun;
+    hs.dev.errors_on = cx->err_opt;
+    return true;
+}
+
+// reference record order: per stage sorted by (ray number, hit index), then the
+// block merge of TRayData::Merge (types.cpp:311-355)
+void assemble_records(Context *cx, RunResult &rr) {
+    const int nst = int(cx->stages.size());
+    std::vector<RecordDev> &recs = rr.records;
+    const uint32_t N = uint32_t(rr.ray_hits);
+    // the reference traces no later stage when the only ray carried out of the first
+    // stage is the last numbered one (raytrace.cpp:786-797 never marks it)
+    const bool drop_later = nst > 1 && rr.stage_entries.size() > 1 && rr.stage_entries[1] == 1 && rr.max_enter[1] == N;
+    std::vector<std::vector<RecordDev>> per(nst);
+    for (const RecordDev &r : recs) {
+        const int s = r.stage - 1;
+        if (s < 0 || s >= nst) continue;
+        if (drop_later && s >= 1) continue;
+        // the last ray of a trace-through stage that misses leaves no record (raytrace.cpp:810-811)
+        if (s >= 1 && cx->stages[s].tracethrough && r.element == 0 && rr.max_ttmiss[s] != 0 &&
+            rr.max_ttmiss[s] == rr.max_enter[s] && r.raynum == rr.max_enter[s])
+            continue;
+        per[s].push_back(r);
+    }
+    for (auto &v : per)
+        std::sort(v.begin(), v.end(), [](const RecordDev &a, const RecordDev &b) {
+            return a.raynum != b.raynum ? a.raynum < b.raynum : a.seq < b.seq;
+        });
+    const size_t B = 8192;
+    struct Blk {
+        int stage;
+        size_t off, n;  // contiguous piece of one stage
+        std::vector<std::pair<int, size_t>> pieces;  // (stage, start) of each record when mixed
+    };
+    // A block holds up to B records as a list of (stage, start, count) runs.
+    struct Run {
+        int s;
+        size_t start, n;
+    };
+    std::vector<std::vector<Run>> all;
+    auto blk_size = [](const std::vector<Run> &b) {
+        size_t t = 0;
+        for (auto &r : b) t += r.n;
+        return t;
+    };
+    for (int s = 0; s < nst; ++s) {
+        std::vector<std::vector<Run>> src;
+        for (size_t i = 0; i < per[s].size(); i += B) src.push_back({Run{s, i, std::min(B, per[s].size() - i)}});
+        std::vector<std::vector<Run>> full, partial;
+        for (auto &b : all) (blk_size(b) == B ? full : partial).push_back(b);
+        for (auto &b : src) (blk_size(b) == B ? full : partial).push_back(b);
+        all = full;
+        for (auto &b : partial)
+            for (const Run &r : b) {
+                size_t done = 0;
+                while (done < r.n) {
+                    if (all.empty() || blk_size(all.back()) == B) all.push_back({});
+                    const size_t room = B - blk_size(all.back());
+                    const size_t k = std::min(room, r.n - done);
+                    all.back().push_back(Run{r.s, r.start + done, k});
+                    done += k;
+                }
+            }
+    }
+    cx->records.clear();
+    size_t total = 0;
+    for (auto &v : per) total += v.size();
+    cx->records.reserve(total);
+    for (auto &b : all)
+        for (const Run &r : b) cx->records.insert(cx->records.end(), per[r.s].begin() + r.start, per[r.s].begin() + r.start + r.n);
+    recs.clear();
+    recs.shrink_to_fit();
+}
+
+int run(Context *cx, unsigned seed) {
+    cx->records.clear();
+    memset(&cx->stats, 0, sizeof cx->stats);
+    if (cx->ex_pos.empty() && cx->raycount < 1) {
+        cx->log("invalid number of rays: %d", cx->raycount);
+        return -1;
+    }
+    if (cx->stages.empty()) {
+        cx->log("no stages defined.");
+        return -1;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    if (!init_geometries(cx)) return -1;
+    HostScene hs;
+    if (!flatten(cx, hs)) return -1;
+    RunRequest rq;
+    rq.n_hits = uint64_t(cx->raycount);
+    rq.max_sun = uint64_t(std::max(cx->raymax, 0));
+    rq.seed = seed;
+    rq.precision = cx->precision;
+    rq.records = cx->want_records;
+    rq.device = cx->device;
+    rq.ex_pos = cx->ex_pos;
+    rq.ex_cos = cx->ex_cos;
+    for (auto &f : cx->flux) rq.flux.push_back(f.req);
+    rq.callback = cx->cb;
+    rq.cbdata = cx->cbdata;
+    rq.hit_rate_hint = cx->last_hit_rate;
+    RunResult rr;
+    const double host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    const bool ok = gpu_run(hs, rq, rr);
+    if (!ok) {
+        cx->log("%s", rr.error.c_str());
+        return -1;
+    }
+    cx->sun_rays = rr.sun_rays;
+    if (rr.sun_rays > 0 && cx->ex_pos.empty()) cx->last_hit_rate = double(rr.ray_hits) / double(rr.sun_rays);
+    const int nst = int(cx->stages.size());
+    const uint32_t N = uint32_t(rr.ray_hits);
+    const bool drop_later = nst > 1 && rr.stage_entries[1] == 1 && rr.max_enter[1] == N;
+    // flux maps and per-element counts
+    for (size_t m = 0; m < cx->flux.size(); ++m) {
+        cx->flux[m].counts = rr.flux[m];
+        if (drop_later && cx->flux[m].req.stage >= 1) std::fill(cx->flux[m].counts.begin(), cx->flux[m].counts.end(), 0ull);
+    }
+    cx->elem_first.assign(nst, {});
+    cx->elem_absorbed.assign(nst, {});
+    cx->elem_delivered.assign(nst, {});
+    for (int s = 0; s < nst; ++s) {
+        const int f = hs.dev.stages[s].first_elem, n = hs.dev.stages[s].n_elem;
+        cx->elem_first[s].assign(rr.first_hits.begin() + f, rr.first_hits.begin() + f + n);
+        cx->elem_absorbed[s].assign(rr.absorbed.begin() + f, rr.absorbed.begin() + f + n);
+        cx->elem_delivered[s].assign(rr.delivered.begin() + f, rr.delivered.begin() + f + n);
+        if (drop_later && s >= 1) {
+            std::fill(cx->elem_first[s].begin(), cx->elem_first[s].end(), 0ull);
+            std::fill(cx->elem_absorbed[s].begin(), cx->elem_absorbed[s].end(), 0ull);
+        }
+    }
+    if (drop_later) std::fill(cx->elem_delivered[0].begin(), cx->elem_delivered[0].end(), 0ull);
+    st_b200_stats &S = cx->stats;
+    S.sun_rays = rr.sun_rays;
+    S.ray_hits = rr.ray_hits;
+    S.ray_stage_units = rr.sun_rays;
+    for (int s = 0; s < nst && s < 16; ++s) {
+        S.stage_entries[s] = (drop_later && s >= 1) ? 0 : rr.stage_entries[s];
+        if (s >= 1) S.ray_stage_units += S.stage_entries[s];
+    }
+    S.probe_ms = rr.probe_ms;
+    S.trace_ms = rr.trace_ms;
+    S.kernel_ms = rr.device_ms;
+    S.setup_ms = rr.setup_ms + host_ms;
+    S.batches = rr.batches;
+    S.gpu_launches = rr.gpu_launches;
+    S.h2d_bytes = rr.h2d_bytes;
+    S.d2h_bytes = rr.d2h_bytes;
+    if (rr.flags & 1u) cx->log("warning: a ray reached the limit of intersections per stage; it was stopped there");
+    const auto ta = std::chrono::steady_clock::now();
+    if (cx->want_records) assemble_records(cx, rr);
+    S.readback_ms = rr.readback_ms + std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
+    S.records = cx->records.size();
+    return int(cx->records.size());
+}
+
+Context *C(st_context_t p) { return reinterpret_cast<Context *>(p); }
+StageM *stage_of(Context *cx, st_uint_t i) { return i < cx->stages.size() ? &cx->stages[i] : nullptr; }
+Elem *elem_of(Context *cx, st_uint_t s, st_uint_t i) {
+    StageM *st = stage_of(cx, s);
+    return (st && i < st->elems.size()) ? &st->elems[i] : nullptr;
+}
+
+bool read_surface_file(Context *cx, Elem &e, const char *file) {  // input.cpp:368-573
+    const char *dot = strrchr(file, '.');
+    if (!dot) {
+        cx->log("Could not determine surface file type: '%s'\n", file);
+        return false;
+    }
+    std::string ext(dot + 1);
+    for (auto &c : ext) c = char(tolower(c));
+    FILE *fp = fopen(file, "r");
+    if (!fp) {
+        cx->log("Could not open surface file for read: %s\n", file);
+        return false;
+    }
+    char line[1024];
+    auto rd = [&]() {
+        if (!fgets(line, sizeof line, fp)) line[0] = 0;
+    };
+    bool ok = true;
+    if (ext == "mon") {
+        rd();
+        const int order = atoi(line);
+        e.bcoef.assign(size_t(order + 1) * (order + 1), 0.0);
+        for (int k = 0; k <= order; ++k)
+            for (int m = 0; m <= k; ++m) {
+                rd();
+                e.bcoef[size_t(k) * (order + 1) + m] = atof(line);
+            }
+        e.fit_order = order;
+        e.surface = 'm';
+        e.stype = 6;
+    } else if (ext == "sht") {
+        rd();
+        rd();
+        rd();
+        int idum = 0, order = 0, np = 0;
+        sscanf(line, "%d %d %d", &idum, &order, &np);
+        rd();
+        e.fit_order = order;
+        e.bcoef.assign(size_t(order + 1) * (order + 1), 0.0);
+        for (int k = 0; k <= order; ++k)
+            for (int m = 0; m <= k; ++m) {
+                rd();
+                e.bcoef[size_t(k) * (order + 1) + m] = atof(line);
+            }
+        e.vshot.assign(size_t(5) * np, 0.0);
+        e.vshot_rows = np;
+        for (int k = 0; k < np; ++k) {
+            rd();
+            double *v = &e.vshot[size_t(5) * k];
+            sscanf(line, "%lg %lg %lg %lg %lg", v, v + 1, v + 2, v + 3, v + 4);
+        }
+        e.surface = 'v';
+        e.stype = 5;
+    } else if (ext == "ply") {
+        rd();
+        const int order = atoi(line);
+        e.poly.assign(size_t(order + 1), 0.0);
+        for (int k = 0; k <= order; ++k) {
+            rd();
+            e.poly[k] = atof(line);
+        }
+        e.fit_order = order;
+        e.surface = 'r';
+        e.stype = 8;
+    } else if (ext == "csi") {
+        rd();
+        const int np = atoi(line);
+        e.spl_x.assign(np, 0.0);
+        e.spl_y.assign(np, 0.0);
+        for (int k = 0; k < np; ++k) {
+            rd();
+            sscanf(line, "%lg %lg", &e.spl_x[k], &e.spl_y[k]);
+        }
+        double a = 0, b = 0;
+        rd();
+        sscanf(line, "%lg %lg", &a, &b);
+        spline_y2(e.spl_x, e.spl_y, a, b, e.spl_y2);
+        if (np < 2 || (e.shape != 'a' && e.shape != 'A' && e.shape != 'l' && e.shape != 'L') || e.p[0] < e.spl_x[0] ||
+            e.p[1] > e.spl_x.back()) {
+            cx->log("Error: Element uses cubic spline interpolation:"
+                    "\tMake sure aperture is type 'a' or 'l' and that "
+                    "1st and 2nd parameters are not < and not > the "
+                    "1st and last X values in file respectively.\n");
+            ok = false;
+        } else {
+            e.surface = 'i';
+            e.stype = 9;
+        }
+    } else if (ext == "fed") {
+        // accepted so that scenes load; st_sim_run reports that this surface is not traced
+        rd();
+        rd();
+        const int np = atoi(line);
+        e.vshot.assign(size_t(3) * std::max(np, 0), 0.0);
+        for (int k = 0; k < np; ++k) {
+            rd();
+            sscanf(line, "%lg %lg %lg", &e.vshot[3 * k], &e.vshot[3 * k + 1], &e.vshot[3 * k + 2]);
+        }
+        e.fe_surface = true;
+        e.surface = 'e';
+        e.stype = 4;
+    } else {
+        cx->log("Surface file type extension unknown: '%s'\n", ext.c_str());
+        ok = false;
+    }
+    fclose(fp);
+    return ok;
+}
+
+}  // namespace
+
+// ======================================================================================
+// C API
+// ======================================================================================
+#define CTX(p, r)        \
+    Context *cx = C(p);  \
+    if (!cx) return r;
+
+extern "C" {
+
+st_context_t st_create_context(void) { return new Context; }
+int st_free_context(st_context_t p) {
+    CTX(p, -1);
+    delete cx;
+    return 1;
+}
+int st_num_messages(st_context_t p) {
+    CTX(p, -1);
+    return int(cx->messages.size());
+}
+const char *st_message(st_context_t p, st_uint_t i) {
+    CTX(p, nullptr);
+    return i < cx->messages.size() ? cx->messages[i].c_str() : nullptr;
+}
+void st_clear_messages(st_context_t p) {
+    if (C(p)) C(p)->messages.clear();
+}
+int st_num_optics(st_context_t p) {
+    CTX(p, -1);
+    return int(cx->optics.size());
+}
+int st_add_optic(st_context_t p, const char *name) {
+    CTX(p, -1);
+    cx->optics.push_back(OpticSet());
+    cx->optics.back().name = name ? name : "";
+    return int(cx->optics.size()) - 1;
+}
+int st_delete_optic(st_context_t p, st_uint_t i) {
+    CTX(p, -1);
+    if (i >= cx->optics.size()) return -1;
+    cx->optics.erase(cx->optics.begin() + i);
+    return 1;
+}
+int st_clear_optics(st_context_t p) {
+    CTX(p, -1);
+    cx->optics.clear();
+    return 1;
+}
+int st_optic(st_context_t p, st_uint_t idx, int fb, char dist, int optnum, int apgr, int order, double rreal,
+             double rimag, double ref, double tra, double gratingab12[3], double rmsslope, double rmsspec,
+             int userefltable, int refl_npoints, double *refl_angles, double *refls, int usetranstable,
+             int trans_npoints, double *trans_angles, double *transs) {
+    CTX(p, -1);
+    if (idx >= cx->optics.size()) return -1;
+    Face &f = (fb == 2) ? cx->optics[idx].back : cx->optics[idx].front;
+    f.dist = dist;
+    f.optnum = optnum;
+    f.apgr = apgr;
+    f.order = order;
+    f.n[0] = rreal;
+    f.n[1] = rimag;
+    f.refl = ref;
+    f.trans = tra;
+    // the reference reads four grating coefficients (stapi.cpp:188-189)
+    if (gratingab12)
+        for (int i = 0; i < 4; ++i) f.ab12[i] = gratingab12[i];
+    f.slope = rmsslope;
+    f.spec = rmsspec;
+    if (userefltable && refl_npoints > 0 && refl_angles && refls) {
+        f.use_refl = true;
+        f.refl_tab.clear();
+        for (int i = 0; i < refl_npoints; ++i) {
+            f.refl_tab.push_back(refl_angles[i]);
+            f.refl_tab.push_back(refls[i]);
+        }
+    }
+    if (usetranstable && trans_npoints > 0 && trans_angles && transs) {
+        f.use_trans = true;
+        f.trans_tab.clear();
+        for (int i = 0; i < trans_npoints; ++i) {
+            f.trans_tab.push_back(trans_angles[i]);
+            f.trans_tab.push_back(transs[i]);
+        }
+    }
+    return 1;
+}
+int st_num_stages(st_context_t p) {
+    CTX(p, -1);
+    return int(cx->stages.size());
+}
+int st_add_stage(st_context_t p) {
+    CTX(p, -1);
+    cx->stages.push_back(StageM());
+    return int(cx->stages.size()) - 1;
+}
+int st_add_stages(st_context_t p, st_uint_t n) {
+    CTX(p, -1);
+    for (st_uint_t i = 0; i < n; ++i) cx->stages.push_back(StageM());
+    return int(n);
+}
+int st_delete_stage(st_context_t p, st_uint_t i) {
+    CTX(p, -1);
+    if (i >= cx->stages.size()) return -1;
+    cx->stages.erase(cx->stages.begin() + i);
+    return 1;
+}
+int st_clear_stages(st_context_t p) {
+    CTX(p, -1);
+    cx->stages.clear();
+    return 1;
+}
+#define STAGE_SET(body)                     \
+    CTX(p, -1);                             \
+    StageM *st = stage_of(cx, i);           \
+    if (!st) return -1;                     \
+    body;                                   \
+    return 1;
+int st_stage_xyz(st_context_t p, st_uint_t i, double x, double y, double z) {
+    STAGE_SET(st->origin[0] = x; st->origin[1] = y; st->origin[2] = z)
+}
+int st_stage_aim(st_context_t p, st_uint_t i, double x, double y, double z) {
+    STAGE_SET(st->aim[0] = x; st->aim[1] = y; st->aim[2] = z)
+}
+int st_stage_zrot(st_context_t p, st_uint_t i, double z) { STAGE_SET(st->zrot = z) }
+int st_stage_flags(st_context_t p, st_uint_t i, int virt, int multihit, int tracethrough) {
+    STAGE_SET(st->virt = virt != 0; st->multihit = multihit != 0; st->tracethrough = tracethrough != 0)
+}
+int st_num_elements(st_context_t p, st_uint_t s) {
+    CTX(p, -1);
+    StageM *st = stage_of(cx, s);
+    return st ? int(st->elems.size()) : -1;
+}
+int st_add_element(st_context_t p, st_uint_t s) {
+    CTX(p, -1);
+    StageM *st = stage_of(cx, s);
+    if (!st) return -1;
+    st->elems.push_back(Elem());
+    return int(st->elems.size()) - 1;
+}
+int st_add_elements(st_context_t p, st_uint_t s, st_uint_t n) {
+    CTX(p, -1);
+    if (n < 1) return -1;
+    StageM *st = stage_of(cx, s);
+    if (!st) return -1;
+    st->elems.resize(st->elems.size() + n);
+    return int(n);
+}
+int st_delete_element(st_context_t p, st_uint_t s, st_uint_t i) {
+    CTX(p, -1);
+    StageM *st = stage_of(cx, s);
+    if (!st || i >= st->elems.size()) return -1;
+    st->elems.erase(st->elems.begin() + i);
+    return 1;
+}
+int st_clear_elements(st_context_t p, st_uint_t s) {
+    CTX(p, -1);
+    StageM *st = stage_of(cx, s);
+    if (!st) return -1;
+    st->elems.clear();
+    return 1;
+}
+#define ELEM_SET(body)                      \
+    CTX(p, -1);                             \
+    Elem *e = elem_of(cx, s, i);            \
+    if (!e) return -1;                      \
+    body;                                   \
+    return 1;
+int st_element_enabled(st_context_t p, st_uint_t s, st_uint_t i, int en) { ELEM_SET(e->enabled = en != 0) }
+int st_element_xyz(st_context_t p, st_uint_t s, st_uint_t i, double x, double y, double z) {
+    ELEM_SET(e->origin[0] = x; e->origin[1] = y; e->origin[2] = z)
+}
+int st_element_aim(st_context_t p, st_uint_t s, st_uint_t i, double x, double y, double z) {
+    ELEM_SET(e->aim[0] = x; e->aim[1] = y; e->aim[2] = z)
+}
+int st_element_zrot(st_context_t p, st_uint_t s, st_uint_t i, double z) { ELEM_SET(e->zrot = z) }
+int st_element_aperture(st_context_t p, st_uint_t s, st_uint_t i, char ap) { ELEM_SET(e->shape = ap) }
+int st_element_aperture_params(st_context_t p, st_uint_t s, st_uint_t i, double prm[8]) {
+    ELEM_SET(for (int k = 0; k < 8; ++k) e->p[k] = prm[k])
+}
+int st_element_surface(st_context_t p, st_uint_t s, st_uint_t i, char sf) { ELEM_SET(e->surface = sf) }
+int st_element_surface_params(st_context_t p, st_uint_t s, st_uint_t i, double prm[8]) {
+    CTX(p, -1);
+    Elem *e = elem_of(cx, s, i);
+    if (!e) return -1;
+    return translate_surface(cx, *e, prm) ? 1 : -1;
+}
+int st_element_surface_file(st_context_t p, st_uint_t s, st_uint_t i, const char *file) {
+    CTX(p, -1);
+    Elem *e = elem_of(cx, s, i);
+    if (!e || !file) return -1;
+    return read_surface_file(cx, *e, file) ? 1 : -1;
+}
+int st_element_interaction(st_context_t p, st_uint_t s, st_uint_t i, int t) { ELEM_SET(e->interaction = t) }
+int st_element_optic(st_context_t p, st_uint_t s, st_uint_t i, const char *name) {
+    ELEM_SET(e->optic = name ? name : "")
+}
+int st_sun(st_context_t p, int ps, char shape, double sigma) {
+    CTX(p, -1);
+    cx->sun.point_source = ps != 0;
+    cx->sun.shape = shape;
+    cx->sun.sigma = sigma;
+    return 1;
+}
+int st_sun_xyz(st_context_t p, double x, double y, double z) {
+    CTX(p, -1);
+    cx->sun.origin[0] = x;
+    cx->sun.origin[1] = y;
+    cx->sun.origin[2] = z;
+    return 1;
+}
+// solar position formula of stapi.cpp:485-527 (x west, y zenith, z north)
+int st_sun_position(st_context_t, double lat, double day, double hour, double *x, double *y, double *z) {
+    const double d2r = kPi / 180;
+    const double decl = 180 / kPi * asin(0.39795 * cos(0.98563 * kPi / 180 * (day - 173)));
+    const double ha = 15 * (hour - 12);
+    const double el = 180 / kPi * asin(sin(decl * d2r) * sin(lat * d2r) + cos(decl * d2r) * cos(ha * d2r) * cos(lat * d2r));
+    double az = 180 / kPi *
+                acos((sin(d2r * decl) * cos(d2r * lat) - cos(d2r * decl) * sin(d2r * lat) * cos(d2r * ha)) / cos(d2r * el) +
+                     0.0000000001);
+    if (sin(ha * d2r) > 0.0) az = 360 - az;
+    if (x) *x = -sin(az * d2r) * cos(el * d2r);
+    if (y) *y = sin(el * d2r);
+    if (z) *z = cos(az * d2r) * cos(el * d2r);
+    return 1;
+}
+int st_sun_userdata(st_context_t p, st_uint_t n, double angle[], double intensity[]) {
+    CTX(p, -1);
+    if (n <= 2) return -1;
+    SunM &s = cx->sun;
+    s.max_angle = 0;
+    s.max_intensity = 0;
+    s.ang.assign(2 * n - 1, 0.0);
+    s.inten.assign(2 * n - 1, 0.0);
+    for (st_uint_t i = 0; i < n; ++i) {
+        s.ang[n + i - 1] = angle[i];
+        s.inten[n + i - 1] = intensity[i];
+        s.max_angle = std::max(s.max_angle, angle[i]);
+        s.max_intensity = std::max(s.max_intensity, intensity[i]);
+    }
+    for (st_uint_t i = 0; i + 1 < n; ++i) {
+        s.ang[i] = -angle[n - i - 1];
+        s.inten[i] = intensity[n - i - 1];
+    }
+    return int(n);
+}
+int st_num_intersections(st_context_t p) {
+    CTX(p, -1);
+    return int(cx->records.size());
+}
+int st_locations(st_context_t p, double *x, double *y, double *z) {
+    CTX(p, -1);
+    for (size_t i = 0; i < cx->records.size(); ++i) {
+        x[i] = cx->records[i].pos[0];
+        y[i] = cx->records[i].pos[1];
+        z[i] = cx->records[i].pos[2];
+    }
+    return 1;
+}
+int st_cosines(st_context_t p, double *x, double *y, double *z) {
+    CTX(p, -1);
+    for (size_t i = 0; i < cx->records.size(); ++i) {
+        x[i] = cx->records[i].cos[0];
+        y[i] = cx->records[i].cos[1];
+        z[i] = cx->records[i].cos[2];
+    }
+    return 1;
+}
+int st_elementmap(st_context_t p, int *m) {
+    CTX(p, -1);
+    for (size_t i = 0; i < cx->records.size(); ++i) m[i] = cx->records[i].element;
+    return 1;
+}
+int st_stagemap(st_context_t p, int *m) {
+    CTX(p, -1);
+    for (size_t i = 0; i < cx->records.size(); ++i) m[i] = cx->records[i].stage;
+    return 1;
+}
+int st_raynumbers(st_context_t p, int *m) {
+    CTX(p, -1);
+    for (size_t i = 0; i < cx->records.size(); ++i) m[i] = int(cx->records[i].raynum);
+    return 1;
+}
+int st_sun_stats(st_context_t p, double *xmin, double *xmax, double *ymin, double *ymax, int *nsun) {
+    CTX(p, -1);
+    if (xmin) *xmin = cx->sun.xmin;
+    if (xmax) *xmax = cx->sun.xmax;
+    if (ymin) *ymin = cx->sun.ymin;
+    if (ymax) *ymax = cx->sun.ymax;
+    if (nsun) *nsun = int(cx->sun_rays);
+    return 1;
+}
+int st_sim_params(st_context_t p, int raycount, int maxcount, int dyn) {
+    CTX(p, -1);
+    cx->raycount = raycount;
+    cx->raymax = maxcount;
+    cx->dyn = dyn != 0;
+    return 1;
+}
+int st_sim_errors(st_context_t p, int sun, int opt) {
+    CTX(p, -1);
+    cx->err_sun = sun != 0;
+    cx->err_opt = opt != 0;
+    return 1;
+}
+int st_sim_run(st_context_t p, unsigned int seed,
+               int (*cb)(st_uint_t, st_uint_t, st_uint_t, st_uint_t, st_uint_t, void *), void *data) {
+    CTX(p, -1);
+    cx->cb = cb;
+    cx->cbdata = data;
+    return run(cx, seed);
+}
+
+// transform utilities (stapi.cpp:737-778)
+void st_calc_euler_angles(double origin[3], double aimpoint[3], double zrot, double euler[3]) {
+    euler[0] = euler[1] = euler[2] = 0;
+    euler_of(origin, aimpoint, zrot, euler);
+}
+void st_transform_to_local(double posref[3], double cosref[3], double origin[3], double R[3][3], double posloc[3],
+                           double cosloc[3]) {
+    const double d[3] = {posref[0] - origin[0], posref[1] - origin[1], posref[2] - origin[2]};
+    mulv(&R[0][0], d, posloc);
+    mulv(&R[0][0], cosref, cosloc);
+}
+void st_transform_to_reference(double posloc[3], double cosloc[3], double origin[3], double R[3][3], double posref[3],
+                               double cosref[3]) {
+    double d[3];
+    mulv(&R[0][0], posloc, d);
+    mulv(&R[0][0], cosloc, cosref);
+    for (int i = 0; i < 3; ++i) posref[i] = d[i] + origin[i];
+}
+void st_matrix_vector_mult(double m[3][3], double v[3], double mxv[3]) { mulv(&m[0][0], v, mxv); }
+void st_calc_transform_matrices(double euler[3], double rreftoloc[3][3], double rloctoref[3][3]) {
+    rot_from_euler(euler, &rreftoloc[0][0]);
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) rloctoref[i][j] = rreftoloc[j][i];
+}
+void st_matrix_transpose(double in[3][3], double out[3][3]) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) out[i][j] = in[j][i];
+}
+
+// ---------------- B200 extensions ----------------
+int st_b200_set_precision(st_context_t p, int mode) {
+    CTX(p, -1);
+    if (mode != ST_B200_FP64 && mode != ST_B200_MIXED) return -1;
+    cx->precision = mode;
+    return 1;
+}
+int st_b200_set_records(st_context_t p, int on) {
+    CTX(p, -1);
+    cx->want_records = on != 0;
+    return 1;
+}
+int st_b200_set_device(st_context_t p, int device) {
+    CTX(p, -1);
+    if (device < 0) return -1;
+    cx->device = device;
+    return 1;
+}
+int st_b200_explicit_rays(st_context_t p, st_uint_t n, const double *pos, const double *cos) {
+    CTX(p, -1);
+    if (n && (!pos || !cos)) return -1;
+    cx->ex_pos.assign(pos, pos + 3 * n);
+    cx->ex_cos.assign(cos, cos + 3 * n);
+    return int(n);
+}
+int st_b200_add_flux_map(st_context_t p, int stage, int element, int kind, int nx, int ny, double x0, double x1,
+                         double y0, double y1, int absorbed_only) {
+    CTX(p, -1);
+    if (cx->flux.size() >= size_t(kMaxFluxMaps) || nx <= 0 || ny <= 0 || stage < 1 || element < 1 || (kind != 0 && kind != 1)) {
+        cx->log("invalid flux map request");
+        return -1;
+    }
+    FluxMap m;
+    m.req = FluxMapReq{stage - 1, element - 1, kind, nx, ny, absorbed_only ? 1 : 0, x0, x1, y0, y1};
+    cx->flux.push_back(m);
+    return int(cx->flux.size()) - 1;
+}
+int st_b200_clear_flux_maps(st_context_t p) {
+    CTX(p, -1);
+    cx->flux.clear();
+    return 1;
+}
+int st_b200_flux_counts(st_context_t p, int map, unsigned long long *counts) {
+    CTX(p, -1);
+    if (map < 0 || size_t(map) >= cx->flux.size() || !counts) return -1;
+    const auto &c = cx->flux[map].counts;
+    const size_t n = size_t(cx->flux[map].req.nx) * cx->flux[map].req.ny;
+    for (size_t i = 0; i < n; ++i) counts[i] = i < c.size() ? c[i] : 0ull;
+    return 1;
+}
+int st_b200_run_stats(st_context_t p, st_b200_stats *out) {
+    CTX(p, -1);
+    if (!out) return -1;
+    *out = cx->stats;
+    return 1;
+}
+int st_b200_element_counts(st_context_t p, int stage, unsigned long long *first_hits, unsigned long long *absorbed,
+                           unsigned long long *delivered) {
+    CTX(p, -1);
+    if (stage < 1 || size_t(stage) > cx->elem_first.size()) return -1;
+    const size_t s = size_t(stage - 1);
+    for (size_t i = 0; i < cx->elem_first[s].size(); ++i) {
+        if (first_hits) first_hits[i] = cx->elem_first[s][i];
+        if (absorbed) absorbed[i] = cx->elem_absorbed[s][i];
+        if (delivered) delivered[i] = cx->elem_delivered[s][i];
+    }
+    return 1;
+}
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+// Host-side interface between the scene/context code (st_host.cpp, plain C++)
+// and the CUDA run driver (st_run.cu).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "st_scene.h"
+
+namespace stb {
+
+// Flattened scene in host memory; gpu_run() uploads it once per run.
+struct HostScene {
+    std::vector<ElemRec> elems;
+    std::vector<OpticRec> optics;
+    std::vector<double> surf_data, tables;
+    std::vector<BvhNode> bvh;
+    std::vector<int> bvh_items;
+    std::vector<int> cell_start, cell_items;
+    std::vector<double> cdf_theta, cdf;
+    SceneDev dev;  // stages, sun scalars and flags; device pointers are filled by gpu_run
+};
+
+struct FluxMapReq {
+    int stage, elem, kind, nx, ny, absorbed_only;
+    double x0, x1, y0, y1;
+};
+
+struct RunRequest {
+    uint64_t n_hits = 0;      // rays to number (first-stage hits); explicit mode: ignored
+    uint64_t max_sun = 0;     // sun-ray cap (st_sim_params maxcount)
+    uint32_t seed = 0;
+    int precision = 0;
+    bool records = true;
+    int device = 0;
+    std::vector<double> ex_pos, ex_cos;  // explicit rays (global frame)
+    std::vector<FluxMapReq> flux;
+    int (*callback)(unsigned long, unsigned long, unsigned long, unsigned long, unsigned long, void *) = nullptr;
+    void *cbdata = nullptr;
+    double hit_rate_hint = 0.0;  // expected first-stage hits per sun ray (0 = measure with a pilot batch)
+};
+
+struct RunResult {
+    bool ok = false;
+    bool cancelled = false;
+    std::string error;
+    uint64_t sun_rays = 0, ray_hits = 0;
+    std::vector<RecordDev> records;  // unordered, as produced by the device
+    std::vector<uint64_t> stage_entries;
+    std::vector<uint32_t> max_enter, max_ttmiss;
+    std::vector<std::vector<unsigned long long>> flux;
+    std::vector<unsigned long long> first_hits, absorbed, delivered;
+    double device_ms = 0;  // first launch to last completion, CUDA events on the run's stream
+    double probe_ms = 0, trace_ms = 0, setup_ms = 0, readback_ms = 0;
+    int batches = 0, gpu_launches = 0;
+    unsigned flags = 0;
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;
+};
+
+bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out);
+
+}  // namespace stb

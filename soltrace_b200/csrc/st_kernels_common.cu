@@ -1,0 +1,19 @@
+// Precision-independent kernels: ordered compaction of the probe's hits.
+#define ST_COMMON_KERNELS
+#include "st_launch.h"
+#include "st_trace_impl.cuh"
+
+namespace stb {
+void launch_offsets(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_t *total, cudaStream_t st) {
+    k_offsets<<<1, 1024, 0, st>>>(counts, nb, offsets, total);
+}
+void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uint32_t *counts,
+                    const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st) {
+    const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;
+    k_compact<<<nb, kProbeBlock, 0, st>>>(s0, n, hit_elem, counts, offsets, hit_sid, hit_el);
+}
+void launch_advance(const uint32_t *total, const uint64_t *hit_sid, uint64_t s0, uint32_t n, RunState *rs,
+                    cudaStream_t st) {
+    k_advance<<<1, 1, 0, st>>>(total, hit_sid, s0, n, rs);
+}
+}  // namespace stb

@@ -1,0 +1,66 @@
+// Kernel launchers of the B200 trace (defined in st_kernels_fp64.cu,
+// st_kernels_mixed.cu and st_kernels_common.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "st_scene.h"
+
+namespace stb {
+
+constexpr int kProbeBlock = 256;
+constexpr int kTraceBlock = 128;
+
+enum RunFlags : unsigned {
+    kFlagHitCap = 1u,         // a ray reached kMaxHitsPerStage in one stage
+    kFlagBadInteraction = 2u, // interaction type other than 1 or 2 (raytrace.cpp:943-946)
+    kFlagRecordOverflow = 4u,
+};
+
+struct RunCounters {
+    unsigned long long stage_entries[kMaxStages];
+    unsigned int max_enter[kMaxStages];   // largest ray number entering stage i
+    unsigned int max_ttmiss[kMaxStages];  // largest ray number missing trace-through stage i
+    unsigned long long records;
+    unsigned int flags;
+    unsigned int pad_;
+};
+
+// Device-side progress of a run: the ray-number cut-off at the requested hit
+// count is applied on the device, so batches can be queued without host syncs.
+struct RunState {
+    unsigned long long hits_done;  // rays numbered so far
+    unsigned long long target;     // rays to number (~0 in explicit-ray mode)
+    unsigned long long sun_rays;   // SunRayCount so far (final once reached)
+    unsigned int reached;
+    unsigned int pad_;
+};
+
+struct TraceOut {
+    RecordDev *recs;
+    unsigned long long rec_cap;
+    unsigned long long *rec_count;   // records written by this batch (slots beyond rec_cap dropped)
+    RunCounters *ctr;
+    unsigned long long *first_hits;  // per global element index
+    unsigned long long *absorbed;
+    unsigned long long *delivered;   // per global element index (first-stage elements)
+};
+
+
+void launch_probe_fp64(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
+                       const RunState *rs, cudaStream_t st);
+void launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
+                        const RunState *rs, cudaStream_t st);
+// grid-stride trace over min(*total, target - hits_done) numbered rays; `blocks`
+// is the grid size (0 = enough blocks for `max_n` rays)
+void launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
+                       const uint32_t *total, const RunState *rs, const TraceOut &O, uint32_t blocks, cudaStream_t st);
+void launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
+                        const uint32_t *total, const RunState *rs, const TraceOut &O, uint32_t blocks, cudaStream_t st);
+void launch_offsets(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_t *total, cudaStream_t st);
+void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uint32_t *counts,
+                    const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st);
+void launch_advance(const uint32_t *total, const uint64_t *hit_sid, uint64_t s0, uint32_t n, RunState *rs,
+                    cudaStream_t st);
+int trace_blocks_per_sm_fp64(bool records);
+int trace_blocks_per_sm_mixed(bool records);
+}  // namespace stb

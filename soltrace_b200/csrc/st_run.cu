@@ -1,0 +1,367 @@
+// Run driver: uploads the flattened scene, loops sun-ray batches through the
+// probe / compact / trace kernels until the requested number of first-stage hits
+// is numbered, and brings counters, flux maps and records back to the host.
+//
+// Semantics kept from the reference (coretrace/raytrace.cpp:582-604, 780-798):
+// ray numbers go to first-stage hits in sun-ray order; the run stops at the
+// hit numbered `raycount`, and SunRayCount is the number of sun rays generated
+// up to and including that ray; running out of `maxcount` sun rays first is an
+// error.  Because every ray has its own Philox stream keyed by its sun index,
+// batch boundaries do not change any result.
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+
+#include "st_host.h"
+#include "st_launch.h"
+
+namespace stb {
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t ensure(size_t b) {
+        if (b <= bytes && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&p, b ? b : 16);
+        if (e == cudaSuccess) bytes = b;
+        return e;
+    }
+    template <typename T>
+    T *as() const {
+        return static_cast<T *>(p);
+    }
+};
+
+template <typename T>
+cudaError_t upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s, uint64_t &bytes) {
+    cudaError_t e = b.ensure(std::max<size_t>(v.size() * sizeof(T), 16));
+    if (e != cudaSuccess || v.empty()) return e;
+    bytes += v.size() * sizeof(T);
+    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+double ms_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+#define CK(x)                                                                                 \
+    do {                                                                                      \
+        cudaError_t e_ = (x);                                                                 \
+        if (e_ != cudaSuccess) {                                                              \
+            out.error = std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #x;     \
+            return false;                                                                     \
+        }                                                                                     \
+    } while (0)
+
+bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out) {
+    const auto t_setup = std::chrono::steady_clock::now();
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        out.error = "no CUDA device is available to the B200 trace";
+        return false;
+    }
+    if (rq.device < 0 || rq.device >= ndev) {
+        out.error = "CUDA device ordinal out of range";
+        return false;
+    }
+    CK(cudaSetDevice(rq.device));
+    cudaStream_t st;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    struct StreamGuard {
+        cudaStream_t s;
+        ~StreamGuard() { cudaStreamDestroy(s); }
+    } sg{st};
+
+    DevBuf d_elems, d_optics, d_surf, d_tables, d_bvh, d_bvh_items, d_cell_start, d_cell_items, d_cdf_t, d_cdf, d_expos,
+        d_excos;
+    CK(upload(d_elems, hs.elems, st, out.h2d_bytes));
+    CK(upload(d_optics, hs.optics, st, out.h2d_bytes));
+    CK(upload(d_surf, hs.surf_data, st, out.h2d_bytes));
+    CK(upload(d_tables, hs.tables, st, out.h2d_bytes));
+    CK(upload(d_bvh, hs.bvh, st, out.h2d_bytes));
+    CK(upload(d_bvh_items, hs.bvh_items, st, out.h2d_bytes));
+    CK(upload(d_cell_start, hs.cell_start, st, out.h2d_bytes));
+    CK(upload(d_cell_items, hs.cell_items, st, out.h2d_bytes));
+    CK(upload(d_cdf_t, hs.cdf_theta, st, out.h2d_bytes));
+    CK(upload(d_cdf, hs.cdf, st, out.h2d_bytes));
+    CK(upload(d_expos, rq.ex_pos, st, out.h2d_bytes));
+    CK(upload(d_excos, rq.ex_cos, st, out.h2d_bytes));
+
+    SceneDev S = hs.dev;
+    S.elems = d_elems.as<ElemRec>();
+    S.optics = d_optics.as<OpticRec>();
+    S.surf_data = d_surf.as<double>();
+    S.tables = d_tables.as<double>();
+    S.bvh = d_bvh.as<BvhNode>();
+    S.bvh_items = d_bvh_items.as<int>();
+    S.sun.cell_start = d_cell_start.as<int>();
+    S.sun.cell_items = d_cell_items.as<int>();
+    S.sun.cdf_theta = hs.cdf_theta.empty() ? nullptr : d_cdf_t.as<double>();
+    S.sun.cdf = hs.cdf.empty() ? nullptr : d_cdf.as<double>();
+    S.seed = rq.seed;
+    S.precision = rq.precision;
+    const bool explicit_mode = !rq.ex_pos.empty();
+    const uint64_t n_explicit = rq.ex_pos.size() / 3;
+    S.explicit_rays = explicit_mode ? 1 : 0;
+    S.ex_pos = d_expos.as<double>();
+    S.ex_cos = d_excos.as<double>();
+
+    // run-level accumulators: [first_hits | absorbed | delivered | flux bins of every map]
+    const size_t ne = hs.elems.size();
+    std::vector<size_t> flux_off;
+    size_t acc_n = 3 * ne;
+    for (const auto &f : rq.flux) {
+        flux_off.push_back(acc_n);
+        acc_n += size_t(f.nx) * f.ny;
+    }
+    if (rq.flux.size() > size_t(kMaxFluxMaps)) {
+        out.error = "too many flux maps";
+        return false;
+    }
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, rq.device);
+    const int per_sm = rq.precision ? trace_blocks_per_sm_mixed(rq.records) : trace_blocks_per_sm_fp64(rq.records);
+    const uint32_t trace_grid = uint32_t(dev_sms * per_sm);
+
+    const int nst = S.n_stages;
+    const uint64_t kMaxBatch = uint64_t(1) << 25;
+    DevBuf d_acc, d_ctr, d_rs, d_rec_count, d_hit_elem, d_counts, d_offsets, d_total, d_hit_sid, d_hit_el, d_recs;
+    unsigned long long rec_cap = 0;
+    CK(cudaStreamSynchronize(st));
+    out.setup_ms = ms_since(t_setup);
+
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        bool restart = false;
+        out.records.clear();
+        out.stage_entries.assign(nst, 0);
+        out.max_enter.assign(nst, 0);
+        out.max_ttmiss.assign(nst, 0);
+        out.batches = 0;
+        out.probe_ms = out.trace_ms = 0;
+        CK(d_acc.ensure(std::max<size_t>(acc_n, 1) * 8));
+        CK(d_ctr.ensure(sizeof(RunCounters)));
+        CK(d_rs.ensure(sizeof(RunState)));
+        CK(d_rec_count.ensure(8));
+        CK(cudaMemsetAsync(d_acc.p, 0, std::max<size_t>(acc_n, 1) * 8, st));
+        CK(cudaMemsetAsync(d_ctr.p, 0, sizeof(RunCounters), st));
+        RunState rs0;
+        memset(&rs0, 0, sizeof rs0);
+        rs0.target = explicit_mode ? ~0ull : rq.n_hits;
+        CK(cudaMemcpyAsync(d_rs.p, &rs0, sizeof rs0, cudaMemcpyHostToDevice, st));
+        out.h2d_bytes += sizeof rs0;
+        unsigned long long *acc = d_acc.as<unsigned long long>();
+        S.n_flux = int(rq.flux.size());
+        for (size_t m = 0; m < rq.flux.size(); ++m) {
+            const FluxMapReq &f = rq.flux[m];
+            FluxMapDev &fd = S.flux[m];
+            fd.stage = f.stage;
+            fd.elem = f.elem;
+            fd.kind = f.kind;
+            fd.nx = f.nx;
+            fd.ny = f.ny;
+            fd.absorbed_only = f.absorbed_only;
+            fd.x0 = f.x0;
+            fd.x1 = f.x1;
+            fd.y0 = f.y0;
+            fd.y1 = f.y1;
+            fd.bins = acc + flux_off[m];
+        }
+        TraceOut O;
+        O.ctr = d_ctr.as<RunCounters>();
+        O.first_hits = acc;
+        O.absorbed = acc + ne;
+        O.delivered = acc + 2 * ne;
+        O.rec_count = d_rec_count.as<unsigned long long>();
+        RunState *drs = d_rs.as<RunState>();
+
+        // Batches are queued without host round trips unless records are kept (each
+        // batch's records are copied out) or a progress callback is installed.
+        const bool sync_each = rq.records || rq.callback != nullptr;
+        uint64_t sun_next = 0;
+        double p_est = rq.hit_rate_hint > 0 ? rq.hit_rate_hint : 0.0;
+        RunState rs = rs0;
+        std::vector<cudaEvent_t> evs;
+        struct EvList {
+            std::vector<cudaEvent_t> &v;
+            ~EvList() {
+                for (auto e : v) cudaEventDestroy(e);
+            }
+        } evl{evs};
+        auto new_event = [&]() {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            evs.push_back(e);
+            return e;
+        };
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> probe_ev, trace_ev;
+        cudaEvent_t t_first = new_event(), t_last = new_event();
+        CK(cudaEventRecord(t_first, st));
+        bool done = false;
+        while (!done) {
+            // plan the next group of batches
+            uint64_t want;
+            if (explicit_mode) {
+                want = n_explicit - sun_next;
+            } else {
+                const uint64_t need = rq.n_hits - rs.hits_done;
+                if (p_est <= 0.0)
+                    want = std::min<uint64_t>(uint64_t(1) << 20, rq.max_sun - sun_next);  // pilot batch
+                else
+                    want = uint64_t(1.03 * double(need) / p_est) + 65536;
+                want = std::min<uint64_t>(want, rq.max_sun - sun_next);
+            }
+            if (want == 0) {
+                if (explicit_mode) break;
+                char buf[160];
+                snprintf(buf, sizeof buf, "generated sun rays reached maximum count: %llu",
+                         (unsigned long long)rq.max_sun);
+                out.error = buf;
+                return false;
+            }
+            uint64_t queued = 0;
+            while (queued < want) {
+                const uint64_t n = std::min<uint64_t>(kMaxBatch, want - queued);
+                const uint32_t nb = uint32_t((n + kProbeBlock - 1) / kProbeBlock);
+                CK(d_hit_elem.ensure(n * 4));
+                CK(d_counts.ensure(size_t(nb) * 4));
+                CK(d_offsets.ensure(size_t(nb) * 4));
+                CK(d_total.ensure(8));
+                CK(d_hit_sid.ensure(n * 8));
+                CK(d_hit_el.ensure(n * 4));
+                if (rq.records) {
+                    if (rec_cap == 0) rec_cap = std::min<uint64_t>(n, uint64_t(1) << 22) * uint64_t(nst) * 2 + 4096;
+                    CK(d_recs.ensure(rec_cap * sizeof(RecordDev)));
+                    CK(cudaMemsetAsync(d_rec_count.p, 0, 8, st));
+                }
+                O.recs = rq.records ? d_recs.as<RecordDev>() : nullptr;
+                O.rec_cap = rq.records ? rec_cap : 0;
+                cudaEvent_t p0 = new_event(), p1 = new_event(), p2 = new_event();
+                CK(cudaEventRecord(p0, st));
+                if (rq.precision)
+                    launch_probe_mixed(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(), drs, st);
+                else
+                    launch_probe_fp64(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(), drs, st);
+                launch_offsets(d_counts.as<uint32_t>(), nb, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), st);
+                launch_compact(sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(),
+                               d_offsets.as<uint32_t>(), d_hit_sid.as<uint64_t>(), d_hit_el.as<uint32_t>(), st);
+                CK(cudaEventRecord(p1, st));
+                if (rq.precision)
+                    launch_trace_mixed(rq.records, S, d_hit_sid.as<uint64_t>(), d_hit_el.as<uint32_t>(),
+                                       d_total.as<uint32_t>(), drs, O, trace_grid, st);
+                else
+                    launch_trace_fp64(rq.records, S, d_hit_sid.as<uint64_t>(), d_hit_el.as<uint32_t>(),
+                                      d_total.as<uint32_t>(), drs, O, trace_grid, st);
+                CK(cudaEventRecord(p2, st));
+                launch_advance(d_total.as<uint32_t>(), d_hit_sid.as<uint64_t>(), sun_next, uint32_t(n), drs, st);
+                CK(cudaGetLastError());
+                out.gpu_launches += 5;
+                probe_ev.push_back({p0, p1});
+                trace_ev.push_back({p1, p2});
+                queued += n;
+                sun_next += n;
+                out.batches++;
+                if (sync_each) {
+                    CK(cudaMemcpyAsync(&rs, drs, sizeof rs, cudaMemcpyDeviceToHost, st));
+                    out.d2h_bytes += sizeof rs;
+                    unsigned long long nrec = 0;
+                    if (rq.records) CK(cudaMemcpyAsync(&nrec, d_rec_count.p, 8, cudaMemcpyDeviceToHost, st));
+                    CK(cudaStreamSynchronize(st));
+                    if (rq.records && nrec > rec_cap) {
+                        rec_cap = nrec + nrec / 4 + 4096;  // re-run the whole job with room for it
+                        restart = true;
+                        break;
+                    }
+                    if (nrec) {
+                        const auto tr = std::chrono::steady_clock::now();
+                        const size_t old = out.records.size();
+                        out.records.resize(old + nrec);
+                        out.d2h_bytes += nrec * sizeof(RecordDev);
+                        CK(cudaMemcpyAsync(out.records.data() + old, d_recs.p, nrec * sizeof(RecordDev),
+                                           cudaMemcpyDeviceToHost, st));
+                        CK(cudaStreamSynchronize(st));
+                        out.readback_ms += ms_since(tr);
+                    }
+                    if (rq.callback &&
+                        !rq.callback((unsigned long)rs.sun_rays, (unsigned long)rs.hits_done,
+                                     (unsigned long)(explicit_mode ? n_explicit : rq.n_hits), 1ul, (unsigned long)nst,
+                                     rq.cbdata)) {
+                        out.cancelled = true;
+                        done = true;
+                        break;
+                    }
+                    if (rs.reached) break;
+                }
+            }
+            if (restart) break;
+            CK(cudaMemcpyAsync(&rs, drs, sizeof rs, cudaMemcpyDeviceToHost, st));
+            out.d2h_bytes += sizeof rs;
+            CK(cudaStreamSynchronize(st));
+            if (rs.reached || out.cancelled || (explicit_mode && sun_next >= n_explicit)) done = true;
+            if (!explicit_mode && sun_next > 0) p_est = std::max(double(rs.hits_done) / double(sun_next), 1e-9);
+        }
+        if (restart) continue;
+        CK(cudaEventRecord(t_last, st));
+        CK(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, t_first, t_last);
+        out.device_ms = ms;
+        for (auto &pe : probe_ev) {
+            float x = 0;
+            cudaEventElapsedTime(&x, pe.first, pe.second);
+            out.probe_ms += x;
+        }
+        for (auto &pe : trace_ev) {
+            float x = 0;
+            cudaEventElapsedTime(&x, pe.first, pe.second);
+            out.trace_ms += x;
+        }
+        out.ray_hits = rs.hits_done;
+        out.sun_rays = explicit_mode ? n_explicit : rs.sun_rays;
+        if (!explicit_mode && !rs.reached && !out.cancelled) {
+            out.error = "run ended before the requested hits were numbered";
+            return false;
+        }
+        RunCounters c;
+        CK(cudaMemcpyAsync(&c, d_ctr.p, sizeof c, cudaMemcpyDeviceToHost, st));
+        const auto tr = std::chrono::steady_clock::now();
+        std::vector<unsigned long long> accv(acc_n);
+        if (acc_n) CK(cudaMemcpyAsync(accv.data(), d_acc.p, acc_n * 8, cudaMemcpyDeviceToHost, st));
+        out.d2h_bytes += acc_n * 8 + sizeof c;
+        CK(cudaStreamSynchronize(st));
+        for (int s = 0; s < nst; ++s) {
+            out.stage_entries[s] = c.stage_entries[s];
+            out.max_enter[s] = c.max_enter[s];
+            out.max_ttmiss[s] = c.max_ttmiss[s];
+        }
+        out.flags = c.flags;
+        out.first_hits.assign(accv.begin(), accv.begin() + ne);
+        out.absorbed.assign(accv.begin() + ne, accv.begin() + 2 * ne);
+        out.delivered.assign(accv.begin() + 2 * ne, accv.begin() + 3 * ne);
+        out.flux.clear();
+        for (size_t m = 0; m < rq.flux.size(); ++m)
+            out.flux.emplace_back(accv.begin() + flux_off[m],
+                                  accv.begin() + flux_off[m] + size_t(rq.flux[m].nx) * rq.flux[m].ny);
+        out.readback_ms += ms_since(tr);
+        if (out.flags & kFlagBadInteraction) {
+            out.error = "Bad optical interaction type (only 1 = refraction and 2 = reflection are traced)";
+            return false;
+        }
+        out.ok = true;
+        return true;
+    }
+    out.error = "record buffer could not be sized for this run";
+    return false;
+}
+
+}  // namespace stb

@@ -1,0 +1,136 @@
+// Flattened scene tables as they sit in device memory, shared by the host
+// set-up code (st_host.cpp) and the CUDA trace (st_trace.cu).
+//
+// Layout: one contiguous array of ElemRec for all stages (stage s owns
+// [first_elem, first_elem + n_elem)), one array of OpticRec (front/back faces of
+// every optical property set), plain double arrays for surface-file data and
+// property tables, and the acceleration structures (sun-plane grid for the
+// first stage's sun rays, one BVH per large stage).  Everything is read-only
+// during a trace and small (about 400 B per element), so it stays L2-resident.
+#pragma once
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define ST_HD __host__ __device__
+#else
+#define ST_HD
+#endif
+
+namespace stb {
+
+constexpr int kMaxStages = 16;
+constexpr int kMaxFluxMaps = 8;
+constexpr int kSunCdfCells = 4096;
+
+// surface model codes after coretrace/input.cpp:288-366 translation
+enum SurfType : int {
+    kSurfConic = 1,      // conic of revolution / cone (g, s, p, o, c)
+    kSurfCylinder = 2,   // 't'
+    kSurfFlat = 3,       // 'f'
+    kSurfFE = 4,         // 'e' finite-element data (not supported on the device)
+    kSurfVshot = 5,      // 'v'
+    kSurfZernike = 6,    // 'm'
+    kSurfSingleAxis = 7, // conic with one curvature (Cy = 0)
+    kSurfPoly = 8,       // 'r'
+    kSurfSpline = 9,     // 'i'
+    kSurfTorus = 10,     // 'd'
+};
+
+struct ElemRec {
+    double R[9];      // stage -> element rotation, row-major (RRefToLoc)
+    double o[3];      // element origin in stage coordinates
+    double ap[8];     // aperture parameters A..H
+    double zap;       // ZAperture
+    double kappa, vcx, vcy, curv_rev, cone_deg, ra, rs;
+    double area;      // aperture area
+    double bound_r;   // radius about the origin holding every accepted hit (<0: unbounded)
+    int shape;        // aperture code (lower-case char)
+    int surf;         // surface code as given (char, case preserved)
+    int stype;        // SurfType
+    int interaction;  // 1 refract, 2 reflect
+    int opt_front, opt_back;  // OpticRec index, -1 on virtual stages
+    int enabled;
+    int data_off, data_n, fit_order;  // surface data in SceneDev::surf_data
+    int spl_n;        // spline points (x, y, y2 consecutive blocks)
+    int pad_;
+};
+
+struct OpticRec {
+    double refl, trans, slope, spec;  // slope/spec in mrad
+    double n_in, n_out;               // RefractiveIndex[0], [2] after cross-wiring
+    int dist;                         // 'g', 'p', 'f', ...
+    int refl_tab_off, refl_tab_n;     // (angle, value) pairs in SceneDev::tables
+    int trans_tab_off, trans_tab_n;
+    int pad_;
+};
+
+struct StageRec {
+    double R[9];   // global -> stage rotation
+    double o[3];
+    int first_elem, n_elem;
+    int virt, multihit, tracethrough;
+    int bvh_off;   // first node in SceneDev::bvh, -1 when brute force is used
+    int bvh_items_off;
+    int pad_;
+};
+
+// BVH node over element bounding spheres in stage coordinates.  Leaf when
+// count > 0: items [first, first + count) of SceneDev::bvh_items; inner nodes
+// have children first (left) and first + 1.
+struct BvhNode {
+    float lo[3], hi[3];
+    int first, count;
+};
+
+struct FluxMapDev {
+    int stage, elem;      // 0-based stage, 0-based element index within the stage
+    int kind, nx, ny, absorbed_only;
+    double x0, x1, y0, y1;
+    unsigned long long *bins;
+};
+
+struct SunDev {
+    double xmin, xmax, ymin, ymax;  // sun box in the sun frame
+    double Rsun[9];                 // sun -> first-stage rotation (RLocToRef of the sun frame)
+    double pos_sun_stage[3];
+    double origin[3];               // sun position (point source)
+    int shape;                      // 'g', 'p', 'd', 'f', ...
+    int point_source;
+    double sigma;                   // mrad
+    const double *cdf_theta;        // kSunCdfCells + 1 (mrad)
+    const double *cdf;              // kSunCdfCells + 1
+    // sun-plane culling grid for the first stage (cells over the sun box)
+    int grid_on, gnx, gny;
+    double gx0, gy0, ginv;          // origin and 1/cell size
+    const int *cell_start;          // gnx*gny + 1
+    const int *cell_items;          // element indices (stage-local), ascending per cell
+};
+
+struct SceneDev {
+    const ElemRec *elems;
+    const OpticRec *optics;
+    const double *surf_data;
+    const double *tables;
+    const BvhNode *bvh;
+    const int *bvh_items;
+    StageRec stages[kMaxStages];
+    int n_stages;
+    SunDev sun;
+    int sunshape_on, errors_on;
+    uint32_t seed;
+    int precision;  // 0 FP64, 1 mixed
+    int explicit_rays;
+    const double *ex_pos, *ex_cos;
+    int n_flux;
+    FluxMapDev flux[kMaxFluxMaps];
+};
+
+// One intersection record as the reference stores it (coretrace/types.h:239-246),
+// plus the within-(ray, stage) hit index used to restore the reference's order.
+struct RecordDev {
+    double pos[3], cos[3];
+    int element, stage;
+    uint32_t raynum, seq;
+};
+
+}  // namespace stb

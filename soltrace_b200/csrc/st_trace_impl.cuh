@@ -1,0 +1,569 @@
+// Trace kernels of the B200 SolTrace path.
+//
+// A run is a sequence of sun-ray batches.  Per batch:
+//   k_probe   one thread per sun ray: generate it (generateray.cpp:58-161), find the
+//             nearest first-stage element it hits (raytrace.cpp:653-770), write the
+//             element (0 = miss) per ray and a per-block hit count;
+//   k_offsets single block: exclusive scan of the block counts;
+//   k_compact one thread per sun ray: ordered list of the rays that hit (their sun
+//             index and element), i.e. the reference's ray numbering, in which only
+//             first-stage hits consume a number (raytrace.cpp:780-798);
+//   k_trace   one thread per numbered ray: the rest of the per-ray state machine of
+//             raytrace.cpp:582-1040 through every stage, writing records, flux bins
+//             and counters.
+// Splitting off the probe keeps the trace kernel's warps full: the sun rays that
+// miss everything (most of them on a heliostat field) never enter it.
+#pragma once
+#include "st_device.cuh"
+#include "st_launch.h"
+
+namespace stb {
+
+constexpr int kMaxHitsPerStage = 100000;  // the reference has no bound; a ray trapped between
+                                          // mirrors would loop forever there
+
+// ------------------------------------------------------------------------------------
+// sun ray / explicit ray generation
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ void make_ray(const SceneDev &S, uint64_t sid, RayRng &rng, double pg[3], double cg[3],
+                                         double &xs, double &ys) {
+    const SunDev &sun = S.sun;
+    if (S.explicit_rays) {
+        for (int q = 0; q < 3; ++q) {
+            pg[q] = S.ex_pos[3 * sid + q];
+            cg[q] = S.ex_cos[3 * sid + q];
+        }
+        xs = ys = 0.0;
+        return;
+    }
+    if (sun.point_source) {  // generateray.cpp:101-133
+        for (int q = 0; q < 3; ++q) pg[q] = sun.origin[q];
+        for (int q = 0; q < 3; ++q) {
+            const double sg = (rng.u() <= 0.5) ? -1.0 : 1.0;
+            cg[q] = sg * rng.u();
+        }
+        const double m = sqrt(cg[0] * cg[0] + cg[1] * cg[1] + cg[2] * cg[2]);
+        for (int q = 0; q < 3; ++q) cg[q] = cg[q] / m;
+        xs = ys = 0.0;
+        return;
+    }
+    xs = sun.xmin + (sun.xmax - sun.xmin) * rng.u();
+    ys = sun.ymin + (sun.ymax - sun.ymin) * rng.u();
+    const double psun[3] = {xs, ys, -10000.0}, csun[3] = {0.0, 0.0, 1.0};
+    double pst[3], cst[3];
+    to_ref(sun.Rsun, sun.pos_sun_stage, psun, csun, pst, cst);
+    to_ref(S.stages[0].R, S.stages[0].o, pst, cst, pg, cg);
+}
+
+// ------------------------------------------------------------------------------------
+// nearest accepted hit in a stage (raytrace.cpp:698-770); -1 if none
+// ------------------------------------------------------------------------------------
+template <int MIXED>
+__device__ inline int nearest_brute(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3]) {
+    int best = -1;
+    double bp = 1e99;
+    for (int j = 0; j < st.n_elem; ++j) {
+        const ElemRec &e = S.elems[st.first_elem + j];
+        if (!e.enabled) continue;
+        double pl;
+        if (element_test<MIXED>(S, e, ps, cs, pl, nullptr) && pl < bp) {
+            bp = pl;
+            best = j;
+        }
+    }
+    return best;
+}
+
+// BVH over element bounding spheres; nodes farther than the best hit so far are
+// skipped (the test is on the entry distance minus the 1e-5 nudge, with slack for
+// the float box arithmetic).
+template <int MIXED>
+__device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3]) {
+    const BvhNode *nodes = S.bvh + st.bvh_off;
+    const int *items = S.bvh_items + st.bvh_items_off;
+    const float ox = float(ps[0]), oy = float(ps[1]), oz = float(ps[2]);
+    const float ix = 1.0f / float(cs[0]), iy = 1.0f / float(cs[1]), iz = 1.0f / float(cs[2]);
+    int stack[48];
+    int sp = 0;
+    stack[sp++] = 0;
+    int best = -1;
+    double bp = 1e99;
+    while (sp > 0) {
+        const BvhNode nd = nodes[stack[--sp]];
+        float t0x = (nd.lo[0] - ox) * ix, t1x = (nd.hi[0] - ox) * ix;
+        float t0y = (nd.lo[1] - oy) * iy, t1y = (nd.hi[1] - oy) * iy;
+        float t0z = (nd.lo[2] - oz) * iz, t1z = (nd.hi[2] - oz) * iz;
+        const float tmin = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fminf(t0z, t1z));
+        const float tmax = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fmaxf(t0z, t1z));
+        // NaN-safe: a NaN slab (origin on a face of a zero-width box) keeps the node
+        if (tmax < 0.0f || tmin > tmax) continue;
+        if (double(tmin) > bp * (1.0 + 1e-6) + 1e-3) continue;
+        if (nd.count > 0) {
+            for (int k = 0; k < nd.count; ++k) {
+                const int j = items[nd.first + k];
+                const ElemRec &e = S.elems[st.first_elem + j];
+                if (!e.enabled) continue;
+                double pl;
+                if (element_test<MIXED>(S, e, ps, cs, pl, nullptr) && (pl < bp || (pl == bp && j < best))) {
+                    bp = pl;
+                    best = j;
+                }
+            }
+        } else if (sp + 2 <= 48) {
+            stack[sp++] = nd.first + 1;
+            stack[sp++] = nd.first;
+        }
+    }
+    return best;
+}
+
+template <int MIXED>
+__device__ __forceinline__ int nearest(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3]) {
+    return (st.bvh_off >= 0) ? nearest_bvh<MIXED>(S, st, ps, cs) : nearest_brute<MIXED>(S, st, ps, cs);
+}
+
+// first test of a first-stage sun ray through the sun-plane grid (cells list the
+// elements, ascending, whose bounding disc in the sun plane overlaps the cell)
+template <int MIXED>
+__device__ inline int nearest_sun_grid(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3],
+                                double xs, double ys) {
+    const SunDev &sun = S.sun;
+    int cx = int(floor((xs - sun.gx0) * sun.ginv)), cy = int(floor((ys - sun.gy0) * sun.ginv));
+    cx = min(max(cx, 0), sun.gnx - 1);
+    cy = min(max(cy, 0), sun.gny - 1);
+    const int c = cy * sun.gnx + cx;
+    const int a = sun.cell_start[c], b = sun.cell_start[c + 1];
+    int best = -1;
+    double bp = 1e99;
+    for (int k = a; k < b; ++k) {
+        const int j = sun.cell_items[k];
+        const ElemRec &e = S.elems[st.first_elem + j];
+        if (!e.enabled) continue;
+        double pl;
+        if (element_test<MIXED>(S, e, ps, cs, pl, nullptr) && pl < bp) {
+            bp = pl;
+            best = j;
+        }
+    }
+    return best;
+}
+
+// ------------------------------------------------------------------------------------
+// optics (raytrace.cpp:885-946 test value; interaction.cpp:58-199)
+// ------------------------------------------------------------------------------------
+template <int MIXED>
+__device__ inline double test_value(const SceneDev &S, const OpticRec &op, int type, const double cin[3], const double n[3]) {
+    const int off = (type == 1) ? op.trans_tab_off : op.refl_tab_off;
+    const int np = (type == 1) ? op.trans_tab_n : op.refl_tab_n;
+    if (np <= 0) return (type == 1) ? op.trans : op.refl;
+    const double *tab = S.tables + off;  // (angle, value) pairs
+    double ia;
+    if (MIXED) {
+        const float nn = sqrtf(float(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]));
+        const float c = -(float(cin[0]) * float(n[0]) + float(cin[1]) * float(n[1]) + float(cin[2]) * float(n[2])) / nn;
+        ia = double(acosf(fminf(fmaxf(c, -1.f), 1.f)) * 1000.f);
+    } else {
+        const double nn = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        const double un[3] = {-n[0] / nn, -n[1] / nn, -n[2] / nn};
+        ia = acos(cin[0] * un[0] + cin[1] * un[1] + cin[2] * un[2]) * 1000.;
+    }
+    if (ia >= tab[2 * (np - 1)]) return tab[2 * (np - 1) + 1];
+    int m = 0;
+    while (m < np - 1 && tab[2 * m] < ia) m++;
+    if (m == 0) return tab[1];
+    return (tab[2 * m + 1] + tab[2 * (m - 1) + 1]) / 2.0;
+}
+
+__device__ __forceinline__ void reflect(const double cin[3], const double n[3], double out[3]) {
+    const double a = (cin[0] * n[0] + cin[1] * n[1] + cin[2] * n[2]) / (n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    for (int q = 0; q < 3; ++q) out[q] = cin[q] - 2.0 * a * n[q];
+}
+
+// refraction with an unpolarised Fresnel split; a non-converged Newton leaves the
+// incoming direction (the reference leaves the previous output untouched)
+template <int MIXED>
+__device__ inline void refract(const OpticRec &op, const double cin[3], const double n[3], RayRng &rng, double out[3]) {
+    const double r1 = op.n_in, r2 = op.n_out;
+    const double mu = r1 / r2;
+    const double d2 = n[0] * n[0] + n[1] * n[1] + n[2] * n[2];
+    const double B = (mu * mu - 1.0) / d2;
+    const double A = mu * (cin[0] * n[0] + cin[1] * n[1] + cin[2] * n[2]) / d2;
+    if (B > A * A) {  // total internal reflection
+        reflect(cin, n, out);
+        return;
+    }
+    double rave;
+    if (MIXED) {
+        const float nn = sqrtf(float(d2));
+        const float c = -(float(cin[0]) * float(n[0]) + float(cin[1]) * float(n[1]) + float(cin[2]) * float(n[2])) / nn;
+        const float ia = acosf(fminf(fmaxf(c, -1.f), 1.f));
+        const float f1 = float(r1), f2 = float(r2);
+        const float st = f1 * sinf(ia) / f2, ct = sqrtf(1.f - st * st), ci = cosf(ia);
+        const float rs = (f1 * ci - f2 * ct) / (f1 * ci + f2 * ct), rp = (f1 * ct - f2 * ci) / (f1 * ct + f2 * ci);
+        rave = double((rp * rp + rs * rs) / 2.f);
+    } else {
+        const double nn = sqrt(d2);
+        const double un[3] = {-n[0] / nn, -n[1] / nn, -n[2] / nn};
+        const double ia = acos(cin[0] * un[0] + cin[1] * un[1] + cin[2] * un[2]);
+        const double st = r1 * sin(ia) / r2, ct = sqrt(1 - st * st);
+        const double rsn = r1 * cos(ia) - r2 * ct, rsd = r1 * cos(ia) + r2 * ct;
+        const double rpn = r1 * ct - r2 * cos(ia), rpd = r1 * ct + r2 * cos(ia);
+        rave = ((rpn / rpd) * (rpn / rpd) + (rsn / rsd) * (rsn / rsd)) / 2.0;
+    }
+    if (rave < rng.u()) {
+        double g = -B / (2.0 * A), g1 = g;
+        bool ok = false;
+        for (int i = 1; i < 10; ++i) {
+            g1 = (g * g - B) / (2.0 * (g + A));
+            if (fabs(g - g1) < 0.000005) {
+                ok = true;
+                break;
+            }
+            g = g1;
+        }
+        if (!ok) {
+            for (int q = 0; q < 3; ++q) out[q] = cin[q];
+            return;
+        }
+        for (int q = 0; q < 3; ++q) out[q] = mu * cin[q] + g1 * n[q];
+    } else {
+        reflect(cin, n, out);
+    }
+}
+
+// error sample about `axis` (sunshape: source 1; specularity: source 2 with the
+// reflection re-draw of errors.cpp:222-225)
+template <int MIXED>
+__device__ inline void error_sample(const SceneDev &S, int dist, double delop, bool sunshape, const double axis[3],
+                             RayRng &rng, bool redraw_below, const double nrm[3], double out[3]) {
+    for (unsigned call = 0;; ++call) {
+        const double ut = rng.u();
+        const double up = rng.u();
+        if (MIXED) {
+            float th;
+            switch (dist) {
+                case 'g':
+                case 'G':
+                    th = float(delop) * sqrtf(-2.f * __logf(float(1.0 - ut)));  // 1 - u in double: never 0
+                    break;
+                case 'p':
+                case 'P':
+                    th = float(delop) * sqrtf(float(ut));
+                    break;
+                case 'f':
+                case 'F':
+                    th = asinf(sqrtf(float(ut)));
+                    break;
+                default:
+                    th = float(sample_theta(dist, delop, ut, S.sun, sunshape));
+            }
+            perturb<float>(axis, th, float(up) * 6.2831853f, out);
+        } else {
+            const double th = sample_theta(dist, delop, ut, S.sun, sunshape);
+            perturb<double>(axis, th, up * 2.0 * 3.1415926535897932385, out);
+        }
+        if (!(redraw_below && out[0] * nrm[0] + out[1] * nrm[1] + out[2] * nrm[2] < 0 && call < 50000)) break;
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// record, flux and counter output
+// ------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long warp_reserve(unsigned long long *counter) {
+    const unsigned mask = __activemask();
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    const unsigned rank = __popc(mask & ((1u << lane) - 1u));
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + rank;
+}
+
+__device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed, const double pe[3]) {
+    for (int m = 0; m < S.n_flux; ++m) {
+        const FluxMapDev &f = S.flux[m];
+        if (f.stage != si || f.elem != ej) continue;
+        if (f.absorbed_only && !absorbed) continue;
+        double u, u0, u1;
+        if (f.kind == 0) {
+            u = pe[0];
+            u0 = f.x0;
+            u1 = f.x1;
+        } else {
+            u = atan2(pe[0], pe[2] - f.x1) + kPiD;
+            u0 = 0.0;
+            u1 = 2.0 * kPiD;
+        }
+        const double ix = floor((u - u0) / (u1 - u0) * f.nx);
+        const double iy = floor((pe[1] - f.y0) / (f.y1 - f.y0) * f.ny);
+        if (ix < 0 || ix >= f.nx || iy < 0 || iy >= f.ny) continue;
+        atomicAdd(&f.bins[int(iy) * f.nx + int(ix)], 1ull);
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// kernels
+// ------------------------------------------------------------------------------------
+template <int MIXED>
+__global__ void __launch_bounds__(kProbeBlock) k_probe(SceneDev S, uint64_t s0, uint32_t n, uint32_t *hit_elem,
+                                                        uint32_t *block_counts, const RunState *rs) {
+    const uint32_t i = blockIdx.x * kProbeBlock + threadIdx.x;
+    uint32_t h = 0;
+    if (rs->reached) {  // the requested hits are numbered: this batch is surplus
+        if (threadIdx.x == 0) block_counts[blockIdx.x] = 0;
+        return;
+    }
+    if (i < n) {
+        RayRng rng;
+        rng.init(S.seed, s0 + i, 0);
+        double pg[3], cg[3], xs, ys;
+        make_ray(S, s0 + i, rng, pg, cg, xs, ys);
+        const StageRec &st = S.stages[0];
+        double ps[3], cs[3];
+        to_local(st.R, st.o, pg, cg, ps, cs);
+        int b;
+        if (S.sun.grid_on && !S.explicit_rays && !S.sun.point_source)
+            b = nearest_sun_grid<MIXED>(S, st, ps, cs, xs, ys);
+        else
+            b = nearest<MIXED>(S, st, ps, cs);
+        h = (b >= 0) ? uint32_t(b + 1) : 0u;
+        hit_elem[i] = h;
+    }
+    const int c = __syncthreads_count(h != 0);
+    if (threadIdx.x == 0) block_counts[blockIdx.x] = uint32_t(c);
+}
+
+#ifdef ST_COMMON_KERNELS
+// exclusive scan of the per-block counts (one block; counts fit in 32 bits per batch)
+__global__ void __launch_bounds__(1024) k_offsets(const uint32_t *counts, uint32_t nb, uint32_t *offsets,
+                                                   uint32_t *total) {
+    __shared__ uint32_t warp_sums[32];
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < nb; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = (i < nb) ? counts[i] : 0u;
+        uint32_t x = v;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_sums[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            uint32_t s = warp_sums[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            warp_sums[lane] = s;
+        }
+        __syncthreads();
+        const uint32_t incl = x + (w > 0 ? warp_sums[w - 1] : 0u) + carry;
+        if (i < nb) offsets[i] = incl - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(kProbeBlock) k_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem,
+                                                          const uint32_t *counts, const uint32_t *offsets,
+                                                          uint64_t *hit_sid, uint32_t *hit_el) {
+    __shared__ uint32_t wsum[kProbeBlock / 32];
+    if (counts[blockIdx.x] == 0) return;
+    const uint32_t i = blockIdx.x * kProbeBlock + threadIdx.x;
+    const uint32_t h = (i < n) ? hit_elem[i] : 0u;
+    const unsigned bal = __ballot_sync(0xffffffffu, h != 0);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) wsum[w] = __popc(bal);
+    __syncthreads();
+    uint32_t pre = 0;
+    for (int k = 0; k < w; ++k) pre += wsum[k];
+    if (h != 0) {
+        const uint32_t pos = offsets[blockIdx.x] + pre + __popc(bal & ((1u << lane) - 1u));
+        hit_sid[pos] = s0 + i;
+        hit_el[pos] = h - 1;
+    }
+}
+
+// single thread: apply the cut-off at the requested hit count and advance the run state
+__global__ void k_advance(const uint32_t *total, const uint64_t *hit_sid, uint64_t s0, uint32_t n, RunState *rs) {
+    if (rs->reached) return;
+    const unsigned long long left = rs->target - rs->hits_done;
+    const unsigned long long take = (*total < left) ? *total : left;
+    rs->hits_done += take;
+    if (rs->hits_done == rs->target && take > 0) {
+        rs->reached = 1;
+        rs->sun_rays = hit_sid[take - 1] + 1;
+    } else {
+        rs->sun_rays = s0 + n;
+    }
+}
+#endif  // ST_COMMON_KERNELS
+
+template <int MIXED, int RECORDS>
+__global__ void __launch_bounds__(kTraceBlock) k_trace(SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el,
+                                                        const uint32_t *total, const RunState *rs, TraceOut O) {
+    __shared__ unsigned long long sh_entries[kMaxStages];
+    __shared__ unsigned int sh_max_enter[kMaxStages], sh_max_tt[kMaxStages];
+    __shared__ unsigned int sh_flags;
+    if (threadIdx.x < kMaxStages) {
+        sh_entries[threadIdx.x] = 0;
+        sh_max_enter[threadIdx.x] = 0;
+        sh_max_tt[threadIdx.x] = 0;
+    }
+    if (threadIdx.x == 0) sh_flags = 0;
+    __syncthreads();
+
+    // rays of this batch to trace: the cut-off at the requested hit count (k_advance
+    // applies the same rule after this kernel)
+    uint32_t n = 0, raynum_base = 0;
+    if (!rs->reached) {
+        const unsigned long long left = rs->target - rs->hits_done;
+        n = uint32_t(*total < left ? *total : left);
+        raynum_base = uint32_t(rs->hits_done);
+    }
+    for (uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x; i < n; i += gridDim.x * kTraceBlock) {
+        const uint64_t sid = hit_sid[i];
+        const uint32_t raynum = raynum_base + i + 1;
+        RayRng rng;
+        rng.init(S.seed, sid, 0);
+        double pg[3], cg[3], xs, ys;
+        make_ray(S, sid, rng, pg, cg, xs, ys);
+        int known = int(hit_el[i]);
+        int first_elem0 = -1;  // the ray's first first-stage element (global index)
+        for (int si = 0; si < S.n_stages; ++si) {
+            const StageRec &st = S.stages[si];
+            atomicAdd(&sh_entries[si], 1ull);
+            atomicMax(&sh_max_enter[si], raynum);
+            double ps[3], cs[3];
+            to_local(st.R, st.o, pg, cg, ps, cs);
+            int hits = 0;
+            bool absorbed = false;
+            for (;;) {
+                int j = (hits == 0 && known >= 0) ? known : nearest<MIXED>(S, st, ps, cs);
+                known = -1;
+                if (j < 0) break;
+                const ElemRec &e = S.elems[st.first_elem + j];
+                Hit h;
+                double pl;
+                // re-test the chosen element for the full hit (same arithmetic as the search)
+                if (!element_test<MIXED>(S, e, ps, cs, pl, &h)) break;
+                ++hits;
+                if (hits == 1) {
+                    atomicAdd(&O.first_hits[st.first_elem + j], 1ull);
+                    if (si == 0) first_elem0 = st.first_elem + j;
+                }
+                double pout[3], cout[3];
+                if (st.virt) {
+                    for (int q = 0; q < 3; ++q) {
+                        pout[q] = h.pe[q];
+                        cout[q] = h.ce[q];
+                    }
+                } else {
+                    if (e.interaction != 1 && e.interaction != 2) {
+                        atomicOr(&sh_flags, unsigned(kFlagBadInteraction));
+                        absorbed = true;
+                    } else {
+                        const OpticRec &op = S.optics[h.back ? e.opt_back : e.opt_front];
+                        const double tv = test_value<MIXED>(S, op, e.interaction, h.ce, h.n);
+                        if (tv <= rng.u()) absorbed = true;
+                        if (!absorbed) {
+                            double cin[3] = {h.ce[0], h.ce[1], h.ce[2]};
+                            if (S.sunshape_on && si == 0 && hits == 1) {
+                                double c2[3];
+                                error_sample<MIXED>(S, S.sun.shape, S.sun.sigma / 1000.0, true, cin, rng, false, h.n, c2);
+                                for (int q = 0; q < 3; ++q) cin[q] = c2[q];
+                            }
+                            double nrm[3] = {h.n[0], h.n[1], h.n[2]};
+                            if (S.errors_on) {
+                                double n2[3];
+                                const int d = op.dist;
+                                const int dd = (d == 'g' || d == 'G' || d == 'p' || d == 'P') ? d : 0;
+                                error_sample<MIXED>(S, dd, op.slope / 1000.0, false, nrm, rng, false, nrm, n2);
+                                for (int q = 0; q < 3; ++q) nrm[q] = n2[q];
+                            }
+                            if (e.interaction == 1)
+                                refract<MIXED>(op, cin, nrm, rng, cout);
+                            else
+                                reflect(cin, nrm, cout);
+                            if (S.errors_on) {
+                                const bool diffuse = (op.dist == 'f' || op.dist == 'F');
+                                double axis[3], c3[3];
+                                for (int q = 0; q < 3; ++q) axis[q] = diffuse ? nrm[q] : cout[q];
+                                error_sample<MIXED>(S, op.dist, op.spec / 1000.0, false, axis, rng, e.interaction == 2, nrm,
+                                                    c3);
+                                for (int q = 0; q < 3; ++q) cout[q] = c3[q];
+                            }
+                            for (int q = 0; q < 3; ++q) pout[q] = h.pe[q];
+                        }
+                    }
+                }
+                if (RECORDS) {
+                    const unsigned long long slot = warp_reserve(O.rec_count);
+                    if (slot < O.rec_cap) {
+                        RecordDev r;
+                        to_ref(e.R, e.o, h.pe, h.ce, r.pos, r.cos);
+                        r.element = absorbed ? -(j + 1) : (j + 1);
+                        r.stage = si + 1;
+                        r.raynum = raynum;
+                        r.seq = uint32_t(hits - 1);
+                        O.recs[slot] = r;
+                    }
+                }
+                if (S.n_flux) bin_flux(S, si, j, absorbed, h.pe);
+                if (absorbed) {
+                    atomicAdd(&O.absorbed[st.first_elem + j], 1ull);
+                    if (si == S.n_stages - 1 && first_elem0 >= 0) atomicAdd(&O.delivered[first_elem0], 1ull);
+                    break;
+                }
+                to_ref(e.R, e.o, pout, cout, ps, cs);
+                if (!st.multihit) break;
+                if (hits >= kMaxHitsPerStage) {
+                    atomicOr(&sh_flags, unsigned(kFlagHitCap));
+                    break;
+                }
+            }
+            if (absorbed) break;
+            if (hits == 0) {
+                // a miss (raytrace.cpp:800-826): trace-through stages carry the ray on
+                // unchanged; both record the incoming ray with element 0.  The one miss
+                // the reference does not record (the stage's last ray in a
+                // trace-through stage) is removed on the host from max_ttmiss.
+                if (si == 0) break;  // cannot happen: first-stage rays are numbered hits
+                if (RECORDS) {
+                    const unsigned long long slot = warp_reserve(O.rec_count);
+                    if (slot < O.rec_cap) {
+                        RecordDev r;
+                        to_local(st.R, st.o, pg, cg, r.pos, r.cos);
+                        r.element = 0;
+                        r.stage = si + 1;
+                        r.raynum = raynum;
+                        r.seq = 0;
+                        O.recs[slot] = r;
+                    }
+                }
+                if (!st.tracethrough) break;
+                atomicMax(&sh_max_tt[si], raynum);
+                continue;  // global ray unchanged
+            }
+            to_ref(st.R, st.o, ps, cs, pg, cg);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < S.n_stages && sh_entries[threadIdx.x]) {
+        atomicAdd(&O.ctr->stage_entries[threadIdx.x], sh_entries[threadIdx.x]);
+        atomicMax(&O.ctr->max_enter[threadIdx.x], sh_max_enter[threadIdx.x]);
+        if (sh_max_tt[threadIdx.x]) atomicMax(&O.ctr->max_ttmiss[threadIdx.x], sh_max_tt[threadIdx.x]);
+    }
+    if (threadIdx.x == 0 && sh_flags) atomicOr(&O.ctr->flags, sh_flags);
+}
+
+}  // namespace stb

@@ -1,0 +1,56 @@
+"""Algorithmic work of the trace, per unit, for roofline accounting.
+
+Counted from the reference's arithmetic (FMA = 2 flops; sqrt, division and
+transcendental calls counted separately as special operations), at one
+candidate-element test per ray-stage (culling overhead is not work):
+
+  transform of a ray into a frame (position and direction, 3x3)    33
+  sun-ray generation (two affine maps and two transforms)          72
+  flat-element test (start plane, aperture, acceptance)            84
+  cylinder / quadric closed form with normal                      110
+  hit bookkeeping (record transform)                               33
+  table sunshape sample (inverse CDF) + perturbation frame         50
+  slope-error sample + perturbation frame                         100
+  reflection                                                       17
+  back-transforms element -> stage -> global                       66
+  absorption test                                                   1
+
+Bytes: the probe writes one 4-byte element word per sun ray and the compaction
+re-reads it; every first-stage hit moves 12 bytes (sun index + element) into the
+hit list and the trace kernel reads them back.  Scene tables are L2-resident.
+"""
+
+GEN, XFORM, FLAT, QUAD, BOOK, SUNSHAPE, SLOPE, REFLECT, BACK, ABSORB = 72, 33, 84, 110, 33, 50, 100, 17, 66, 1
+
+# first-stage probe of one sun ray: generate, transform to the heliostat, one flat test
+PROBE_FLOPS_PER_SUN_RAY = GEN + XFORM + FLAT
+# a numbered ray in the first stage: re-test of its element, bookkeeping, absorption,
+# sunshape, slope error, reflection, back-transforms, one blocking re-test
+TRACE_FLOPS_PER_HIT = XFORM + FLAT + BOOK + ABSORB + SUNSHAPE + SLOPE + REFLECT + BACK + XFORM + FLAT
+# a ray entering the receiver stage: transform, cylinder test, bookkeeping, absorption
+TRACE_FLOPS_PER_RECEIVER_ENTRY = XFORM + QUAD + BOOK + ABSORB
+
+PROBE_BYTES_PER_SUN_RAY = 4 + 4
+HIT_LIST_BYTES_PER_HIT = 12 + 12
+
+# Nominal vector peaks of a B200 (148 SMs at 1965 MHz; 64 FP64 and 128 FP32 lanes
+# per SM, 2 flops per FMA).  The pool's measured peaks cover HBM copy bandwidth and
+# bf16 GEMM only.
+NOMINAL_FP64_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
+NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
+
+
+def probe_flops(sun_rays: int) -> float:
+    return float(sun_rays) * PROBE_FLOPS_PER_SUN_RAY
+
+
+def trace_flops(hits: int, receiver_entries: int) -> float:
+    return float(hits) * TRACE_FLOPS_PER_HIT + float(receiver_entries) * TRACE_FLOPS_PER_RECEIVER_ENTRY
+
+
+def probe_bytes(sun_rays: int, hits: int) -> float:
+    return float(sun_rays) * PROBE_BYTES_PER_SUN_RAY + float(hits) * 12
+
+
+def trace_bytes(hits: int) -> float:
+    return float(hits) * 12

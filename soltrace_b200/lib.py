@@ -1,0 +1,99 @@
+"""Loader for the in-tree coretrace_api.so (the CUDA product).
+
+`load()` returns a `StApi` bound to soltrace_b200/coretrace_api.so with the
+st_b200_* extension signatures added.  It raises if the library has not been
+built: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .capi import StApi, c_double_p, st_uint_t
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "coretrace_api.so")
+
+ST_B200_FP64 = 0
+ST_B200_MIXED = 1
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("sun_rays", C.c_ulonglong),
+        ("ray_hits", C.c_ulonglong),
+        ("stage_entries", C.c_ulonglong * 16),
+        ("ray_stage_units", C.c_ulonglong),
+        ("records", C.c_ulonglong),
+        ("kernel_ms", C.c_double),
+        ("probe_ms", C.c_double),
+        ("trace_ms", C.c_double),
+        ("setup_ms", C.c_double),
+        ("readback_ms", C.c_double),
+        ("batches", C.c_int),
+        ("gpu_launches", C.c_int),
+        ("h2d_bytes", C.c_ulonglong),
+        ("d2h_bytes", C.c_ulonglong),
+    ]
+
+
+_u64p = C.POINTER(C.c_ulonglong)
+EXTENSIONS = {
+    "st_b200_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "st_b200_set_records": (C.c_int, [C.c_void_p, C.c_int]),
+    "st_b200_set_device": (C.c_int, [C.c_void_p, C.c_int]),
+    "st_b200_explicit_rays": (C.c_int, [C.c_void_p, st_uint_t, c_double_p, c_double_p]),
+    "st_b200_add_flux_map": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                       C.c_double, C.c_double, C.c_double, C.c_int]),
+    "st_b200_clear_flux_maps": (C.c_int, [C.c_void_p]),
+    "st_b200_flux_counts": (C.c_int, [C.c_void_p, C.c_int, _u64p]),
+    "st_b200_run_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
+    "st_b200_element_counts": (C.c_int, [C.c_void_p, C.c_int, _u64p, _u64p, _u64p]),
+}
+
+
+class B200Api(StApi):
+    def stats(self, ctx) -> dict:
+        s = Stats()
+        self.st_b200_run_stats(ctx, C.byref(s))
+        d = {k: getattr(s, k) for k, _ in Stats._fields_ if k != "stage_entries"}
+        d["stage_entries"] = list(s.stage_entries)
+        return d
+
+    def flux(self, ctx, idx: int, nx: int, ny: int) -> np.ndarray:
+        out = np.zeros(nx * ny, dtype=np.uint64)
+        rc = self.st_b200_flux_counts(ctx, idx, out.ctypes.data_as(_u64p))
+        if rc < 0:
+            raise RuntimeError("st_b200_flux_counts failed")
+        return out.reshape(ny, nx)
+
+    def element_counts(self, ctx, stage: int, n: int):
+        a = np.zeros(n, dtype=np.uint64)
+        b = np.zeros(n, dtype=np.uint64)
+        c = np.zeros(n, dtype=np.uint64)
+        self.st_b200_element_counts(ctx, stage, a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p), c.ctypes.data_as(_u64p))
+        return a, b, c
+
+    def explicit_rays(self, ctx, pos: np.ndarray, cos: np.ndarray) -> int:
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        cos = np.ascontiguousarray(cos, dtype=np.float64)
+        self._ex_keep = (pos, cos)
+        return self.st_b200_explicit_rays(ctx, len(pos), pos.ctypes.data_as(c_double_p), cos.ctypes.data_as(c_double_p))
+
+
+_API = None
+
+
+def load(path: str | None = None) -> B200Api:
+    """Bind the built library; raises FileNotFoundError when it is missing."""
+    global _API
+    p = path or LIB_PATH
+    if path is None and _API is not None:
+        return _API
+    if not os.path.exists(p):
+        raise FileNotFoundError(f"{p} is not built; run `python -m soltrace_b200.build`")
+    api = B200Api(C.CDLL(p), EXTENSIONS)
+    if path is None:
+        _API = api
+    return api

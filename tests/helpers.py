@@ -1,0 +1,50 @@
+"""Shared helpers for the parity tests."""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+
+from soltrace_b200 import scenes
+
+
+def run_scene(api, sc, seed, setup=None):
+    """Push `sc` into a fresh context of `api`, run, and return (n, records, sun stats, messages)."""
+    ctx = api.st_create_context()
+    try:
+        scenes.push(api, ctx, sc)
+        if setup:
+            setup(api, ctx)
+        n = api.run(ctx, seed)
+        rec = api.records(ctx) if n > 0 else api.records(ctx)
+        ss = api.sun_stats(ctx)
+        msg = api.messages(ctx)
+        extra = setup.collect(api, ctx) if setup is not None and hasattr(setup, "collect") else None
+    finally:
+        api.st_free_context(ctx)
+    return n, rec, ss, msg, extra
+
+
+def records_digest(rec: dict) -> str:
+    """sha256 over the raw record arrays in readback order (x y z cx cy cz element stage raynum)."""
+    h = hashlib.sha256()
+    for k in ("x", "y", "z", "cx", "cy", "cz"):
+        h.update(np.ascontiguousarray(rec[k], dtype="<f8").tobytes())
+    for k in ("element", "stage", "raynum"):
+        h.update(np.ascontiguousarray(rec[k], dtype="<i4").tobytes())
+    return h.hexdigest()
+
+
+def assert_same_records(a: dict, b: dict, pos_tol: float, rel_tol: float = 0.0, dir_tol: float = None):
+    """Integer fields identical; positions within pos_tol + rel_tol*|pos|; directions within dir_tol."""
+    assert len(a["x"]) == len(b["x"]), (len(a["x"]), len(b["x"]))
+    for k in ("element", "stage", "raynum"):
+        assert np.array_equal(a[k], b[k]), k
+    for k in ("x", "y", "z"):
+        tol = pos_tol + rel_tol * np.abs(b[k])
+        d = np.abs(a[k] - b[k])
+        assert np.all(d <= tol), (k, float(d.max()))
+    dtol = pos_tol if dir_tol is None else dir_tol
+    for k in ("cx", "cy", "cz"):
+        d = np.abs(a[k] - b[k])
+        assert np.all(d <= dtol + rel_tol), (k, float(d.max()))
