@@ -1084,36 +1084,48 @@ double table_intensity(const Sun &sun, double theta) {
     return sun.inten[i - 1] + (sun.inten[i] - sun.inten[i - 1]) * (theta - sun.ang[i - 1]) / (sun.ang[i] - sun.ang[i - 1]);
 }
 
-// inverse CDF of p(theta) ~ theta * I(theta) on [0, MaxAngle] (mrad), 4096 cells
+// Inverse CDF of p(theta) ~ theta * I(theta) on [0, MaxAngle] (mrad): trapezoid CDF on
+// 4096 cells, then theta(u) tabulated at 8193 equally spaced probabilities; a sample
+// interpolates linearly between two table entries.  (Per-ray stream only; the
+// reference stream reproduces the reference's 2-D rejection sampling instead.)
 constexpr int kCdfCells = 4096;
+constexpr int kInvCells = 8192;
 void build_sun_cdf(Sun &sun) {
-    sun.cdf_theta.assign(kCdfCells + 1, 0.0);
-    sun.cdf.assign(kCdfCells + 1, 0.0);
-    if (sun.ang.size() < 2 || !(sun.max_angle > 0)) return;
+    sun.cdf_theta.clear();
+    sun.cdf.clear();
+    if (sun.ang.size() < 3 || !(sun.max_angle > 0)) return;
+    std::vector<double> th(kCdfCells + 1, 0.0), cdf(kCdfCells + 1, 0.0);
     const double dt = sun.max_angle / kCdfCells;
     double prev = 0.0;
     for (int j = 0; j <= kCdfCells; ++j) {
-        const double th = dt * j;
-        const double pdf = th * table_intensity(sun, th);
-        sun.cdf_theta[j] = th;
-        if (j > 0) sun.cdf[j] = sun.cdf[j - 1] + 0.5 * (prev + pdf) * dt;
+        th[j] = dt * j;
+        const double pdf = th[j] * table_intensity(sun, th[j]);
+        if (j > 0) cdf[j] = cdf[j - 1] + 0.5 * (prev + pdf) * dt;
         prev = pdf;
     }
-    const double tot = sun.cdf[kCdfCells];
-    for (int j = 0; j <= kCdfCells; ++j) sun.cdf[j] = tot > 0 ? sun.cdf[j] / tot : 0.0;
+    const double tot = cdf[kCdfCells];
+    for (int j = 0; j <= kCdfCells; ++j) cdf[j] = tot > 0 ? cdf[j] / tot : 0.0;
+    sun.cdf.assign(kInvCells + 1, 0.0);  // theta at u = j / kInvCells
+    for (int j = 0; j <= kInvCells; ++j) {
+        const double u = double(j) / kInvCells;
+        int lo = 0, hi = kCdfCells;
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (cdf[mid] <= u)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const double f = (cdf[hi] > cdf[lo]) ? (u - cdf[lo]) / (cdf[hi] - cdf[lo]) : 0.0;
+        sun.cdf[j] = th[lo] + f * (th[hi] - th[lo]);
+    }
 }
 double sample_sun_table(const Sun &sun, double u) {
-    int lo = 0, hi = kCdfCells;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (sun.cdf[mid] <= u)
-            lo = mid;
-        else
-            hi = mid;
-    }
-    const double c0 = sun.cdf[lo], c1 = sun.cdf[hi];
-    const double f = (c1 > c0) ? (u - c0) / (c1 - c0) : 0.0;
-    return sun.cdf_theta[lo] + f * (sun.cdf_theta[hi] - sun.cdf_theta[lo]);
+    if (sun.cdf.empty()) return 0.0;
+    const double x = u * kInvCells;
+    const int j = std::min(int(x), kInvCells - 1);
+    const double f = x - j;
+    return sun.cdf[j] + f * (sun.cdf[j + 1] - sun.cdf[j]);
 }
 
 // rotate (sin t cos p, sin t sin p, cos t) from the frame whose z axis is 'axis'
@@ -1898,7 +1910,7 @@ int run_trace(Context *cx, unsigned seed) {
     double pos_sun_stage[3];
     std::vector<double> proj;
     if (!sun_to_primary(cx, s0, pos_sun_stage, proj)) return -1;
-    if (cx->sun.shape == 'd' || cx->sun.shape == 'D') build_sun_cdf(cx->sun);
+    build_sun_cdf(cx->sun);
 
     Minstd seq;
     seq.seed(seed);

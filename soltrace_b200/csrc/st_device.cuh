@@ -4,8 +4,11 @@
 // reference's per-ray state machine (coretrace/raytrace.cpp:582-1040); the
 // citation on each gives the reference routine whose results it reproduces.
 // FP64 paths keep the reference's arithmetic order where it matters for
-// agreement to 1e-9 m; MIXED paths move element-local work to float after
-// re-basing the ray near the element in double.
+// agreement to 1e-9 m.  In MIXED mode the geometry that fixes hit positions
+// (transforms, closed-form roots, the torus quartic, Newton refinement,
+// reflection and refraction directions) stays in double, which is what holds
+// explicit-ray positions within 1e-5 m at km scale; aperture tests, property
+// tables, Fresnel coefficients, error sampling and flux binning run in float.
 #pragma once
 #include <cstdint>
 #include <cmath>
@@ -274,103 +277,6 @@ __device__ inline int quadric_hit(const ElemRec &e, const double P[3], const dou
         n[1] = -gy / m;
         n[2] = -gz / m;
     }
-    return 0;
-}
-
-// Mixed-precision quadric: the ray is re-based (in double) to the point of closest
-// approach to the element origin, the quadratic is solved in float about that point,
-// and path lengths are re-assembled in double before the reference's root choice.
-__device__ inline int quadric_hit_mixed(const ElemRec &e, const double P[3], const double D[3], double out[3],
-                                 double n[3], double &t) {
-    const int s = e.surf | 0x20;
-    // re-base at the closest approach to the surface's centre of curvature, measured
-    // only along the curved axes (a cylinder or trough ignores its straight y axis)
-    const bool straight_y = (s == 't') || (e.stype == kSurfSingleAxis);
-    const double zc0 = (s == 's' || s == 't') ? ((s == 's') ? 1.0 / e.vcx : 1.0 / e.curv_rev)
-                                              : ((s == 'o') ? 1.0 / e.kappa / e.vcx : 0.0);
-    const double wy = straight_y ? 0.0 : 1.0;
-    const double dd = D[0] * D[0] + wy * D[1] * D[1] + D[2] * D[2];
-    const double t0 = dd > 1e-300 ? -(P[0] * D[0] + wy * P[1] * D[1] + (P[2] - zc0) * D[2]) / dd : 0.0;
-    const float px = float(P[0] + t0 * D[0]), py = float(P[1] + t0 * D[1]), pz = float(P[2] + t0 * D[2]);
-    const float dx = float(D[0]), dy = float(D[1]), dz = float(D[2]);
-    float zc = 0.f, kx = 1.f, ky = 1.f, kz = 1.f, a2 = 1.f, b2 = 1.f, A, B, C;
-    if (s == 'p') {
-        a2 = float(2.0 / e.vcx);
-        b2 = e.vcy > 0.0 ? float(2.0 / e.vcy) : 1e10f;
-        ky = (e.stype == kSurfSingleAxis) ? 0.f : 1.f;
-        kz = 0.f;
-        A = dx * dx * kx / a2 + dy * dy * ky / b2;
-        B = 2.f * (kx * px * dx / a2 + ky * py * dy / b2) - dz;
-        C = kx * px * px / a2 + ky * py * py / b2 - pz;
-    } else {
-        float rhs;
-        if (s == 's') {
-            ky = (e.stype == kSurfSingleAxis) ? 0.f : 1.f;
-            const float r = float(1.0 / e.vcx);
-            zc = r;
-            rhs = r * r;
-        } else if (s == 'o') {
-            kz = float(e.kappa);
-            zc = float(1.0 / e.kappa / e.vcx);
-            rhs = float(1.0 / e.kappa / (e.vcx * e.vcx));
-        } else {
-            ky = 0.f;
-            const float r = float(1.0 / e.curv_rev);
-            zc = r;
-            rhs = r * r;
-        }
-        const float zd = pz - zc;
-        A = dx * dx * kx + dy * dy * ky + dz * dz * kz;
-        B = 2.f * (kx * px * dx + ky * py * dy + kz * zd * dz);
-        C = kx * px * px + ky * py * py + kz * zd * zd - rhs;
-    }
-    double tt;
-    if (fabsf(A) < 1e-12f) {
-        const double t1 = t0 + double(-C / B);
-        if (!(t1 > 0)) return 1;
-        tt = t1;
-    } else {
-        const float disc = B * B - 4.f * A * C;
-        if (!(disc > 0.f)) return 1;
-        const float q = sqrtf(disc);
-        // numerically stable pair of roots about the re-based point
-        const float qq = -0.5f * (B + copysignf(q, B));
-        float r1 = qq / A, r2 = (qq != 0.f) ? C / qq : r1;
-        const float lo = fminf(r1, r2), hi = fmaxf(r1, r2);
-        // t2 is the smaller root when A > 0 (the reference's (-B - q)/2A)
-        const double t2 = t0 + double(A > 0.f ? lo : hi);
-        const double t1 = t0 + double(A > 0.f ? hi : lo);
-        if (t2 > 0) {
-            tt = t2;
-            if (P[2] + t2 * D[2] > e.zap) tt = t1;
-            const bool finite_len = (s == 't') || (s == 's' && e.stype == kSurfSingleAxis);
-            if (finite_len) {
-                const double yt = P[1] + tt * D[1];
-                if (yt < -e.ap[2] / 2.0 || yt > e.ap[2] / 2.0) tt = t1;
-            }
-        } else if (t2 == 0 || (t2 < 0 && t1 > 0)) {
-            tt = t1;
-        } else {
-            return 1;
-        }
-    }
-    t = tt;
-    out[0] = P[0] + tt * D[0];
-    out[1] = P[1] + tt * D[1];
-    out[2] = P[2] + tt * D[2];
-    const float ox = float(out[0]), oy = float(out[1]), oz = float(out[2]);
-    const float gx = 2.f * kx * ox / a2, gy = 2.f * ky * oy / b2;
-    float gz, m;
-    if (s == 'p') {
-        gz = -1.f;
-        m = sqrtf(gx * gx + gy * gy + 1.f);
-    } else {
-        gz = 2.f * kz * (oz - zc);
-        m = sqrtf(gx * gx + gy * gy + gz * gz);
-    }
-    n[0] = double(-gx / m);
-    n[1] = double(-gy / m);
-    n[2] = double(-gz / m);
     return 0;
 }
 
@@ -927,9 +833,18 @@ struct Hit {
     int back;
 };
 
+// Surfaces that are rare in large fields (torus quartic, Newton-iterated conics,
+// cones and file-defined surfaces) stay out of line so that the hot flat and
+// closed-form quadric paths inline without call-saved registers.
+static __device__ __noinline__ int cold_intersect(const SceneDev &S, const ElemRec &e, const double pe[3],
+                                           const double ce[3], double out[3], double n[3], double &t) {
+    if (e.stype == kSurfTorus) return torus_hit(e, pe, ce, out, n, t);
+    return newton_hit(e, S.surf_data, pe, ce, out, n, t);
+}
+
 template <int MIXED>
-__device__ inline bool element_test(const SceneDev &S, const ElemRec &e, const double ps[3], const double cs[3], double &plen,
-                             Hit *full) {
+__device__ __forceinline__ bool element_test(const SceneDev &S, const ElemRec &e, const double ps[3],
+                                             const double cs[3], double &plen, Hit *full) {
     double pe[3], ce[3];
     to_local(e.R, e.o, ps, cs, pe, ce);
     pe[0] = pe[0] + 1.0e-5 * ce[0];
@@ -948,19 +863,19 @@ __device__ inline bool element_test(const SceneDev &S, const ElemRec &e, const d
             break;
         }
         case kSurfCylinder:
-            err = MIXED ? quadric_hit_mixed(e, pe, ce, out, n, t) : quadric_hit(e, pe, ce, out, n, t);
+            err = quadric_hit(e, pe, ce, out, n, t);
             break;
         case kSurfTorus:
-            err = torus_hit(e, pe, ce, out, n, t);
+            err = cold_intersect(S, e, pe, ce, out, n, t);
             break;
         default: {
             const int s = e.surf | 0x20;
             const bool closed = (s == 'p') || (s == 's' && (e.stype == kSurfConic || e.stype == kSurfSingleAxis)) ||
                                 (s == 'o' && e.stype == kSurfConic);
             if (closed)
-                err = MIXED ? quadric_hit_mixed(e, pe, ce, out, n, t) : quadric_hit(e, pe, ce, out, n, t);
+                err = quadric_hit(e, pe, ce, out, n, t);
             else
-                err = newton_hit(e, S.surf_data, pe, ce, out, n, t);
+                err = cold_intersect(S, e, pe, ce, out, n, t);
         }
     }
     if (err > 0 || t < 0) return false;
@@ -1003,18 +918,12 @@ __device__ inline double sample_theta(int dist, double delop, double u, const Su
         case 'd':
         case 'D': {
             (void)sunshape;
-            if (sun.cdf == nullptr) return 0.0;  // no table was given (st_sun_userdata)
-            int lo = 0, hi = kSunCdfCells;
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (sun.cdf[mid] <= u)
-                    lo = mid;
-                else
-                    hi = mid;
-            }
-            const double c0 = sun.cdf[lo], c1 = sun.cdf[hi];
-            const double f = (c1 > c0) ? (u - c0) / (c1 - c0) : 0.0;
-            return (sun.cdf_theta[lo] + f * (sun.cdf_theta[hi] - sun.cdf_theta[lo])) / 1000.0;
+            if (sun.inv_cdf == nullptr) return 0.0;  // no table was given (st_sun_userdata)
+            // theta(u) tabulated at u = j / kSunInvCells, linear in between
+            const double x = u * kSunInvCells;
+            const int j = min(int(x), kSunInvCells - 1);
+            const double f = x - j;
+            return (sun.inv_cdf[j] + f * (sun.inv_cdf[j + 1] - sun.inv_cdf[j])) / 1000.0;
         }
         case 'f':
         case 'F':

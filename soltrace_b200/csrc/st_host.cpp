@@ -100,6 +100,10 @@ struct Context {
     int (*cb)(unsigned long, unsigned long, unsigned long, unsigned long, unsigned long, void *) = nullptr;
     void *cbdata = nullptr;
     double last_hit_rate = 0.0;  // batch planning hint carried between runs of a context
+    Workspace *ws = nullptr;     // device buffers reused by every run of this context
+    ~Context() {
+        if (ws) workspace_destroy(ws);
+    }
     Context() { memset(&stats, 0, sizeof stats); }
     void log(const char *fmt, ...) {
         char buf[513];
@@ -711,9 +715,10 @@ bool sun_setup(Context *cx, HostScene &hs) {
     sd.point_source = sun.point_source ? 1 : 0;
     sd.sigma = sun.sigma;
 
-    // inverse CDF of theta * I(theta) on [0, MaxAngle] for table sunshapes
-    hs.cdf_theta.clear();
-    hs.cdf.clear();
+    // Inverse CDF of p(theta) ~ theta * I(theta) on [0, MaxAngle] for table sunshapes:
+    // trapezoid CDF on kSunCdfCells cells, then theta(u) tabulated at kSunInvCells + 1
+    // equally spaced probabilities so that a sample costs one interpolation.
+    hs.inv_cdf.clear();
     if (sun.ang.size() >= 3 && sun.max_angle > 0) {
         auto intensity = [&](double th) {
             size_t i = 0;
@@ -721,20 +726,32 @@ bool sun_setup(Context *cx, HostScene &hs) {
             if (i == 0) return sun.inten[0];
             return sun.inten[i - 1] + (sun.inten[i] - sun.inten[i - 1]) * (th - sun.ang[i - 1]) / (sun.ang[i] - sun.ang[i - 1]);
         };
-        const int K = kSunCdfCells;
-        hs.cdf_theta.assign(K + 1, 0.0);
-        hs.cdf.assign(K + 1, 0.0);
+        const int K = kSunCdfCells, KI = kSunInvCells;
+        std::vector<double> th(K + 1, 0.0), cdf(K + 1, 0.0);
         const double dth = sun.max_angle / K;
         double prev = 0.0;
         for (int j = 0; j <= K; ++j) {
-            const double th = dth * j;
-            const double pdf = th * intensity(th);
-            hs.cdf_theta[j] = th;
-            if (j > 0) hs.cdf[j] = hs.cdf[j - 1] + 0.5 * (prev + pdf) * dth;
+            th[j] = dth * j;
+            const double pdf = th[j] * intensity(th[j]);
+            if (j > 0) cdf[j] = cdf[j - 1] + 0.5 * (prev + pdf) * dth;
             prev = pdf;
         }
-        const double tot = hs.cdf[K];
-        for (int j = 0; j <= K; ++j) hs.cdf[j] = tot > 0 ? hs.cdf[j] / tot : 0.0;
+        const double tot = cdf[K];
+        for (int j = 0; j <= K; ++j) cdf[j] = tot > 0 ? cdf[j] / tot : 0.0;
+        hs.inv_cdf.assign(KI + 1, 0.0);
+        for (int j = 0; j <= KI; ++j) {
+            const double u = double(j) / KI;
+            int lo = 0, hi = K;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (cdf[mid] <= u)
+                    lo = mid;
+                else
+                    hi = mid;
+            }
+            const double f = (cdf[hi] > cdf[lo]) ? (u - cdf[lo]) / (cdf[hi] - cdf[lo]) : 0.0;
+            hs.inv_cdf[j] = th[lo] + f * (th[hi] - th[lo]);
+        }
     }
 
     // sun-plane grid over the first stage: every element whose bounding disc (centre
@@ -781,6 +798,15 @@ bool sun_setup(Context *cx, HostScene &hs) {
                         const double ddy = std::max(std::max(ay - cy_[j], 0.0), cy_[j] - by);
                         if (ddx * ddx + ddy * ddy <= pad * pad) cells[size_t(gy) * nx + gx].push_back(int(j));
                     }
+            }
+            hs.disc.assign(st.elems.size(), float4{0.f, 0.f, 0.f, 0.f});
+            for (size_t j = 0; j < st.elems.size(); ++j) {
+                // float disc for the probe's pre-test: radius widened by the float rounding
+                // of centre and ray coordinates (~1e-7 relative)
+                const double pad = rad[j] * (1.0 + 1e-9) + 1e-6 * (1.0 + fabs(cx_[j]) + fabs(cy_[j]));
+                const double fr = pad + 4e-7 * (fabs(cx_[j]) + fabs(cy_[j]) + fabs(sun.xmin) + fabs(sun.xmax) +
+                                                fabs(sun.ymin) + fabs(sun.ymax) + pad);
+                hs.disc[j] = float4{float(cx_[j]), float(cy_[j]), float(fr), 0.f};
             }
             hs.cell_start.assign(size_t(nx) * ny + 1, 0);
             for (size_t c = 0; c < cells.size(); ++c) {
@@ -1004,7 +1030,8 @@ int run(Context *cx, unsigned seed) {
     rq.hit_rate_hint = cx->last_hit_rate;
     RunResult rr;
     const double host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    const bool ok = gpu_run(hs, rq, rr);
+    if (!cx->ws) cx->ws = workspace_create();
+    const bool ok = gpu_run(hs, rq, rr, *cx->ws);
     if (!ok) {
         cx->log("%s", rr.error.c_str());
         return -1;

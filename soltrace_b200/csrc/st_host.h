@@ -5,6 +5,8 @@
 #include <string>
 #include <vector>
 
+#include <vector_types.h>
+
 #include "st_scene.h"
 
 namespace stb {
@@ -17,7 +19,8 @@ struct HostScene {
     std::vector<BvhNode> bvh;
     std::vector<int> bvh_items;
     std::vector<int> cell_start, cell_items;
-    std::vector<double> cdf_theta, cdf;
+    std::vector<double> inv_cdf;  // table-sunshape inverse CDF (kSunInvCells + 1 entries)
+    std::vector<float4> disc;     // first-stage projected bounding discs (sun-plane grid)
     SceneDev dev;  // stages, sun scalars and flags; device pointers are filled by gpu_run
 };
 
@@ -57,6 +60,9 @@ struct RunResult {
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
 };
 
-bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out);
+struct Workspace;
+Workspace *workspace_create();
+void workspace_destroy(Workspace *w);
+bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspace &ws);
 
 }  // namespace stb

@@ -1,5 +1,6 @@
 // Precision-independent kernels: ordered compaction of the probe's hits.
 #define ST_COMMON_KERNELS
+#include <algorithm>
 #include "st_launch.h"
 #include "st_trace_impl.cuh"
 
@@ -15,5 +16,14 @@ void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uin
 void launch_advance(const uint32_t *total, const uint64_t *hit_sid, uint64_t s0, uint32_t n, RunState *rs,
                     cudaStream_t st) {
     k_advance<<<1, 1, 0, st>>>(total, hit_sid, s0, n, rs);
+}
+void launch_sort_by_element(const uint32_t *total, const uint64_t *hit_sid, const uint32_t *hit_el, uint32_t n_elem0,
+                            uint32_t *elem_count, uint32_t *elem_cursor, uint32_t *scratch_total, uint64_t *s_sid,
+                            uint32_t *s_el, uint32_t *s_idx, uint32_t max_n, cudaStream_t st) {
+    const uint32_t blocks = std::max(1u, std::min<uint32_t>((max_n + 255) / 256, 148u * 8u));
+    cudaMemsetAsync(elem_count, 0, size_t(n_elem0) * 4, st);
+    k_elem_hist<<<blocks, 256, 0, st>>>(total, hit_el, elem_count);
+    k_offsets<<<1, 1024, 0, st>>>(elem_count, n_elem0, elem_cursor, scratch_total);
+    k_elem_scatter<<<blocks, 256, 0, st>>>(total, hit_sid, hit_el, elem_cursor, s_sid, s_el, s_idx);
 }
 }  // namespace stb

@@ -11,11 +11,12 @@ void launch_probe_fp64(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit
     k_probe<0><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs);
 }
 void launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
-                       const uint32_t *total, const RunState *rs, const TraceOut &O, uint32_t blocks, cudaStream_t st) {
+                       const uint32_t *hit_idx, const uint32_t *total, RunState *rs, const TraceOut &O,
+                       uint32_t blocks, cudaStream_t st) {
     if (records)
-        k_trace<0, 1><<<blocks, kTraceBlock, 0, st>>>(S, hit_sid, hit_el, total, rs, O);
+        k_trace<0, 1><<<blocks, kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs, O);
     else
-        k_trace<0, 0><<<blocks, kTraceBlock, 0, st>>>(S, hit_sid, hit_el, total, rs, O);
+        k_trace<0, 0><<<blocks, kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs, O);
 }
 // resident trace blocks per SM, from this instantiation's register and shared-memory use
 int trace_blocks_per_sm_fp64(bool records) {

@@ -32,7 +32,7 @@ struct RunState {
     unsigned long long target;     // rays to number (~0 in explicit-ray mode)
     unsigned long long sun_rays;   // SunRayCount so far (final once reached)
     unsigned int reached;
-    unsigned int pad_;
+    unsigned int cursor;           // trace work queue: next hit-list entry to hand out
 };
 
 struct TraceOut {
@@ -53,9 +53,15 @@ void launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hi
 // grid-stride trace over min(*total, target - hits_done) numbered rays; `blocks`
 // is the grid size (0 = enough blocks for `max_n` rays)
 void launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
-                       const uint32_t *total, const RunState *rs, const TraceOut &O, uint32_t blocks, cudaStream_t st);
+                       const uint32_t *hit_idx, const uint32_t *total, RunState *rs, const TraceOut &O,
+                       uint32_t blocks, cudaStream_t st);
 void launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
-                        const uint32_t *total, const RunState *rs, const TraceOut &O, uint32_t blocks, cudaStream_t st);
+                        const uint32_t *hit_idx, const uint32_t *total, RunState *rs, const TraceOut &O,
+                        uint32_t blocks, cudaStream_t st);
+// counting sort of the batch's hits by first-stage element (n_elem0 buckets)
+void launch_sort_by_element(const uint32_t *total, const uint64_t *hit_sid, const uint32_t *hit_el, uint32_t n_elem0,
+                            uint32_t *elem_count, uint32_t *elem_cursor, uint32_t *scratch_total, uint64_t *s_sid,
+                            uint32_t *s_el, uint32_t *s_idx, uint32_t max_n, cudaStream_t st);
 void launch_offsets(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_t *total, cudaStream_t st);
 void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uint32_t *counts,
                     const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st);

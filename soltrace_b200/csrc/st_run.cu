@@ -49,6 +49,28 @@ cudaError_t upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s, uint64_t 
     return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
 }
 
+}  // namespace
+
+// Device buffers, stream and events of one context, kept across runs so that a
+// repeated st_sim_run pays no allocation: every buffer only grows.
+struct Workspace {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    DevBuf elems, optics, surf, tables, bvh, bvh_items, cell_start, cell_items, inv_cdf, disc, expos, excos;
+    DevBuf acc, ctr, rs, rec_count, hit_elem, counts, offsets, total, hit_sid, hit_el, recs;
+    DevBuf ecount, ecursor, etotal, s_sid, s_el, s_idx;
+    std::vector<cudaEvent_t> events;
+    ~Workspace() {
+        if (device >= 0) cudaSetDevice(device);
+        for (auto e : events) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+Workspace *workspace_create() { return new Workspace; }
+void workspace_destroy(Workspace *w) { delete w; }
+
+namespace {
 double ms_since(std::chrono::steady_clock::time_point t0) {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -64,7 +86,7 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
         }                                                                                     \
     } while (0)
 
-bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out) {
+bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspace &ws) {
     const auto t_setup = std::chrono::steady_clock::now();
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -76,15 +98,16 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out) {
         return false;
     }
     CK(cudaSetDevice(rq.device));
-    cudaStream_t st;
-    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    struct StreamGuard {
-        cudaStream_t s;
-        ~StreamGuard() { cudaStreamDestroy(s); }
-    } sg{st};
-
-    DevBuf d_elems, d_optics, d_surf, d_tables, d_bvh, d_bvh_items, d_cell_start, d_cell_items, d_cdf_t, d_cdf, d_expos,
-        d_excos;
+    if (ws.device != rq.device) {  // a workspace serves one device: start afresh on another
+        ws.~Workspace();
+        new (&ws) Workspace();
+        ws.device = rq.device;
+    }
+    if (!ws.stream) CK(cudaStreamCreateWithFlags(&ws.stream, cudaStreamNonBlocking));
+    cudaStream_t st = ws.stream;
+    DevBuf &d_elems = ws.elems, &d_optics = ws.optics, &d_surf = ws.surf, &d_tables = ws.tables, &d_bvh = ws.bvh,
+           &d_bvh_items = ws.bvh_items, &d_cell_start = ws.cell_start, &d_cell_items = ws.cell_items,
+           &d_inv_cdf = ws.inv_cdf, &d_disc = ws.disc, &d_expos = ws.expos, &d_excos = ws.excos;
     CK(upload(d_elems, hs.elems, st, out.h2d_bytes));
     CK(upload(d_optics, hs.optics, st, out.h2d_bytes));
     CK(upload(d_surf, hs.surf_data, st, out.h2d_bytes));
@@ -93,8 +116,8 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out) {
     CK(upload(d_bvh_items, hs.bvh_items, st, out.h2d_bytes));
     CK(upload(d_cell_start, hs.cell_start, st, out.h2d_bytes));
     CK(upload(d_cell_items, hs.cell_items, st, out.h2d_bytes));
-    CK(upload(d_cdf_t, hs.cdf_theta, st, out.h2d_bytes));
-    CK(upload(d_cdf, hs.cdf, st, out.h2d_bytes));
+    CK(upload(d_inv_cdf, hs.inv_cdf, st, out.h2d_bytes));
+    CK(upload(d_disc, hs.disc, st, out.h2d_bytes));
     CK(upload(d_expos, rq.ex_pos, st, out.h2d_bytes));
     CK(upload(d_excos, rq.ex_cos, st, out.h2d_bytes));
 
@@ -107,8 +130,8 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out) {
     S.bvh_items = d_bvh_items.as<int>();
     S.sun.cell_start = d_cell_start.as<int>();
     S.sun.cell_items = d_cell_items.as<int>();
-    S.sun.cdf_theta = hs.cdf_theta.empty() ? nullptr : d_cdf_t.as<double>();
-    S.sun.cdf = hs.cdf.empty() ? nullptr : d_cdf.as<double>();
+    S.sun.inv_cdf = hs.inv_cdf.empty() ? nullptr : d_inv_cdf.as<double>();
+    S.sun.disc = d_disc.as<float4>();
     S.seed = rq.seed;
     S.precision = rq.precision;
     const bool explicit_mode = !rq.ex_pos.empty();
@@ -136,7 +159,20 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out) {
 
     const int nst = S.n_stages;
     const uint64_t kMaxBatch = uint64_t(1) << 25;
-    DevBuf d_acc, d_ctr, d_rs, d_rec_count, d_hit_elem, d_counts, d_offsets, d_total, d_hit_sid, d_hit_el, d_recs;
+    DevBuf &d_acc = ws.acc, &d_ctr = ws.ctr, &d_rs = ws.rs, &d_rec_count = ws.rec_count, &d_hit_elem = ws.hit_elem,
+           &d_counts = ws.counts, &d_offsets = ws.offsets, &d_total = ws.total, &d_hit_sid = ws.hit_sid,
+           &d_hit_el = ws.hit_el, &d_recs = ws.recs;
+    // rays are regrouped by first-stage element when that stage is large enough to
+    // have a BVH (their blocking tests then walk the same nodes in a warp)
+    const uint32_t n_elem0 = uint32_t(S.stages[0].n_elem);
+    const bool sort_hits = S.stages[0].bvh_off >= 0 && n_elem0 > 1;
+    DevBuf &d_ecount = ws.ecount, &d_ecursor = ws.ecursor, &d_etotal = ws.etotal, &d_s_sid = ws.s_sid,
+           &d_s_el = ws.s_el, &d_s_idx = ws.s_idx;
+    if (sort_hits) {
+        CK(d_ecount.ensure(size_t(n_elem0) * 4));
+        CK(d_ecursor.ensure(size_t(n_elem0) * 4));
+        CK(d_etotal.ensure(8));
+    }
     unsigned long long rec_cap = 0;
     CK(cudaStreamSynchronize(st));
     out.setup_ms = ms_since(t_setup);
@@ -191,18 +227,14 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out) {
         uint64_t sun_next = 0;
         double p_est = rq.hit_rate_hint > 0 ? rq.hit_rate_hint : 0.0;
         RunState rs = rs0;
-        std::vector<cudaEvent_t> evs;
-        struct EvList {
-            std::vector<cudaEvent_t> &v;
-            ~EvList() {
-                for (auto e : v) cudaEventDestroy(e);
-            }
-        } evl{evs};
+        size_t ev_used = 0;
         auto new_event = [&]() {
-            cudaEvent_t e;
-            cudaEventCreate(&e);
-            evs.push_back(e);
-            return e;
+            if (ev_used == ws.events.size()) {
+                cudaEvent_t e;
+                cudaEventCreate(&e);
+                ws.events.push_back(e);
+            }
+            return ws.events[ev_used++];
         };
         std::vector<std::pair<cudaEvent_t, cudaEvent_t>> probe_ev, trace_ev;
         cudaEvent_t t_first = new_event(), t_last = new_event();
@@ -239,6 +271,11 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out) {
                 CK(d_total.ensure(8));
                 CK(d_hit_sid.ensure(n * 8));
                 CK(d_hit_el.ensure(n * 4));
+                if (sort_hits) {
+                    CK(d_s_sid.ensure(n * 8));
+                    CK(d_s_el.ensure(n * 4));
+                    CK(d_s_idx.ensure(n * 4));
+                }
                 if (rq.records) {
                     if (rec_cap == 0) rec_cap = std::min<uint64_t>(n, uint64_t(1) << 22) * uint64_t(nst) * 2 + 4096;
                     CK(d_recs.ensure(rec_cap * sizeof(RecordDev)));
@@ -255,13 +292,23 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out) {
                 launch_offsets(d_counts.as<uint32_t>(), nb, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), st);
                 launch_compact(sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(),
                                d_offsets.as<uint32_t>(), d_hit_sid.as<uint64_t>(), d_hit_el.as<uint32_t>(), st);
+                const uint64_t *t_sid = d_hit_sid.as<uint64_t>();
+                const uint32_t *t_el = d_hit_el.as<uint32_t>(), *t_idx = nullptr;
+                if (sort_hits) {
+                    launch_sort_by_element(d_total.as<uint32_t>(), d_hit_sid.as<uint64_t>(), d_hit_el.as<uint32_t>(),
+                                           n_elem0, d_ecount.as<uint32_t>(), d_ecursor.as<uint32_t>(),
+                                           d_etotal.as<uint32_t>(), d_s_sid.as<uint64_t>(), d_s_el.as<uint32_t>(),
+                                           d_s_idx.as<uint32_t>(), uint32_t(n), st);
+                    out.gpu_launches += 3;
+                    t_sid = d_s_sid.as<uint64_t>();
+                    t_el = d_s_el.as<uint32_t>();
+                    t_idx = d_s_idx.as<uint32_t>();
+                }
                 CK(cudaEventRecord(p1, st));
                 if (rq.precision)
-                    launch_trace_mixed(rq.records, S, d_hit_sid.as<uint64_t>(), d_hit_el.as<uint32_t>(),
-                                       d_total.as<uint32_t>(), drs, O, trace_grid, st);
+                    launch_trace_mixed(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(), drs, O, trace_grid, st);
                 else
-                    launch_trace_fp64(rq.records, S, d_hit_sid.as<uint64_t>(), d_hit_el.as<uint32_t>(),
-                                      d_total.as<uint32_t>(), drs, O, trace_grid, st);
+                    launch_trace_fp64(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(), drs, O, trace_grid, st);
                 CK(cudaEventRecord(p2, st));
                 launch_advance(d_total.as<uint32_t>(), d_hit_sid.as<uint64_t>(), sun_next, uint32_t(n), drs, st);
                 CK(cudaGetLastError());

@@ -9,6 +9,7 @@
 // during a trace and small (about 400 B per element), so it stays L2-resident.
 #pragma once
 #include <cstdint>
+#include <vector_types.h>
 
 #ifdef __CUDACC__
 #define ST_HD __host__ __device__
@@ -21,6 +22,7 @@ namespace stb {
 constexpr int kMaxStages = 16;
 constexpr int kMaxFluxMaps = 8;
 constexpr int kSunCdfCells = 4096;
+constexpr int kSunInvCells = 8192;
 
 // surface model codes after coretrace/input.cpp:288-366 translation
 enum SurfType : int {
@@ -97,13 +99,13 @@ struct SunDev {
     int shape;                      // 'g', 'p', 'd', 'f', ...
     int point_source;
     double sigma;                   // mrad
-    const double *cdf_theta;        // kSunCdfCells + 1 (mrad)
-    const double *cdf;              // kSunCdfCells + 1
+    const double *inv_cdf;          // theta (mrad) at u = j / kSunInvCells, j = 0..kSunInvCells
     // sun-plane culling grid for the first stage (cells over the sun box)
     int grid_on, gnx, gny;
     double gx0, gy0, ginv;          // origin and 1/cell size
     const int *cell_start;          // gnx*gny + 1
     const int *cell_items;          // element indices (stage-local), ascending per cell
+    const float4 *disc;             // per first-stage element: projected centre x, y and radius
 };
 
 struct SceneDev {

@@ -135,8 +135,15 @@ __device__ inline int nearest_sun_grid(const SceneDev &S, const StageRec &st, co
     const int a = sun.cell_start[c], b = sun.cell_start[c + 1];
     int best = -1;
     double bp = 1e99;
+    const float fx = float(xs), fy = float(ys);
     for (int k = a; k < b; ++k) {
         const int j = sun.cell_items[k];
+        // the ray can only meet element j inside its projected bounding disc (the disc the
+        // grid was built from, already padded for rounding): a float test before the
+        // double-precision element transform
+        const float4 d = sun.disc[j];
+        const float dx = fx - d.x, dy = fy - d.y;
+        if (dx * dx + dy * dy > d.z * d.z) continue;
         const ElemRec &e = S.elems[st.first_elem + j];
         if (!e.enabled) continue;
         double pl;
@@ -280,25 +287,44 @@ __device__ __forceinline__ unsigned long long warp_reserve(unsigned long long *c
     return base + rank;
 }
 
+template <int MIXED>
 __device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed, const double pe[3]) {
     for (int m = 0; m < S.n_flux; ++m) {
         const FluxMapDev &f = S.flux[m];
         if (f.stage != si || f.elem != ej) continue;
         if (f.absorbed_only && !absorbed) continue;
-        double u, u0, u1;
-        if (f.kind == 0) {
-            u = pe[0];
-            u0 = f.x0;
-            u1 = f.x1;
+        int ix, iy;
+        if (MIXED) {
+            float u, u0, u1;
+            if (f.kind == 0) {
+                u = float(pe[0]);
+                u0 = float(f.x0);
+                u1 = float(f.x1);
+            } else {
+                u = atan2f(float(pe[0]), float(pe[2] - f.x1)) + 3.14159265f;
+                u0 = 0.f;
+                u1 = 6.28318531f;
+            }
+            ix = int(floorf((u - u0) / (u1 - u0) * f.nx));
+            iy = int(floorf(float((pe[1] - f.y0) / (f.y1 - f.y0)) * f.ny));
         } else {
-            u = atan2(pe[0], pe[2] - f.x1) + kPiD;
-            u0 = 0.0;
-            u1 = 2.0 * kPiD;
+            double u, u0, u1;
+            if (f.kind == 0) {
+                u = pe[0];
+                u0 = f.x0;
+                u1 = f.x1;
+            } else {
+                u = atan2(pe[0], pe[2] - f.x1) + kPiD;
+                u0 = 0.0;
+                u1 = 2.0 * kPiD;
+            }
+            const double dx = floor((u - u0) / (u1 - u0) * f.nx), dy = floor((pe[1] - f.y0) / (f.y1 - f.y0) * f.ny);
+            if (dx < 0 || dx >= f.nx || dy < 0 || dy >= f.ny) continue;
+            ix = int(dx);
+            iy = int(dy);
         }
-        const double ix = floor((u - u0) / (u1 - u0) * f.nx);
-        const double iy = floor((pe[1] - f.y0) / (f.y1 - f.y0) * f.ny);
         if (ix < 0 || ix >= f.nx || iy < 0 || iy >= f.ny) continue;
-        atomicAdd(&f.bins[int(iy) * f.nx + int(ix)], 1ull);
+        atomicAdd(&f.bins[iy * f.nx + ix], 1ull);
     }
 }
 
@@ -393,8 +419,30 @@ __global__ void __launch_bounds__(kProbeBlock) k_compact(uint64_t s0, uint32_t n
     }
 }
 
+// Counting sort of a batch's hits by first-stage element, so that each warp of the
+// trace kernel carries rays leaving the same element (coherent traversals).  Order
+// within an element is arbitrary: every result is independent of it (per-ray
+// random streams, integer flux atomics, records ordered by ray number).
+__global__ void __launch_bounds__(256) k_elem_hist(const uint32_t *total, const uint32_t *hit_el, uint32_t *elem_count) {
+    const uint32_t n = *total;
+    for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) atomicAdd(&elem_count[hit_el[i]], 1u);
+}
+__global__ void __launch_bounds__(256) k_elem_scatter(const uint32_t *total, const uint64_t *hit_sid, const uint32_t *hit_el,
+                                                      uint32_t *elem_cursor, uint64_t *s_sid, uint32_t *s_el,
+                                                      uint32_t *s_idx) {
+    const uint32_t n = *total;
+    for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
+        const uint32_t e = hit_el[i];
+        const uint32_t pos = atomicAdd(&elem_cursor[e], 1u);
+        s_sid[pos] = hit_sid[i];
+        s_el[pos] = e;
+        s_idx[pos] = i;
+    }
+}
+
 // single thread: apply the cut-off at the requested hit count and advance the run state
 __global__ void k_advance(const uint32_t *total, const uint64_t *hit_sid, uint64_t s0, uint32_t n, RunState *rs) {
+    rs->cursor = 0;  // the next batch's trace work queue starts empty
     if (rs->reached) return;
     const unsigned long long left = rs->target - rs->hits_done;
     const unsigned long long take = (*total < left) ? *total : left;
@@ -410,29 +458,47 @@ __global__ void k_advance(const uint32_t *total, const uint64_t *hit_sid, uint64
 
 template <int MIXED, int RECORDS>
 __global__ void __launch_bounds__(kTraceBlock) k_trace(SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el,
-                                                        const uint32_t *total, const RunState *rs, TraceOut O) {
+                                                        const uint32_t *hit_idx, const uint32_t *total,
+                                                        RunState *rs, TraceOut O) {
     __shared__ unsigned long long sh_entries[kMaxStages];
     __shared__ unsigned int sh_max_enter[kMaxStages], sh_max_tt[kMaxStages];
-    __shared__ unsigned int sh_flags;
+    __shared__ unsigned int sh_flags, sh_warps_done;
     if (threadIdx.x < kMaxStages) {
         sh_entries[threadIdx.x] = 0;
         sh_max_enter[threadIdx.x] = 0;
         sh_max_tt[threadIdx.x] = 0;
     }
-    if (threadIdx.x == 0) sh_flags = 0;
+    if (threadIdx.x == 0) {
+        sh_flags = 0;
+        sh_warps_done = 0;
+    }
     __syncthreads();
 
     // rays of this batch to trace: the cut-off at the requested hit count (k_advance
     // applies the same rule after this kernel)
-    uint32_t n = 0, raynum_base = 0;
+    // (entries may be sorted by element: hit_idx gives each entry's sun-order index)
+    uint32_t n = 0, take = 0, raynum_base = 0;
     if (!rs->reached) {
         const unsigned long long left = rs->target - rs->hits_done;
-        n = uint32_t(*total < left ? *total : left);
+        n = *total;
+        take = uint32_t(n < left ? n : left);
         raynum_base = uint32_t(rs->hits_done);
     }
-    for (uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x; i < n; i += gridDim.x * kTraceBlock) {
+    if (!hit_idx) n = take;
+    // warps take 32 consecutive entries at a time from the queue: consecutive entries
+    // share their first element once sorted, and no warp waits for another
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        __syncwarp();
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&rs->cursor, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const uint32_t i = base + lane;
+        const uint32_t idx = (i < n) ? (hit_idx ? hit_idx[i] : i) : 0xffffffffu;
+        if (i >= n || idx >= take) continue;  // past the list, or beyond the requested hit count
         const uint64_t sid = hit_sid[i];
-        const uint32_t raynum = raynum_base + i + 1;
+        const uint32_t raynum = raynum_base + idx + 1;
         RayRng rng;
         rng.init(S.seed, sid, 0);
         double pg[3], cg[3], xs, ys;
@@ -518,7 +584,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(SceneDev S, const uint64_
                         O.recs[slot] = r;
                     }
                 }
-                if (S.n_flux) bin_flux(S, si, j, absorbed, h.pe);
+                if (S.n_flux) bin_flux<MIXED>(S, si, j, absorbed, h.pe);
                 if (absorbed) {
                     atomicAdd(&O.absorbed[st.first_elem + j], 1ull);
                     if (si == S.n_stages - 1 && first_elem0 >= 0) atomicAdd(&O.delivered[first_elem0], 1ull);
@@ -557,13 +623,29 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(SceneDev S, const uint64_
             to_ref(st.R, st.o, ps, cs, pg, cg);
         }
     }
-    __syncthreads();
-    if (threadIdx.x < S.n_stages && sh_entries[threadIdx.x]) {
-        atomicAdd(&O.ctr->stage_entries[threadIdx.x], sh_entries[threadIdx.x]);
-        atomicMax(&O.ctr->max_enter[threadIdx.x], sh_max_enter[threadIdx.x]);
-        if (sh_max_tt[threadIdx.x]) atomicMax(&O.ctr->max_ttmiss[threadIdx.x], sh_max_tt[threadIdx.x]);
+    // the last warp of the block to finish flushes the block's counters (no barrier,
+    // so finished warps never wait for the block's slowest ray)
+    __syncwarp();
+    unsigned last = 0;
+    if (lane == 0) {
+        __threadfence_block();
+        last = (atomicAdd(&sh_warps_done, 1u) == (kTraceBlock / 32) - 1) ? 1u : 0u;
     }
-    if (threadIdx.x == 0 && sh_flags) atomicOr(&O.ctr->flags, sh_flags);
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) {
+        __threadfence_block();
+        for (int s2 = lane; s2 < S.n_stages; s2 += 32) {
+            const unsigned long long ent = atomicAdd(&sh_entries[s2], 0ull);
+            if (ent) {
+                atomicAdd(&O.ctr->stage_entries[s2], ent);
+                atomicMax(&O.ctr->max_enter[s2], atomicMax(&sh_max_enter[s2], 0u));
+                const unsigned tt = atomicMax(&sh_max_tt[s2], 0u);
+                if (tt) atomicMax(&O.ctr->max_ttmiss[s2], tt);
+            }
+        }
+        const unsigned fl = atomicOr(&sh_flags, 0u);
+        if (lane == 0 && fl) atomicOr(&O.ctr->flags, fl);
+    }
 }
 
 }  // namespace stb

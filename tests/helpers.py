@@ -36,14 +36,17 @@ def records_digest(rec: dict) -> str:
 
 
 def assert_same_records(a: dict, b: dict, pos_tol: float, rel_tol: float = 0.0, dir_tol: float = None):
-    """Integer fields identical; positions within pos_tol + rel_tol*|pos|; directions within dir_tol."""
+    """Integer fields identical; positions within pos_tol + rel_tol * (scene size), the scene
+    size being the largest coordinate in the records (round-off grows with the length of the
+    path a ray has travelled, not with its final coordinate); directions within dir_tol."""
     assert len(a["x"]) == len(b["x"]), (len(a["x"]), len(b["x"]))
     for k in ("element", "stage", "raynum"):
         assert np.array_equal(a[k], b[k]), k
+    scale = max(float(np.max(np.abs(b[k]))) for k in ("x", "y", "z")) if len(b["x"]) else 0.0
     for k in ("x", "y", "z"):
-        tol = pos_tol + rel_tol * np.abs(b[k])
+        tol = pos_tol + rel_tol * scale
         d = np.abs(a[k] - b[k])
-        assert np.all(d <= tol), (k, float(d.max()))
+        assert np.all(d <= tol), (k, float(d.max()), tol)
     dtol = pos_tol if dir_tol is None else dir_tol
     for k in ("cx", "cy", "cz"):
         d = np.abs(a[k] - b[k])
