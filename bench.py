@@ -337,6 +337,8 @@ def main():
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(last["h2d_bytes"]),
                 "d2h_bytes_per_step": int(last["d2h_bytes"]), "ms_per_step": wall_ms / len(runs)},
         "gpu_launches": int(launches),
+        "autotuned_variants": {"probe": runs[-1]["probe_variant"], "trace": runs[-1]["trace_variant"],
+                               "fp64_trace": runs64[-1]["trace_variant"]},
         "units_per_step": units / len(runs), "sun_rays_per_step": sun_rays / len(runs),
         "roofline": roofline, "clocks": clk.summary(), "cpu_baseline": cpu,
     }

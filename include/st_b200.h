@@ -64,6 +64,7 @@ typedef struct st_b200_stats {
     int gpu_launches;                     /* kernels launched by the run */
     unsigned long long h2d_bytes;         /* host -> device bytes copied by the run */
     unsigned long long d2h_bytes;         /* device -> host bytes copied by the run */
+    int probe_variant, trace_variant;     /* autotuned kernel variants used */
 } st_b200_stats;
 int st_b200_run_stats(st_context_t pcxt, st_b200_stats *out);
 

@@ -907,7 +907,16 @@ __device__ __forceinline__ bool element_test(const SceneDev &S, const ElemRec &e
 // delta*sqrt(u), a table sunshape inverts the CDF of theta*I(theta), the diffuse
 // distribution is asin(sqrt(u)); phi is an independent uniform as in the reference.
 // ------------------------------------------------------------------------------------
-__device__ inline double sample_theta(int dist, double delop, double u, const SunDev &sun, bool sunshape) {
+// table sunshape: theta(u) tabulated at u = j / kSunInvCells, linear in between (mrad -> rad)
+__device__ __forceinline__ double sample_table(const SunDev &sun, double u) {
+    if (sun.inv_cdf == nullptr) return 0.0;  // no table was given (st_sun_userdata)
+    const double x = u * kSunInvCells;
+    const int j = min(int(x), kSunInvCells - 1);
+    const double f = x - j;
+    return (sun.inv_cdf[j] + f * (sun.inv_cdf[j + 1] - sun.inv_cdf[j])) / 1000.0;
+}
+
+__device__ __forceinline__ double sample_theta(int dist, double delop, double u, const SunDev &sun) {
     switch (dist) {
         case 'g':
         case 'G':
@@ -916,20 +925,32 @@ __device__ inline double sample_theta(int dist, double delop, double u, const Su
         case 'P':
             return delop * sqrt(u);
         case 'd':
-        case 'D': {
-            (void)sunshape;
-            if (sun.inv_cdf == nullptr) return 0.0;  // no table was given (st_sun_userdata)
-            // theta(u) tabulated at u = j / kSunInvCells, linear in between
-            const double x = u * kSunInvCells;
-            const int j = min(int(x), kSunInvCells - 1);
-            const double f = x - j;
-            return (sun.inv_cdf[j] + f * (sun.inv_cdf[j + 1] - sun.inv_cdf[j])) / 1000.0;
-        }
+        case 'D':
+            return sample_table(sun, u);
         case 'f':
         case 'F':
             return asin(sqrt(u));
         default:
             return 0.0;
+    }
+}
+
+__device__ __forceinline__ float sample_theta_f(int dist, float delop, double u, const SunDev &sun) {
+    switch (dist) {
+        case 'g':
+        case 'G':
+            return delop * sqrtf(-2.f * __logf(float(1.0 - u)));  // 1 - u in double: never 0
+        case 'p':
+        case 'P':
+            return delop * sqrtf(float(u));
+        case 'd':
+        case 'D':
+            return float(sample_table(sun, u));
+        case 'f':
+        case 'F':
+            return asinf(sqrtf(float(u)));
+        default:
+            return 0.f;
     }
 }
 

@@ -758,7 +758,7 @@ bool sun_setup(Context *cx, HostScene &hs) {
     // = projected origin, radius = accept radius) overlaps a cell is listed there
     sd.grid_on = 0;
     hs.cell_start.assign(2, 0);
-    hs.cell_items.clear();
+    hs.cell_disc.clear();
     if (!sun.point_source && st.elems.size() >= 4) {
         bool bounded = true;
         double rmax = 0;
@@ -799,19 +799,28 @@ bool sun_setup(Context *cx, HostScene &hs) {
                         if (ddx * ddx + ddy * ddy <= pad * pad) cells[size_t(gy) * nx + gx].push_back(int(j));
                     }
             }
-            hs.disc.assign(st.elems.size(), float4{0.f, 0.f, 0.f, 0.f});
+            std::vector<float4> disc(st.elems.size());
             for (size_t j = 0; j < st.elems.size(); ++j) {
                 // float disc for the probe's pre-test: radius widened by the float rounding
                 // of centre and ray coordinates (~1e-7 relative)
                 const double pad = rad[j] * (1.0 + 1e-9) + 1e-6 * (1.0 + fabs(cx_[j]) + fabs(cy_[j]));
                 const double fr = pad + 4e-7 * (fabs(cx_[j]) + fabs(cy_[j]) + fabs(sun.xmin) + fabs(sun.xmax) +
                                                 fabs(sun.ymin) + fabs(sun.ymax) + pad);
-                hs.disc[j] = float4{float(cx_[j]), float(cy_[j]), float(fr), 0.f};
+                int bits;
+                const int jj = int(j);
+                memcpy(&bits, &jj, 4);
+                float w;
+                memcpy(&w, &bits, 4);
+                disc[j] = float4{float(cx_[j]), float(cy_[j]), float(fr), w};
             }
-            hs.cell_start.assign(size_t(nx) * ny + 1, 0);
+            // (start, end) pair per cell: cell c at [2c, 2c + 1], read on the device as one int2
+            hs.cell_start.assign(2 * size_t(nx) * ny, 0);
+            int at = 0;
             for (size_t c = 0; c < cells.size(); ++c) {
-                hs.cell_start[c + 1] = hs.cell_start[c] + int(cells[c].size());
-                hs.cell_items.insert(hs.cell_items.end(), cells[c].begin(), cells[c].end());
+                hs.cell_start[2 * c] = at;
+                for (int j : cells[c]) hs.cell_disc.push_back(disc[j]);
+                at += int(cells[c].size());
+                hs.cell_start[2 * c + 1] = at;
             }
             sd.grid_on = 1;
             sd.gnx = nx;
@@ -1076,6 +1085,8 @@ int run(Context *cx, unsigned seed) {
     S.gpu_launches = rr.gpu_launches;
     S.h2d_bytes = rr.h2d_bytes;
     S.d2h_bytes = rr.d2h_bytes;
+    S.probe_variant = rr.probe_variant;
+    S.trace_variant = rr.trace_variant;
     if (rr.flags & 1u) cx->log("warning: a ray reached the limit of intersections per stage; it was stopped there");
     const auto ta = std::chrono::steady_clock::now();
     if (cx->want_records) assemble_records(cx, rr);

@@ -18,9 +18,9 @@ struct HostScene {
     std::vector<double> surf_data, tables;
     std::vector<BvhNode> bvh;
     std::vector<int> bvh_items;
-    std::vector<int> cell_start, cell_items;
+    std::vector<int> cell_start;
+    std::vector<float4> cell_disc;  // sun-plane grid entries: disc centre x, y, radius, element
     std::vector<double> inv_cdf;  // table-sunshape inverse CDF (kSunInvCells + 1 entries)
-    std::vector<float4> disc;     // first-stage projected bounding discs (sun-plane grid)
     SceneDev dev;  // stages, sun scalars and flags; device pointers are filled by gpu_run
 };
 
@@ -58,6 +58,7 @@ struct RunResult {
     int batches = 0, gpu_launches = 0;
     unsigned flags = 0;
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
+    int probe_variant = 0, trace_variant = 0;
 };
 
 struct Workspace;

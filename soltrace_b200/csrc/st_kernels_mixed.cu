@@ -3,23 +3,48 @@
 #include "st_trace_impl.cuh"
 
 namespace stb {
+// Register-budget variants (same code, different __launch_bounds__ minimum blocks per
+// SM): kProbeMinBlocks / kTraceMinBlocks in st_launch.h; the autotuner picks one.
 void launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
-                       const RunState *rs, cudaStream_t st) {
+                       const RunState *rs, int variant, cudaStream_t st) {
     const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;
-    k_probe<1><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs);
+    if (S.sun.grid_on && !S.explicit_rays && !S.sun.point_source) {
+        switch (variant) {
+            case 1: k_probe_grid<1, kProbeMinBlocks[1]><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs); break;
+            case 2: k_probe_grid<1, kProbeMinBlocks[2]><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs); break;
+            default: k_probe_grid<1, kProbeMinBlocks[0]><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs);
+        }
+    } else {
+        k_probe<1><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs);
+    }
+}
+
+template <int R, int V>
+static void trace_one(const SceneDev &S, const uint64_t *a, const uint32_t *b, const uint32_t *c, const uint32_t *t,
+                      RunState *rs, const TraceOut &O, uint32_t blocks, cudaStream_t st) {
+    k_trace<1, R, kTraceMinBlocks[V]><<<blocks, kTraceBlock, 0, st>>>(S, a, b, c, t, rs, O);
 }
 void launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
                        const uint32_t *hit_idx, const uint32_t *total, RunState *rs, const TraceOut &O,
-                       uint32_t blocks, cudaStream_t st) {
-    if (records)
-        k_trace<1, 1><<<blocks, kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs, O);
-    else
-        k_trace<1, 0><<<blocks, kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs, O);
+                       uint32_t blocks, int variant, cudaStream_t st) {
+    using Fn = void (*)(const SceneDev &, const uint64_t *, const uint32_t *, const uint32_t *, const uint32_t *,
+                        RunState *, const TraceOut &, uint32_t, cudaStream_t);
+    static const Fn table[2][kTraceVariants] = {{trace_one<0, 0>, trace_one<0, 1>, trace_one<0, 2>},
+                                                 {trace_one<1, 0>, trace_one<1, 1>, trace_one<1, 2>}};
+    table[records ? 1 : 0][(variant >= 0 && variant < kTraceVariants) ? variant : 0](S, hit_sid, hit_el, hit_idx, total, rs,
+                                                                                    O, blocks, st);
 }
-// resident trace blocks per SM, from this instantiation's register and shared-memory use
-int trace_blocks_per_sm_mixed(bool records) {
+
+// resident trace blocks per SM of a variant, from its register and shared-memory use
+int trace_blocks_per_sm_mixed(bool records, int variant) {
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, records ? k_trace<1, 1> : k_trace<1, 0>, kTraceBlock, 0);
+    const void *k;
+    switch (variant) {
+        case 1: k = records ? (const void *)k_trace<1, 1, kTraceMinBlocks[1]> : (const void *)k_trace<1, 0, kTraceMinBlocks[1]>; break;
+        case 2: k = records ? (const void *)k_trace<1, 1, kTraceMinBlocks[2]> : (const void *)k_trace<1, 0, kTraceMinBlocks[2]>; break;
+        default: k = records ? (const void *)k_trace<1, 1, kTraceMinBlocks[0]> : (const void *)k_trace<1, 0, kTraceMinBlocks[0]>;
+    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kTraceBlock, 0);
     return nb > 0 ? nb : 1;
 }
 }  // namespace stb

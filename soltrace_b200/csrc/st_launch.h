@@ -9,6 +9,12 @@ namespace stb {
 
 constexpr int kProbeBlock = 256;
 constexpr int kTraceBlock = 128;
+// register-budget variants of the probe and trace kernels (minimum resident blocks per
+// SM given to __launch_bounds__); all compute the same results
+constexpr int kProbeVariants = 3;
+constexpr int kProbeMinBlocks[kProbeVariants] = {1, 3, 4};
+constexpr int kTraceVariants = 3;
+constexpr int kTraceMinBlocks[kTraceVariants] = {1, 4, 5};
 
 enum RunFlags : unsigned {
     kFlagHitCap = 1u,         // a ray reached kMaxHitsPerStage in one stage
@@ -47,17 +53,17 @@ struct TraceOut {
 
 
 void launch_probe_fp64(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
-                       const RunState *rs, cudaStream_t st);
+                       const RunState *rs, int variant, cudaStream_t st);
 void launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
-                        const RunState *rs, cudaStream_t st);
+                        const RunState *rs, int variant, cudaStream_t st);
 // grid-stride trace over min(*total, target - hits_done) numbered rays; `blocks`
 // is the grid size (0 = enough blocks for `max_n` rays)
 void launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
                        const uint32_t *hit_idx, const uint32_t *total, RunState *rs, const TraceOut &O,
-                       uint32_t blocks, cudaStream_t st);
+                       uint32_t blocks, int variant, cudaStream_t st);
 void launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
                         const uint32_t *hit_idx, const uint32_t *total, RunState *rs, const TraceOut &O,
-                        uint32_t blocks, cudaStream_t st);
+                        uint32_t blocks, int variant, cudaStream_t st);
 // counting sort of the batch's hits by first-stage element (n_elem0 buckets)
 void launch_sort_by_element(const uint32_t *total, const uint64_t *hit_sid, const uint32_t *hit_el, uint32_t n_elem0,
                             uint32_t *elem_count, uint32_t *elem_cursor, uint32_t *scratch_total, uint64_t *s_sid,
@@ -67,6 +73,6 @@ void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uin
                     const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st);
 void launch_advance(const uint32_t *total, const uint64_t *hit_sid, uint64_t s0, uint32_t n, RunState *rs,
                     cudaStream_t st);
-int trace_blocks_per_sm_fp64(bool records);
-int trace_blocks_per_sm_mixed(bool records);
+int trace_blocks_per_sm_fp64(bool records, int variant);
+int trace_blocks_per_sm_mixed(bool records, int variant);
 }  // namespace stb

@@ -56,10 +56,16 @@ cudaError_t upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s, uint64_t 
 struct Workspace {
     int device = -1;
     cudaStream_t stream = nullptr;
-    DevBuf elems, optics, surf, tables, bvh, bvh_items, cell_start, cell_items, inv_cdf, disc, expos, excos;
+    DevBuf elems, optics, surf, tables, bvh, bvh_items, cell_start, cell_disc, inv_cdf, expos, excos;
     DevBuf acc, ctr, rs, rec_count, hit_elem, counts, offsets, total, hit_sid, hit_el, recs;
     DevBuf ecount, ecursor, etotal, s_sid, s_el, s_idx;
     std::vector<cudaEvent_t> events;
+    // autotuned kernel variants per precision (FP64, mixed), chosen on the first run
+    struct Tuning {
+        bool done = false;
+        int probe = 0, trace = 0;
+    } tune[2];
+    DevBuf tune_rs, tune_ctr, tune_acc;
     ~Workspace() {
         if (device >= 0) cudaSetDevice(device);
         for (auto e : events) cudaEventDestroy(e);
@@ -76,6 +82,111 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 }
 
 }  // namespace
+
+// Autotuner: time every register-budget variant of the probe and of the trace kernel on
+// the same 2^21 sun rays (indices 0.., outputs discarded into scratch buffers) and keep
+// the fastest of each for this workspace and precision.  Variants share their arithmetic,
+// so the choice changes timing only.
+static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, uint64_t max_sun, int dev_sms,
+                            cudaStream_t st, DevBuf &hit_elem, DevBuf &counts, DevBuf &offsets, DevBuf &total,
+                            DevBuf &hit_sid, DevBuf &hit_el, DevBuf &ecount, DevBuf &ecursor, DevBuf &etotal,
+                            DevBuf &s_sid, DevBuf &s_el, DevBuf &s_idx, bool sort_hits, uint32_t n_elem0, size_t ne,
+                            int &launches) {
+    Workspace::Tuning &tu = ws.tune[precision ? 1 : 0];
+    const uint64_t n = std::min<uint64_t>(uint64_t(1) << 21, max_sun);
+    if (n == 0) return cudaSuccess;
+    const uint32_t nb = uint32_t((n + kProbeBlock - 1) / kProbeBlock);
+    cudaError_t e;
+    if ((e = hit_elem.ensure(n * 4)) || (e = counts.ensure(size_t(nb) * 4)) || (e = offsets.ensure(size_t(nb) * 4)) ||
+        (e = total.ensure(8)) || (e = hit_sid.ensure(n * 8)) || (e = hit_el.ensure(n * 4)) ||
+        (e = ws.tune_rs.ensure(sizeof(RunState))) || (e = ws.tune_ctr.ensure(sizeof(RunCounters))) ||
+        (e = ws.tune_acc.ensure(std::max<size_t>(3 * ne, 1) * 8)))
+        return e;
+    if (sort_hits && ((e = s_sid.ensure(n * 8)) || (e = s_el.ensure(n * 4)) || (e = s_idx.ensure(n * 4)))) return e;
+    SceneDev S = S0;
+    S.n_flux = 0;
+    RunState r0;
+    memset(&r0, 0, sizeof r0);
+    r0.target = ~0ull;
+    RunState *rs = ws.tune_rs.as<RunState>();
+    TraceOut O;
+    memset(&O, 0, sizeof O);
+    O.ctr = ws.tune_ctr.as<RunCounters>();
+    unsigned long long *acc = ws.tune_acc.as<unsigned long long>();
+    O.first_hits = acc;
+    O.absorbed = acc + ne;
+    O.delivered = acc + 2 * ne;
+    O.rec_count = nullptr;
+    cudaMemcpyAsync(rs, &r0, sizeof r0, cudaMemcpyHostToDevice, st);
+    cudaEvent_t ev[2 * (kProbeVariants + kTraceVariants) + 2];
+    for (auto &x : ev) cudaEventCreate(&x);
+    auto probe = [&](int v) {
+        if (precision)
+            launch_probe_mixed(S, 0, uint32_t(n), hit_elem.as<uint32_t>(), counts.as<uint32_t>(), rs, v, st);
+        else
+            launch_probe_fp64(S, 0, uint32_t(n), hit_elem.as<uint32_t>(), counts.as<uint32_t>(), rs, v, st);
+        launches++;
+    };
+    probe(0);  // warm the caches
+    for (int v = 0; v < kProbeVariants; ++v) {
+        cudaEventRecord(ev[2 * v], st);
+        probe(v);
+        cudaEventRecord(ev[2 * v + 1], st);
+    }
+    launch_offsets(counts.as<uint32_t>(), nb, offsets.as<uint32_t>(), total.as<uint32_t>(), st);
+    launch_compact(0, uint32_t(n), hit_elem.as<uint32_t>(), counts.as<uint32_t>(), offsets.as<uint32_t>(),
+                   hit_sid.as<uint64_t>(), hit_el.as<uint32_t>(), st);
+    launches += 2;
+    const uint64_t *t_sid = hit_sid.as<uint64_t>();
+    const uint32_t *t_el = hit_el.as<uint32_t>(), *t_idx = nullptr;
+    if (sort_hits) {
+        launch_sort_by_element(total.as<uint32_t>(), hit_sid.as<uint64_t>(), hit_el.as<uint32_t>(), n_elem0,
+                               ecount.as<uint32_t>(), ecursor.as<uint32_t>(), etotal.as<uint32_t>(),
+                               s_sid.as<uint64_t>(), s_el.as<uint32_t>(), s_idx.as<uint32_t>(), uint32_t(n), st);
+        launches += 3;
+        t_sid = s_sid.as<uint64_t>();
+        t_el = s_el.as<uint32_t>();
+        t_idx = s_idx.as<uint32_t>();
+    }
+    const int base = 2 * kProbeVariants;
+    for (int v = -1; v < kTraceVariants; ++v) {
+        const int vv = v < 0 ? 0 : v;  // v = -1 warms the caches
+        const int per_sm = precision ? trace_blocks_per_sm_mixed(false, vv) : trace_blocks_per_sm_fp64(false, vv);
+        cudaMemsetAsync(&rs->cursor, 0, sizeof(unsigned), st);
+        if (v >= 0) cudaEventRecord(ev[base + 2 * v], st);
+        if (precision)
+            launch_trace_mixed(false, S, t_sid, t_el, t_idx, total.as<uint32_t>(), rs, O, uint32_t(dev_sms * per_sm), vv, st);
+        else
+            launch_trace_fp64(false, S, t_sid, t_el, t_idx, total.as<uint32_t>(), rs, O, uint32_t(dev_sms * per_sm), vv, st);
+        launches++;
+        if (v >= 0) cudaEventRecord(ev[base + 2 * v + 1], st);
+    }
+    e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) {
+        float best = 1e30f;
+        for (int v = 0; v < kProbeVariants; ++v) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev[2 * v], ev[2 * v + 1]);
+            if (ms < best * 0.98f) {
+                best = ms;
+                tu.probe = v;
+            }
+        }
+        best = 1e30f;
+        for (int v = 0; v < kTraceVariants; ++v) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev[base + 2 * v], ev[base + 2 * v + 1]);
+            if (ms < best * 0.98f) {
+                best = ms;
+                tu.trace = v;
+            }
+        }
+        tu.done = true;
+    }
+    for (auto &x : ev) cudaEventDestroy(x);
+    return e;
+}
 
 #define CK(x)                                                                                 \
     do {                                                                                      \
@@ -106,8 +217,8 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     if (!ws.stream) CK(cudaStreamCreateWithFlags(&ws.stream, cudaStreamNonBlocking));
     cudaStream_t st = ws.stream;
     DevBuf &d_elems = ws.elems, &d_optics = ws.optics, &d_surf = ws.surf, &d_tables = ws.tables, &d_bvh = ws.bvh,
-           &d_bvh_items = ws.bvh_items, &d_cell_start = ws.cell_start, &d_cell_items = ws.cell_items,
-           &d_inv_cdf = ws.inv_cdf, &d_disc = ws.disc, &d_expos = ws.expos, &d_excos = ws.excos;
+           &d_bvh_items = ws.bvh_items, &d_cell_start = ws.cell_start, &d_cell_disc = ws.cell_disc,
+           &d_inv_cdf = ws.inv_cdf, &d_expos = ws.expos, &d_excos = ws.excos;
     CK(upload(d_elems, hs.elems, st, out.h2d_bytes));
     CK(upload(d_optics, hs.optics, st, out.h2d_bytes));
     CK(upload(d_surf, hs.surf_data, st, out.h2d_bytes));
@@ -115,9 +226,8 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     CK(upload(d_bvh, hs.bvh, st, out.h2d_bytes));
     CK(upload(d_bvh_items, hs.bvh_items, st, out.h2d_bytes));
     CK(upload(d_cell_start, hs.cell_start, st, out.h2d_bytes));
-    CK(upload(d_cell_items, hs.cell_items, st, out.h2d_bytes));
+    CK(upload(d_cell_disc, hs.cell_disc, st, out.h2d_bytes));
     CK(upload(d_inv_cdf, hs.inv_cdf, st, out.h2d_bytes));
-    CK(upload(d_disc, hs.disc, st, out.h2d_bytes));
     CK(upload(d_expos, rq.ex_pos, st, out.h2d_bytes));
     CK(upload(d_excos, rq.ex_cos, st, out.h2d_bytes));
 
@@ -129,9 +239,8 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     S.bvh = d_bvh.as<BvhNode>();
     S.bvh_items = d_bvh_items.as<int>();
     S.sun.cell_start = d_cell_start.as<int>();
-    S.sun.cell_items = d_cell_items.as<int>();
+    S.sun.cell_disc = d_cell_disc.as<float4>();
     S.sun.inv_cdf = hs.inv_cdf.empty() ? nullptr : d_inv_cdf.as<double>();
-    S.sun.disc = d_disc.as<float4>();
     S.seed = rq.seed;
     S.precision = rq.precision;
     const bool explicit_mode = !rq.ex_pos.empty();
@@ -154,8 +263,6 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     }
     int dev_sms = 148;
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, rq.device);
-    const int per_sm = rq.precision ? trace_blocks_per_sm_mixed(rq.records) : trace_blocks_per_sm_fp64(rq.records);
-    const uint32_t trace_grid = uint32_t(dev_sms * per_sm);
 
     const int nst = S.n_stages;
     const uint64_t kMaxBatch = uint64_t(1) << 25;
@@ -174,6 +281,16 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
         CK(d_etotal.ensure(8));
     }
     unsigned long long rec_cap = 0;
+    Workspace::Tuning &tu = ws.tune[rq.precision ? 1 : 0];
+    if (!tu.done && !explicit_mode)
+        CK(autotune(ws, S, rq.precision, rq.max_sun, dev_sms, st, d_hit_elem, d_counts, d_offsets, d_total, d_hit_sid,
+                    d_hit_el, d_ecount, d_ecursor, d_etotal, d_s_sid, d_s_el, d_s_idx, sort_hits, n_elem0, ne,
+                    out.gpu_launches));
+    out.probe_variant = tu.probe;
+    out.trace_variant = tu.trace;
+    const int per_sm = rq.precision ? trace_blocks_per_sm_mixed(rq.records, tu.trace)
+                                    : trace_blocks_per_sm_fp64(rq.records, tu.trace);
+    const uint32_t trace_grid = uint32_t(dev_sms * per_sm);
     CK(cudaStreamSynchronize(st));
     out.setup_ms = ms_since(t_setup);
 
@@ -286,9 +403,11 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 cudaEvent_t p0 = new_event(), p1 = new_event(), p2 = new_event();
                 CK(cudaEventRecord(p0, st));
                 if (rq.precision)
-                    launch_probe_mixed(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(), drs, st);
+                    launch_probe_mixed(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(), drs,
+                                       tu.probe, st);
                 else
-                    launch_probe_fp64(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(), drs, st);
+                    launch_probe_fp64(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(), drs,
+                                      tu.probe, st);
                 launch_offsets(d_counts.as<uint32_t>(), nb, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), st);
                 launch_compact(sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(),
                                d_offsets.as<uint32_t>(), d_hit_sid.as<uint64_t>(), d_hit_el.as<uint32_t>(), st);
@@ -306,9 +425,11 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 }
                 CK(cudaEventRecord(p1, st));
                 if (rq.precision)
-                    launch_trace_mixed(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(), drs, O, trace_grid, st);
+                    launch_trace_mixed(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(), drs, O, trace_grid,
+                                       tu.trace, st);
                 else
-                    launch_trace_fp64(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(), drs, O, trace_grid, st);
+                    launch_trace_fp64(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(), drs, O, trace_grid,
+                                      tu.trace, st);
                 CK(cudaEventRecord(p2, st));
                 launch_advance(d_total.as<uint32_t>(), d_hit_sid.as<uint64_t>(), sun_next, uint32_t(n), drs, st);
                 CK(cudaGetLastError());

@@ -103,9 +103,9 @@ struct SunDev {
     // sun-plane culling grid for the first stage (cells over the sun box)
     int grid_on, gnx, gny;
     double gx0, gy0, ginv;          // origin and 1/cell size
-    const int *cell_start;          // gnx*gny + 1
-    const int *cell_items;          // element indices (stage-local), ascending per cell
-    const float4 *disc;             // per first-stage element: projected centre x, y and radius
+    const int *cell_start;          // (start, end) per cell: cell c at [2c, 2c+1], read as int2
+    const float4 *cell_disc;        // per cell entry, ascending element order: projected
+                                    // centre x, y, radius, element index (int bits)
 };
 
 struct SceneDev {

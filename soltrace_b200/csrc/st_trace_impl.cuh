@@ -132,18 +132,18 @@ __device__ inline int nearest_sun_grid(const SceneDev &S, const StageRec &st, co
     cx = min(max(cx, 0), sun.gnx - 1);
     cy = min(max(cy, 0), sun.gny - 1);
     const int c = cy * sun.gnx + cx;
-    const int a = sun.cell_start[c], b = sun.cell_start[c + 1];
+    const int2 range = reinterpret_cast<const int2 *>(sun.cell_start)[c];  // (start, end) of cell c
     int best = -1;
     double bp = 1e99;
     const float fx = float(xs), fy = float(ys);
-    for (int k = a; k < b; ++k) {
-        const int j = sun.cell_items[k];
-        // the ray can only meet element j inside its projected bounding disc (the disc the
-        // grid was built from, already padded for rounding): a float test before the
-        // double-precision element transform
-        const float4 d = sun.disc[j];
+    for (int k = range.x; k < range.y; ++k) {
+        // cell entry: the element's projected bounding disc (centre, radius padded for
+        // rounding) and its index; the ray can only meet the element inside the disc, a
+        // float test before the double-precision element transform
+        const float4 d = sun.cell_disc[k];
         const float dx = fx - d.x, dy = fy - d.y;
         if (dx * dx + dy * dy > d.z * d.z) continue;
+        const int j = __float_as_int(d.w);
         const ElemRec &e = S.elems[st.first_elem + j];
         if (!e.enabled) continue;
         double pl;
@@ -241,33 +241,15 @@ __device__ inline void refract(const OpticRec &op, const double cin[3], const do
 // error sample about `axis` (sunshape: source 1; specularity: source 2 with the
 // reflection re-draw of errors.cpp:222-225)
 template <int MIXED>
-__device__ inline void error_sample(const SceneDev &S, int dist, double delop, bool sunshape, const double axis[3],
-                             RayRng &rng, bool redraw_below, const double nrm[3], double out[3]) {
+__device__ inline void error_sample(const SceneDev &S, int dist, double delop, const double axis[3], RayRng &rng,
+                                    bool redraw_below, const double nrm[3], double out[3]) {
     for (unsigned call = 0;; ++call) {
         const double ut = rng.u();
         const double up = rng.u();
         if (MIXED) {
-            float th;
-            switch (dist) {
-                case 'g':
-                case 'G':
-                    th = float(delop) * sqrtf(-2.f * __logf(float(1.0 - ut)));  // 1 - u in double: never 0
-                    break;
-                case 'p':
-                case 'P':
-                    th = float(delop) * sqrtf(float(ut));
-                    break;
-                case 'f':
-                case 'F':
-                    th = asinf(sqrtf(float(ut)));
-                    break;
-                default:
-                    th = float(sample_theta(dist, delop, ut, S.sun, sunshape));
-            }
-            perturb<float>(axis, th, float(up) * 6.2831853f, out);
+            perturb<float>(axis, sample_theta_f(dist, float(delop), ut, S.sun), float(up) * 6.2831853f, out);
         } else {
-            const double th = sample_theta(dist, delop, ut, S.sun, sunshape);
-            perturb<double>(axis, th, up * 2.0 * 3.1415926535897932385, out);
+            perturb<double>(axis, sample_theta(dist, delop, ut, S.sun), up * 2.0 * 3.1415926535897932385, out);
         }
         if (!(redraw_below && out[0] * nrm[0] + out[1] * nrm[1] + out[2] * nrm[2] < 0 && call < 50000)) break;
     }
@@ -353,6 +335,38 @@ __global__ void __launch_bounds__(kProbeBlock) k_probe(SceneDev S, uint64_t s0, 
             b = nearest_sun_grid<MIXED>(S, st, ps, cs, xs, ys);
         else
             b = nearest<MIXED>(S, st, ps, cs);
+        h = (b >= 0) ? uint32_t(b + 1) : 0u;
+        hit_elem[i] = h;
+    }
+    const int c = __syncthreads_count(h != 0);
+    if (threadIdx.x == 0) block_counts[blockIdx.x] = uint32_t(c);
+}
+
+// Probe specialised to generated sun rays on a first stage culled by the sun-plane grid
+// (no BVH or explicit-ray code, so fewer registers and more resident warps).
+template <int MIXED, int MINB>
+__global__ void __launch_bounds__(kProbeBlock, MINB) k_probe_grid(SceneDev S, uint64_t s0, uint32_t n,
+                                                                   uint32_t *hit_elem, uint32_t *block_counts,
+                                                                   const RunState *rs) {
+    const uint32_t i = blockIdx.x * kProbeBlock + threadIdx.x;
+    uint32_t h = 0;
+    if (rs->reached) {
+        if (threadIdx.x == 0) block_counts[blockIdx.x] = 0;
+        return;
+    }
+    if (i < n) {
+        RayRng rng;
+        rng.init(S.seed, s0 + i, 0);
+        const SunDev &sun = S.sun;
+        const double xs = sun.xmin + (sun.xmax - sun.xmin) * rng.u();
+        const double ys = sun.ymin + (sun.ymax - sun.ymin) * rng.u();
+        const double psun[3] = {xs, ys, -10000.0}, csun[3] = {0.0, 0.0, 1.0};
+        double pst[3], cst[3], pg[3], cg[3], ps[3], cs[3];
+        to_ref(sun.Rsun, sun.pos_sun_stage, psun, csun, pst, cst);
+        const StageRec &st = S.stages[0];
+        to_ref(st.R, st.o, pst, cst, pg, cg);
+        to_local(st.R, st.o, pg, cg, ps, cs);
+        const int b = nearest_sun_grid<MIXED>(S, st, ps, cs, xs, ys);
         h = (b >= 0) ? uint32_t(b + 1) : 0u;
         hit_elem[i] = h;
     }
@@ -456,8 +470,8 @@ __global__ void k_advance(const uint32_t *total, const uint64_t *hit_sid, uint64
 }
 #endif  // ST_COMMON_KERNELS
 
-template <int MIXED, int RECORDS>
-__global__ void __launch_bounds__(kTraceBlock) k_trace(SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el,
+template <int MIXED, int RECORDS, int MINB>
+__global__ void __launch_bounds__(kTraceBlock, MINB) k_trace(SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el,
                                                         const uint32_t *hit_idx, const uint32_t *total,
                                                         RunState *rs, TraceOut O) {
     __shared__ unsigned long long sh_entries[kMaxStages];
@@ -545,7 +559,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(SceneDev S, const uint64_
                             double cin[3] = {h.ce[0], h.ce[1], h.ce[2]};
                             if (S.sunshape_on && si == 0 && hits == 1) {
                                 double c2[3];
-                                error_sample<MIXED>(S, S.sun.shape, S.sun.sigma / 1000.0, true, cin, rng, false, h.n, c2);
+                                error_sample<MIXED>(S, S.sun.shape, S.sun.sigma / 1000.0, cin, rng, false, h.n, c2);
                                 for (int q = 0; q < 3; ++q) cin[q] = c2[q];
                             }
                             double nrm[3] = {h.n[0], h.n[1], h.n[2]};
@@ -553,7 +567,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(SceneDev S, const uint64_
                                 double n2[3];
                                 const int d = op.dist;
                                 const int dd = (d == 'g' || d == 'G' || d == 'p' || d == 'P') ? d : 0;
-                                error_sample<MIXED>(S, dd, op.slope / 1000.0, false, nrm, rng, false, nrm, n2);
+                                error_sample<MIXED>(S, dd, op.slope / 1000.0, nrm, rng, false, nrm, n2);
                                 for (int q = 0; q < 3; ++q) nrm[q] = n2[q];
                             }
                             if (e.interaction == 1)
@@ -564,8 +578,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace(SceneDev S, const uint64_
                                 const bool diffuse = (op.dist == 'f' || op.dist == 'F');
                                 double axis[3], c3[3];
                                 for (int q = 0; q < 3; ++q) axis[q] = diffuse ? nrm[q] : cout[q];
-                                error_sample<MIXED>(S, op.dist, op.spec / 1000.0, false, axis, rng, e.interaction == 2, nrm,
-                                                    c3);
+                                error_sample<MIXED>(S, op.dist, op.spec / 1000.0, axis, rng, e.interaction == 2, nrm, c3);
                                 for (int q = 0; q < 3; ++q) cout[q] = c3[q];
                             }
                             for (int q = 0; q < 3; ++q) pout[q] = h.pe[q];

@@ -35,6 +35,8 @@ class Stats(C.Structure):
         ("gpu_launches", C.c_int),
         ("h2d_bytes", C.c_ulonglong),
         ("d2h_bytes", C.c_ulonglong),
+        ("probe_variant", C.c_int),
+        ("trace_variant", C.c_int),
     ]
 
 
