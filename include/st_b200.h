@@ -76,6 +76,26 @@ int st_b200_run_stats(st_context_t pcxt, st_b200_stats *out);
 int st_b200_element_counts(st_context_t pcxt, int stage, unsigned long long *first_hits,
                            unsigned long long *absorbed, unsigned long long *delivered);
 
+/* First-stage probe without device allocation.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: code running inside a framework that owns
+ * the device's memory pool, or a real-time loop in which an allocation (which may
+ * synchronise the whole device) is not allowed.  For the context's scene it traces sun
+ * rays [s0, s0 + n) (with the per-ray streams of `seed`, exactly as st_sim_run does)
+ * to the first stage and writes, in sun-ray order, the sun index and the 0-based
+ * element of every ray that hits into the caller's device arrays hit_sid and
+ * hit_elem (room for n entries each); *n_hits receives the count.  The k-th listed
+ * hit is the ray st_sim_run numbers k.  Arithmetic is FP64.
+ *
+ * Scene tables and scratch live in a 32 MiB static device array that every GPU
+ * loading this library keeps until the process exits; n <= 4194304 and scenes whose
+ * tables do not fit are rejected with -1 and a message.  The first call on a device
+ * looks up the array's address (make that call before any stream capture).  Calls
+ * share the array: calls that overlap on the GPU race.  `stream` is a cudaStream_t
+ * (NULL: the legacy default stream); the call returns after the work completes. */
+int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsigned long long s0, unsigned int n,
+                          unsigned long long *hit_sid, unsigned int *hit_elem, unsigned int *n_hits, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,6 +31,7 @@ UNITS = {
     "st_kernels_fp64.cu": ["-fmad=false"],
     "st_kernels_mixed.cu": [],
     "st_kernels_common.cu": [],
+    "st_noalloc.cu": [],
 }
 HEADERS = ["st_scene.h", "st_device.cuh", "st_trace_impl.cuh", "st_host.h", "st_launch.h"]
 

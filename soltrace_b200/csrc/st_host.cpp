@@ -1096,6 +1096,29 @@ int run(Context *cx, unsigned seed) {
 }
 
 Context *C(st_context_t p) { return reinterpret_cast<Context *>(p); }
+
+}  // namespace
+
+namespace stb {
+// Geometry set-up and flattening of a context's scene for callers outside this file;
+// on failure the reason is appended to the context's messages and false is returned.
+bool prepare_scene(void *ctx, HostScene &hs) {
+    Context *cx = C(ctx);
+    if (!cx) return false;
+    if (cx->stages.empty()) {
+        cx->log("no stages defined.");
+        return false;
+    }
+    if (!init_geometries(cx)) return false;
+    if (!flatten(cx, hs)) return false;
+    return true;
+}
+void report(void *ctx, const std::string &msg) {
+    if (C(ctx)) C(ctx)->log("%s", msg.c_str());
+}
+}  // namespace stb
+
+namespace {
 StageM *stage_of(Context *cx, st_uint_t i) { return i < cx->stages.size() ? &cx->stages[i] : nullptr; }
 Elem *elem_of(Context *cx, st_uint_t s, st_uint_t i) {
     StageM *st = stage_of(cx, s);

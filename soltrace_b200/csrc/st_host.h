@@ -66,4 +66,8 @@ Workspace *workspace_create();
 void workspace_destroy(Workspace *w);
 bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspace &ws);
 
+// st_host.cpp: set up and flatten the scene of a context; append a message to it
+bool prepare_scene(void *ctx, HostScene &hs);
+void report(void *ctx, const std::string &msg);
+
 }  // namespace stb
