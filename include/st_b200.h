@@ -87,7 +87,7 @@ int st_b200_element_counts(st_context_t pcxt, int stage, unsigned long long *fir
  * hit_elem (room for n entries each); *n_hits receives the count.  The k-th listed
  * hit is the ray st_sim_run numbers k.  Arithmetic is FP64.
  *
- * Scene tables and scratch live in a 32 MiB static device array that every GPU
+ * Scene tables and scratch live in a 48 MiB static device array that every GPU
  * loading this library keeps until the process exits; n <= 4194304 and scenes whose
  * tables do not fit are rejected with -1 and a message.  The first call on a device
  * looks up the array's address (make that call before any stream capture).  Calls

@@ -516,6 +516,8 @@ double accept_radius(const Elem &e) {
             rap = std::max(fabs(e.p[0]), fabs(e.p[1]));
             break;
         case 'l':
+            // x1 = x2 = 0 leaves x unbounded (intersect.cpp applies no x limit then)
+            if (e.p[0] == 0.0 && e.p[1] == 0.0) return -1.0;
             rap = sqrt(sq(std::max(fabs(e.p[0]), fabs(e.p[1]))) + sq(e.p[2] / 2.0));
             break;
         case 'i':
@@ -547,6 +549,62 @@ double accept_radius(const Elem &e) {
         return -1.0;
     }
     return sqrt(rap * rap + zext * zext) * (1.0 + 1e-9) + 1e-6;
+}
+
+// Element-local box [x0,x1] x [y0,y1] x [-hz,hz] holding every hit the trace can accept,
+// for elements whose accepted hits lie on a surface of bounded sag over the aperture
+// (flat, parabolic and spherical-cap sections); false otherwise.
+bool local_box(const Elem &e, double &x0, double &x1, double &y0, double &y1, double &hz) {
+    const double rb = accept_radius(e);
+    if (rb < 0) return false;
+    if (e.stype == 2 || e.stype == 10) return false;  // cylinder, torus: the radius bound only
+    const char sh = char(tolower(e.shape));
+    switch (sh) {
+        case 'r':
+            x0 = -e.p[0] / 2.0;
+            x1 = e.p[0] / 2.0;
+            y0 = -e.p[1] / 2.0;
+            y1 = e.p[1] / 2.0;
+            break;
+        case 'l':
+            x0 = std::min(e.p[0], e.p[1]);
+            x1 = std::max(e.p[0], e.p[1]);
+            y0 = -fabs(e.p[2]) / 2.0;
+            y1 = fabs(e.p[2]) / 2.0;
+            break;
+        case 'i':
+        case 'q':
+            x0 = y0 = 1e300;
+            x1 = y1 = -1e300;
+            for (int k = 0; k < (sh == 'q' ? 8 : 6); k += 2) {
+                x0 = std::min(x0, e.p[k]);
+                x1 = std::max(x1, e.p[k]);
+                y0 = std::min(y0, e.p[k + 1]);
+                y1 = std::max(y1, e.p[k + 1]);
+            }
+            break;
+        case 'a': {
+            const double ra = std::max(fabs(e.p[0]), fabs(e.p[1]));
+            x0 = y0 = -ra;
+            x1 = y1 = ra;
+            break;
+        }
+        default: {  // 'c', 'h', 't': inside the circle of diameter p0
+            const double ra = fabs(e.p[0]) / 2.0;
+            x0 = y0 = -ra;
+            x1 = y1 = ra;
+        }
+    }
+    // sag over the aperture, as accept_radius bounds it: 0 for flat elements, the paraboloid's
+    // z at the farthest aperture corner, ZAperture for spherical caps
+    const double rxy2 = std::max(sq(x0), sq(x1)) + std::max(sq(y0), sq(y1));
+    if (e.stype == 3)
+        hz = 0.0;
+    else if (tolower(e.surface) == 'p')
+        hz = 0.5 * std::max(fabs(e.vcx), fabs(e.vcy)) * rxy2 * (1.0 + 1e-9) + 1e-9;
+    else
+        hz = std::max(fabs(e.zap), 0.0) * (1.0 + 1e-9) + 1e-9;
+    return true;
 }
 
 // Median-split BVH over element bounding spheres (stage coordinates).
@@ -759,6 +817,7 @@ bool sun_setup(Context *cx, HostScene &hs) {
     sd.grid_on = 0;
     hs.cell_start.assign(2, 0);
     hs.cell_disc.clear();
+    hs.cell_par.clear();
     if (!sun.point_source && st.elems.size() >= 4) {
         bool bounded = true;
         double rmax = 0;
@@ -799,26 +858,74 @@ bool sun_setup(Context *cx, HostScene &hs) {
                         if (ddx * ddx + ddy * ddy <= pad * pad) cells[size_t(gy) * nx + gx].push_back(int(j));
                     }
             }
-            std::vector<float4> disc(st.elems.size());
+            // Per element a float disc (centre, radius) and a parallelogram about the same
+            // centre for the probe's pre-tests; both contain every sun-plane point whose ray can
+            // be accepted by the element.
+            //
+            // Parallelogram: the projection (along the sun's z) of the element's local box lies
+            // inside the parallelogram spanned from the projected box centre by the projected
+            // half-axes ax = hx P(X), ay = hy P(Y), widened by the projected half sag
+            // az = hz P(Z): with (u, v) = [ax ay]^-1 q, a point q of the footprint has
+            // |u| <= 1 + |uz| and |v| <= 1 + |vz| where (uz, vz) = [ax ay]^-1 az.  Near edge-on
+            // elements, and surfaces without a box, keep the disc alone (rows all zero).
+            //
+            // Disc: the radius is widened by the float rounding of centre and ray coordinates
+            // (~1e-7 relative) and by the distance from the projected origin to the centre.
+            std::vector<float4> disc(st.elems.size()), par(st.elems.size(), float4{0.f, 0.f, 0.f, 0.f});
+            const double box_ext = fabs(sun.xmin) + fabs(sun.xmax) + fabs(sun.ymin) + fabs(sun.ymax);
             for (size_t j = 0; j < st.elems.size(); ++j) {
-                // float disc for the probe's pre-test: radius widened by the float rounding
-                // of centre and ray coordinates (~1e-7 relative)
-                const double pad = rad[j] * (1.0 + 1e-9) + 1e-6 * (1.0 + fabs(cx_[j]) + fabs(cy_[j]));
-                const double fr = pad + 4e-7 * (fabs(cx_[j]) + fabs(cy_[j]) + fabs(sun.xmin) + fabs(sun.xmax) +
-                                                fabs(sun.ymin) + fabs(sun.ymax) + pad);
+                const Elem &e = st.elems[j];
+                double ccx = cx_[j], ccy = cy_[j];
+                double x0, x1, y0, y1, hz;
+                if (local_box(e, x0, x1, y0, y1, hz)) {
+                    const double pad = 1e-3 + 2e-6 * (1.0 + fabs(cx_[j]) + fabs(cy_[j]) + box_ext + rad[j]);
+                    const double hx = (x1 - x0) / 2.0 + pad, hy = (y1 - y0) / 2.0 + pad, hzz = hz + pad;
+                    const double lx = (x0 + x1) / 2.0, ly = (y0 + y1) / 2.0;
+                    double c3[3], ax3[3], ay3[3], az3[3], c2[3], a2[3], b2[3], z2[3];
+                    for (int q = 0; q < 3; ++q) {
+                        c3[q] = e.origin[q] + lx * e.R[q] + ly * e.R[3 + q];
+                        ax3[q] = hx * e.R[q];
+                        ay3[q] = hy * e.R[3 + q];
+                        az3[q] = hzz * e.R[6 + q];
+                    }
+                    mulv(Rs, c3, c2);
+                    mulv(Rs, ax3, a2);
+                    mulv(Rs, ay3, b2);
+                    mulv(Rs, az3, z2);
+                    const double det = a2[0] * b2[1] - a2[1] * b2[0];
+                    const double la = sqrt(sq(a2[0]) + sq(a2[1])), lb = sqrt(sq(b2[0]) + sq(b2[1]));
+                    if (fabs(det) > 1e-3 * la * lb) {  // not within ~0.06 deg of edge-on
+                        const double i00 = b2[1] / det, i01 = -b2[0] / det, i10 = -a2[1] / det, i11 = a2[0] / det;
+                        const double uz = i00 * z2[0] + i01 * z2[1], vz = i10 * z2[0] + i11 * z2[1];
+                        // limits widened for the float evaluation of (u, v): 1e-5, plus 1e-6 of the
+                        // largest term a row can produce over the parallelogram (skewed footprints)
+                        const double Q = 2.0 * (la + lb + sqrt(sq(z2[0]) + sq(z2[1]))) + 1.0;
+                        const double lu = (1.0 + fabs(uz)) * (1.0 + 1e-5) + 1e-6 * (fabs(i00) + fabs(i01)) * Q;
+                        const double lv = (1.0 + fabs(vz)) * (1.0 + 1e-5) + 1e-6 * (fabs(i10) + fabs(i11)) * Q;
+                        par[j] = float4{float(i00 / lu), float(i01 / lu), float(i10 / lv), float(i11 / lv)};
+                        ccx = c2[0];
+                        ccy = c2[1];
+                    }
+                }
+                const double shift = sqrt(sq(ccx - cx_[j]) + sq(ccy - cy_[j]));
+                const double pad = rad[j] * (1.0 + 1e-9) + 1e-6 * (1.0 + fabs(cx_[j]) + fabs(cy_[j])) + shift;
+                const double fr = pad + 4e-7 * (fabs(ccx) + fabs(ccy) + box_ext + pad);
                 int bits;
                 const int jj = int(j);
                 memcpy(&bits, &jj, 4);
                 float w;
                 memcpy(&w, &bits, 4);
-                disc[j] = float4{float(cx_[j]), float(cy_[j]), float(fr), w};
+                disc[j] = float4{float(ccx), float(ccy), float(fr), w};
             }
             // (start, end) pair per cell: cell c at [2c, 2c + 1], read on the device as one int2
             hs.cell_start.assign(2 * size_t(nx) * ny, 0);
             int at = 0;
             for (size_t c = 0; c < cells.size(); ++c) {
                 hs.cell_start[2 * c] = at;
-                for (int j : cells[c]) hs.cell_disc.push_back(disc[j]);
+                for (int j : cells[c]) {
+                    hs.cell_disc.push_back(disc[j]);
+                    hs.cell_par.push_back(par[j]);
+                }
                 at += int(cells[c].size());
                 hs.cell_start[2 * c + 1] = at;
             }
@@ -894,6 +1001,13 @@ bool flatten(Context *cx, HostScene &hs) {
             r.rs = e.rs;
             r.area = e.area;
             r.bound_r = accept_radius(e);
+            {
+                // float bounding sphere for the BVH leaf pre-test: 1 mm plus 1e-6 of the centre's
+                // coordinates on top of the exact radius; unbounded elements always pass
+                const double cmax = std::max(fabs(e.origin[0]), std::max(fabs(e.origin[1]), fabs(e.origin[2])));
+                const float w = r.bound_r < 0 ? 3.0e38f : float(r.bound_r * (1.0 + 1e-6) + 1e-3 + 1e-6 * cmax);
+                hs.elem_sphere.push_back(make_float4(float(e.origin[0]), float(e.origin[1]), float(e.origin[2]), w));
+            }
             r.shape = tolower(e.shape);
             r.surf = e.surface;
             r.stype = e.stype;

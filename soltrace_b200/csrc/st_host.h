@@ -19,7 +19,9 @@ struct HostScene {
     std::vector<BvhNode> bvh;
     std::vector<int> bvh_items;
     std::vector<int> cell_start;
+    std::vector<float4> elem_sphere;  // per element: origin (stage coordinates), padded bounding radius
     std::vector<float4> cell_disc;  // sun-plane grid entries: disc centre x, y, radius, element
+    std::vector<float4> cell_par;   // sun-plane grid entries: footprint parallelogram (dual basis rows)
     std::vector<double> inv_cdf;  // table-sunshape inverse CDF (kSunInvCells + 1 entries)
     SceneDev dev;  // stages, sun scalars and flags; device pointers are filled by gpu_run
 };

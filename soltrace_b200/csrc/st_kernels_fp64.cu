@@ -7,18 +7,35 @@
 namespace stb {
 // Register-budget variants (same code, different __launch_bounds__ minimum blocks per
 // SM): kProbeMinBlocks / kTraceMinBlocks in st_launch.h; the autotuner picks one.
-void launch_probe_fp64(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
-                       const RunState *rs, int variant, cudaStream_t st) {
+template <int V>
+static void resolve_one(const SceneDev &S, uint64_t s0, uint32_t *hit_elem, uint32_t *block_counts,
+                        const uint32_t *cand, const uint32_t *cand_count, const RunState *rs, cudaStream_t st) {
+    // persistent grid: every resident block of the variant on every SM
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sun_resolve<0, kProbeMinBlocks[V]>, kResolveBlock, 0);
+        per_sm = per_sm > 0 ? per_sm : 1;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    k_sun_resolve<0, kProbeMinBlocks[V]><<<sms * per_sm, kResolveBlock, 0, st>>>(S, s0, hit_elem, block_counts, cand,
+                                                                                 cand_count, rs);
+}
+int launch_probe_fp64(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
+                  uint32_t *cand, uint32_t *cand_count, const RunState *rs, int variant, cudaStream_t st) {
     const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;
     if (S.sun.grid_on && !S.explicit_rays && !S.sun.point_source) {
+        launch_sun_candidates(S, s0, n, hit_elem, block_counts, cand, cand_count, rs, st);
         switch (variant) {
-            case 1: k_probe_grid<0, kProbeMinBlocks[1]><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs); break;
-            case 2: k_probe_grid<0, kProbeMinBlocks[2]><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs); break;
-            default: k_probe_grid<0, kProbeMinBlocks[0]><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs);
+            case 1: resolve_one<1>(S, s0, hit_elem, block_counts, cand, cand_count, rs, st); break;
+            case 2: resolve_one<2>(S, s0, hit_elem, block_counts, cand, cand_count, rs, st); break;
+            default: resolve_one<0>(S, s0, hit_elem, block_counts, cand, cand_count, rs, st);
         }
-    } else {
-        k_probe<0><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs);
+        return 2;
     }
+    k_probe<0><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs);
+    return 1;
 }
 
 template <int R, int V>

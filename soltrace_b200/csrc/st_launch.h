@@ -8,11 +8,12 @@
 namespace stb {
 
 constexpr int kProbeBlock = 256;
+constexpr int kResolveBlock = 128;  // threads per block of the grid probe's element-test kernel
 constexpr int kTraceBlock = 128;
 // register-budget variants of the probe and trace kernels (minimum resident blocks per
 // SM given to __launch_bounds__); all compute the same results
 constexpr int kProbeVariants = 3;
-constexpr int kProbeMinBlocks[kProbeVariants] = {1, 3, 4};
+constexpr int kProbeMinBlocks[kProbeVariants] = {4, 6, 8};
 constexpr int kTraceVariants = 3;
 constexpr int kTraceMinBlocks[kTraceVariants] = {1, 4, 5};
 
@@ -52,10 +53,16 @@ struct TraceOut {
 };
 
 
-void launch_probe_fp64(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
-                       const RunState *rs, int variant, cudaStream_t st);
-void launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
-                        const RunState *rs, int variant, cudaStream_t st);
+// First-stage probe of sun rays [s0, s0 + n): hit_elem[i] = element + 1 or 0, and the hit
+// count of every kProbeBlock rays.  `cand` (room for n entries) and `cand_count` are
+// scratch of the grid probe.  Returns the number of kernels launched.
+int launch_probe_fp64(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
+                      uint32_t *cand, uint32_t *cand_count, const RunState *rs, int variant, cudaStream_t st);
+int launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
+                       uint32_t *cand, uint32_t *cand_count, const RunState *rs, int variant, cudaStream_t st);
+// first kernel of the grid probe (shared by both precisions)
+void launch_sun_candidates(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
+                           uint32_t *cand, uint32_t *cand_count, const RunState *rs, cudaStream_t st);
 // grid-stride trace over min(*total, target - hits_done) numbered rays; `blocks`
 // is the grid size (0 = enough blocks for `max_n` rays)
 void launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,

@@ -4,7 +4,7 @@
 // device allocation (which can synchronise the device) is not allowed.
 //
 // Scene tables and per-call scratch live in one file-scope device array of
-// kNoAllocBytes (32 MiB).  Every GPU that loads this library holds that array until
+// kNoAllocBytes (48 MiB).  Every GPU that loads this library holds that array until
 // the process exits; all calls share it and it keeps the last call's contents, so
 // everything that must start at zero is cleared by each call, and calls that overlap
 // on the GPU (from different host threads or on different streams) race.
@@ -19,7 +19,7 @@
 namespace stb {
 namespace {
 
-constexpr size_t kNoAllocBytes = size_t(32) << 20;
+constexpr size_t kNoAllocBytes = size_t(48) << 20;
 constexpr uint32_t kNoAllocMaxRays = uint32_t(1) << 22;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
@@ -102,12 +102,15 @@ extern "C" int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsig
     const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;
     Carve cv{scratch};
     ElemRec *d_elems = cv.take<ElemRec>(hs.elems.size());
+    float4 *d_sphere = cv.take<float4>(hs.elem_sphere.size());
     double *d_surf = cv.take<double>(hs.surf_data.size());
     BvhNode *d_bvh = cv.take<BvhNode>(hs.bvh.size());
     int *d_bvh_items = cv.take<int>(hs.bvh_items.size());
     int *d_cells = cv.take<int>(hs.cell_start.size());
     float4 *d_cdisc = cv.take<float4>(hs.cell_disc.size());
+    float4 *d_cpar = cv.take<float4>(hs.cell_par.size());
     uint32_t *d_hit_elem = cv.take<uint32_t>(n);
+    uint32_t *d_cand = cv.take<uint32_t>(size_t(n) + 1);  // probe candidate count, then list
     uint32_t *d_counts = cv.take<uint32_t>(nb);
     uint32_t *d_offsets = cv.take<uint32_t>(nb);
     uint32_t *d_total = cv.take<uint32_t>(2);
@@ -120,11 +123,13 @@ extern "C" int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsig
     }
     SceneDev S = hs.dev;
     S.elems = d_elems;
+    S.elem_sphere = d_sphere;
     S.surf_data = d_surf;
     S.bvh = d_bvh;
     S.bvh_items = d_bvh_items;
     S.sun.cell_start = d_cells;
     S.sun.cell_disc = d_cdisc;
+    S.sun.cell_par = d_cpar;
     S.sun.inv_cdf = nullptr;
     S.optics = nullptr;
     S.tables = nullptr;
@@ -135,15 +140,17 @@ extern "C" int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsig
     RunState r0;
     memset(&r0, 0, sizeof r0);
     r0.target = ~0ull;  // no cut-off: every hit of the range is listed
-    if ((e = put(d_elems, hs.elems, st)) != cudaSuccess || (e = put(d_surf, hs.surf_data, st)) != cudaSuccess ||
+    if ((e = put(d_elems, hs.elems, st)) != cudaSuccess || (e = put(d_sphere, hs.elem_sphere, st)) != cudaSuccess ||
+        (e = put(d_surf, hs.surf_data, st)) != cudaSuccess ||
         (e = put(d_bvh, hs.bvh, st)) != cudaSuccess || (e = put(d_bvh_items, hs.bvh_items, st)) != cudaSuccess ||
         (e = put(d_cells, hs.cell_start, st)) != cudaSuccess || (e = put(d_cdisc, hs.cell_disc, st)) != cudaSuccess ||
+        (e = put(d_cpar, hs.cell_par, st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(d_rs, &r0, sizeof r0, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
         (e = cudaMemsetAsync(d_total, 0, 8, st)) != cudaSuccess) {
         report(pcxt, std::string("st_b200_probe_noalloc: ") + cudaGetErrorString(e));
         return -1;
     }
-    launch_probe_fp64(S, s0, n, d_hit_elem, d_counts, d_rs, 0, st);
+    launch_probe_fp64(S, s0, n, d_hit_elem, d_counts, d_cand + 1, d_cand, d_rs, 0, st);
     launch_offsets(d_counts, nb, d_offsets, d_total, st);
     launch_compact(s0, n, d_hit_elem, d_counts, d_offsets, reinterpret_cast<uint64_t *>(hit_sid), hit_elem, st);
     uint32_t total = 0;

@@ -56,8 +56,10 @@ cudaError_t upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s, uint64_t 
 struct Workspace {
     int device = -1;
     cudaStream_t stream = nullptr;
-    DevBuf elems, optics, surf, tables, bvh, bvh_items, cell_start, cell_disc, inv_cdf, expos, excos;
+    DevBuf elems, elem_sphere, optics, surf, tables, bvh, bvh_items, cell_start, cell_disc, cell_par, inv_cdf, expos,
+        excos;
     DevBuf acc, ctr, rs, rec_count, hit_elem, counts, offsets, total, hit_sid, hit_el, recs;
+    DevBuf cand;  // grid probe's candidate list: count, then one sun-ray index per entry
     DevBuf ecount, ecursor, etotal, s_sid, s_el, s_idx;
     std::vector<cudaEvent_t> events;
     // autotuned kernel variants per precision (FP64, mixed), chosen on the first run
@@ -100,7 +102,7 @@ static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, ui
     if ((e = hit_elem.ensure(n * 4)) || (e = counts.ensure(size_t(nb) * 4)) || (e = offsets.ensure(size_t(nb) * 4)) ||
         (e = total.ensure(8)) || (e = hit_sid.ensure(n * 8)) || (e = hit_el.ensure(n * 4)) ||
         (e = ws.tune_rs.ensure(sizeof(RunState))) || (e = ws.tune_ctr.ensure(sizeof(RunCounters))) ||
-        (e = ws.tune_acc.ensure(std::max<size_t>(3 * ne, 1) * 8)))
+        (e = ws.tune_acc.ensure(std::max<size_t>(3 * ne, 1) * 8)) || (e = ws.cand.ensure((n + 1) * 4)))
         return e;
     if (sort_hits && ((e = s_sid.ensure(n * 8)) || (e = s_el.ensure(n * 4)) || (e = s_idx.ensure(n * 4)))) return e;
     SceneDev S = S0;
@@ -120,12 +122,14 @@ static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, ui
     cudaMemcpyAsync(rs, &r0, sizeof r0, cudaMemcpyHostToDevice, st);
     cudaEvent_t ev[2 * (kProbeVariants + kTraceVariants) + 2];
     for (auto &x : ev) cudaEventCreate(&x);
+    uint32_t *cand_count = ws.cand.as<uint32_t>(), *cand = cand_count + 1;
     auto probe = [&](int v) {
         if (precision)
-            launch_probe_mixed(S, 0, uint32_t(n), hit_elem.as<uint32_t>(), counts.as<uint32_t>(), rs, v, st);
+            launches += launch_probe_mixed(S, 0, uint32_t(n), hit_elem.as<uint32_t>(), counts.as<uint32_t>(), cand,
+                                           cand_count, rs, v, st);
         else
-            launch_probe_fp64(S, 0, uint32_t(n), hit_elem.as<uint32_t>(), counts.as<uint32_t>(), rs, v, st);
-        launches++;
+            launches += launch_probe_fp64(S, 0, uint32_t(n), hit_elem.as<uint32_t>(), counts.as<uint32_t>(), cand,
+                                          cand_count, rs, v, st);
     };
     probe(0);  // warm the caches
     for (int v = 0; v < kProbeVariants; ++v) {
@@ -220,6 +224,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
            &d_bvh_items = ws.bvh_items, &d_cell_start = ws.cell_start, &d_cell_disc = ws.cell_disc,
            &d_inv_cdf = ws.inv_cdf, &d_expos = ws.expos, &d_excos = ws.excos;
     CK(upload(d_elems, hs.elems, st, out.h2d_bytes));
+    CK(upload(ws.elem_sphere, hs.elem_sphere, st, out.h2d_bytes));
     CK(upload(d_optics, hs.optics, st, out.h2d_bytes));
     CK(upload(d_surf, hs.surf_data, st, out.h2d_bytes));
     CK(upload(d_tables, hs.tables, st, out.h2d_bytes));
@@ -227,12 +232,14 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     CK(upload(d_bvh_items, hs.bvh_items, st, out.h2d_bytes));
     CK(upload(d_cell_start, hs.cell_start, st, out.h2d_bytes));
     CK(upload(d_cell_disc, hs.cell_disc, st, out.h2d_bytes));
+    CK(upload(ws.cell_par, hs.cell_par, st, out.h2d_bytes));
     CK(upload(d_inv_cdf, hs.inv_cdf, st, out.h2d_bytes));
     CK(upload(d_expos, rq.ex_pos, st, out.h2d_bytes));
     CK(upload(d_excos, rq.ex_cos, st, out.h2d_bytes));
 
     SceneDev S = hs.dev;
     S.elems = d_elems.as<ElemRec>();
+    S.elem_sphere = ws.elem_sphere.as<float4>();
     S.optics = d_optics.as<OpticRec>();
     S.surf_data = d_surf.as<double>();
     S.tables = d_tables.as<double>();
@@ -240,6 +247,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     S.bvh_items = d_bvh_items.as<int>();
     S.sun.cell_start = d_cell_start.as<int>();
     S.sun.cell_disc = d_cell_disc.as<float4>();
+    S.sun.cell_par = ws.cell_par.as<float4>();
     S.sun.inv_cdf = hs.inv_cdf.empty() ? nullptr : d_inv_cdf.as<double>();
     S.seed = rq.seed;
     S.precision = rq.precision;
@@ -402,12 +410,14 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 O.rec_cap = rq.records ? rec_cap : 0;
                 cudaEvent_t p0 = new_event(), p1 = new_event(), p2 = new_event();
                 CK(cudaEventRecord(p0, st));
+                CK(ws.cand.ensure((n + 1) * 4));
+                uint32_t *cand_count = ws.cand.as<uint32_t>(), *cand = cand_count + 1;
                 if (rq.precision)
-                    launch_probe_mixed(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(), drs,
-                                       tu.probe, st);
+                    out.gpu_launches += launch_probe_mixed(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(),
+                                                           d_counts.as<uint32_t>(), cand, cand_count, drs, tu.probe, st);
                 else
-                    launch_probe_fp64(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(), drs,
-                                      tu.probe, st);
+                    out.gpu_launches += launch_probe_fp64(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(),
+                                                          d_counts.as<uint32_t>(), cand, cand_count, drs, tu.probe, st);
                 launch_offsets(d_counts.as<uint32_t>(), nb, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), st);
                 launch_compact(sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(),
                                d_offsets.as<uint32_t>(), d_hit_sid.as<uint64_t>(), d_hit_el.as<uint32_t>(), st);
@@ -433,7 +443,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 CK(cudaEventRecord(p2, st));
                 launch_advance(d_total.as<uint32_t>(), d_hit_sid.as<uint64_t>(), sun_next, uint32_t(n), drs, st);
                 CK(cudaGetLastError());
-                out.gpu_launches += 5;
+                out.gpu_launches += 4;  // offsets, compact, trace, advance
                 probe_ev.push_back({p0, p1});
                 trace_ev.push_back({p1, p2});
                 queued += n;

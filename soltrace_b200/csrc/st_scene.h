@@ -106,10 +106,14 @@ struct SunDev {
     const int *cell_start;          // (start, end) per cell: cell c at [2c, 2c+1], read as int2
     const float4 *cell_disc;        // per cell entry, ascending element order: projected
                                     // centre x, y, radius, element index (int bits)
+    const float4 *cell_par;         // per cell entry: rows (a, b), (c, d) of the footprint's
+                                    // dual basis; (x, y) about the centre is kept when
+                                    // |a x + b y| <= 1 and |c x + d y| <= 1 (all zero: disc only)
 };
 
 struct SceneDev {
     const ElemRec *elems;
+    const float4 *elem_sphere;  // per element: origin in stage coordinates and padded bounding radius
     const OpticRec *optics;
     const double *surf_data;
     const double *tables;

@@ -14,6 +14,7 @@
 // Splitting off the probe keeps the trace kernel's warps full: the sun rays that
 // miss everything (most of them on a heliostat field) never enter it.
 #pragma once
+#include <climits>
 #include "st_device.cuh"
 #include "st_launch.h"
 
@@ -78,11 +79,16 @@ __device__ inline int nearest_brute(const SceneDev &S, const StageRec &st, const
 // skipped (the test is on the entry distance minus the 1e-5 nudge, with slack for
 // the float box arithmetic).
 template <int MIXED>
-__device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3]) {
+__device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3],
+                                  int from) {
     const BvhNode *nodes = S.bvh + st.bvh_off;
     const int *items = S.bvh_items + st.bvh_items_off;
     const float ox = float(ps[0]), oy = float(ps[1]), oz = float(ps[2]);
-    const float ix = 1.0f / float(cs[0]), iy = 1.0f / float(cs[1]), iz = 1.0f / float(cs[2]);
+    const float dx = float(cs[0]), dy = float(cs[1]), dz = float(cs[2]);
+    // 1/d with zero components replaced by a tiny signed value, so slab products are never 0*inf
+    const float ix = 1.0f / (fabsf(dx) > 1e-30f ? dx : copysignf(1e-30f, dx));
+    const float iy = 1.0f / (fabsf(dy) > 1e-30f ? dy : copysignf(1e-30f, dy));
+    const float iz = 1.0f / (fabsf(dz) > 1e-30f ? dz : copysignf(1e-30f, dz));
     int stack[48];
     int sp = 0;
     stack[sp++] = 0;
@@ -101,6 +107,17 @@ __device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const d
         if (nd.count > 0) {
             for (int k = 0; k < nd.count; ++k) {
                 const int j = items[nd.first + k];
+                // the flat element the ray is leaving, when its test certainly fails
+                if (j == from) continue;
+                // float pre-test against the element's bounding sphere: the sphere must reach
+                // the ray ahead of its origin.  The radius is padded for the float rounding of
+                // centre, origin and direction (2e-6 of the L1 norms, over ten times the bound).
+                const float4 bs = S.elem_sphere[st.first_elem + j];
+                const float vx = bs.x - ox, vy = bs.y - oy, vz = bs.z - oz;
+                const float tc = vx * dx + vy * dy + vz * dz;
+                const float wx = vx - tc * dx, wy = vy - tc * dy, wz = vz - tc * dz;
+                const float rr = bs.w + 2e-6f * (fabsf(ox) + fabsf(oy) + fabsf(oz) + fabsf(vx) + fabsf(vy) + fabsf(vz));
+                if (tc < -rr || wx * wx + wy * wy + wz * wz > rr * rr) continue;
                 const ElemRec &e = S.elems[st.first_elem + j];
                 if (!e.enabled) continue;
                 double pl;
@@ -118,34 +135,64 @@ __device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const d
 }
 
 template <int MIXED>
-__device__ __forceinline__ int nearest(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3]) {
-    return (st.bvh_off >= 0) ? nearest_bvh<MIXED>(S, st, ps, cs) : nearest_brute<MIXED>(S, st, ps, cs);
+__device__ __forceinline__ int nearest(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3],
+                                       int from = -1) {
+    return (st.bvh_off >= 0) ? nearest_bvh<MIXED>(S, st, ps, cs, from) : nearest_brute<MIXED>(S, st, ps, cs);
 }
 
 // first test of a first-stage sun ray through the sun-plane grid (cells list the
 // elements, ascending, whose bounding disc in the sun plane overlaps the cell)
-template <int MIXED>
-__device__ inline int nearest_sun_grid(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3],
-                                double xs, double ys) {
+// The first-stage ray of sun-frame point (xs, ys), as the reference builds it: sun frame ->
+// stage -> global (generateray.cpp:151-159), then global -> stage (raytrace.cpp:625-627).
+__device__ __forceinline__ void sun_ray_in_stage(const SceneDev &S, double xs, double ys, double ps[3], double cs[3]) {
     const SunDev &sun = S.sun;
+    const StageRec &st = S.stages[0];
+    const double psun[3] = {xs, ys, -10000.0}, csun[3] = {0.0, 0.0, 1.0};
+    double pst[3], cst[3], pg[3], cg[3];
+    to_ref(sun.Rsun, sun.pos_sun_stage, psun, csun, pst, cst);
+    to_ref(st.R, st.o, pst, cst, pg, cg);
+    to_local(st.R, st.o, pg, cg, ps, cs);
+}
+
+// Float pre-test of sun-plane point (fx, fy) against grid entry k: inside the padded disc
+// and the padded footprint parallelogram (both contain every point whose ray the element
+// can accept, so a rejected entry is one the double-precision test rejects too).
+__device__ __forceinline__ bool sun_entry_pass(const SunDev &sun, int k, float fx, float fy) {
+    const float4 d = sun.cell_disc[k];
+    const float qx = fx - d.x, qy = fy - d.y;
+    if (qx * qx + qy * qy > d.z * d.z) return false;
+    const float4 p = sun.cell_par[k];
+    return fabsf(p.x * qx + p.y * qy) <= 1.0f && fabsf(p.z * qx + p.w * qy) <= 1.0f;
+}
+
+// Cell of the sun-plane grid holding point (xs, ys): its entry range [x, y).
+__device__ __forceinline__ int2 sun_cell(const SunDev &sun, double xs, double ys) {
     int cx = int(floor((xs - sun.gx0) * sun.ginv)), cy = int(floor((ys - sun.gy0) * sun.ginv));
     cx = min(max(cx, 0), sun.gnx - 1);
     cy = min(max(cy, 0), sun.gny - 1);
-    const int c = cy * sun.gnx + cx;
-    const int2 range = reinterpret_cast<const int2 *>(sun.cell_start)[c];  // (start, end) of cell c
+    return reinterpret_cast<const int2 *>(sun.cell_start)[cy * sun.gnx + cx];
+}
+
+// Sun-ray probe through the grid for one ray; the double-precision ray is built only once
+// a cell entry passes the float pre-test.
+template <int MIXED>
+__device__ inline int nearest_sun_grid_lazy(const SceneDev &S, const StageRec &st, double xs, double ys) {
+    const SunDev &sun = S.sun;
+    const int2 range = sun_cell(sun, xs, ys);
     int best = -1;
     double bp = 1e99;
     const float fx = float(xs), fy = float(ys);
+    bool have_ray = false;
+    double ps[3], cs[3];
     for (int k = range.x; k < range.y; ++k) {
-        // cell entry: the element's projected bounding disc (centre, radius padded for
-        // rounding) and its index; the ray can only meet the element inside the disc, a
-        // float test before the double-precision element transform
-        const float4 d = sun.cell_disc[k];
-        const float dx = fx - d.x, dy = fy - d.y;
-        if (dx * dx + dy * dy > d.z * d.z) continue;
-        const int j = __float_as_int(d.w);
+        if (!sun_entry_pass(sun, k, fx, fy)) continue;
+        const int j = __float_as_int(sun.cell_disc[k].w);
         const ElemRec &e = S.elems[st.first_elem + j];
         if (!e.enabled) continue;
+        if (!have_ray) {
+            sun_ray_in_stage(S, xs, ys, ps, cs);
+            have_ray = true;
+        }
         double pl;
         if (element_test<MIXED>(S, e, ps, cs, pl, nullptr) && pl < bp) {
             bp = pl;
@@ -154,6 +201,7 @@ __device__ inline int nearest_sun_grid(const SceneDev &S, const StageRec &st, co
     }
     return best;
 }
+
 
 // ------------------------------------------------------------------------------------
 // optics (raytrace.cpp:885-946 test value; interaction.cpp:58-199)
@@ -269,6 +317,14 @@ __device__ __forceinline__ unsigned long long warp_reserve(unsigned long long *c
     return base + rank;
 }
 
+// add 1 to base[idx] for every active lane, one atomic per distinct idx in the warp (the
+// trace's warps mostly carry rays of one element, so their counters coincide)
+__device__ __forceinline__ void warp_count(unsigned long long *base, int idx) {
+    const unsigned mask = __activemask();
+    const unsigned peers = __match_any_sync(mask, idx);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&base[idx], (unsigned long long)__popc(peers));
+}
+
 template <int MIXED>
 __device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed, const double pe[3]) {
     for (int m = 0; m < S.n_flux; ++m) {
@@ -330,11 +386,9 @@ __global__ void __launch_bounds__(kProbeBlock) k_probe(SceneDev S, uint64_t s0, 
         const StageRec &st = S.stages[0];
         double ps[3], cs[3];
         to_local(st.R, st.o, pg, cg, ps, cs);
-        int b;
-        if (S.sun.grid_on && !S.explicit_rays && !S.sun.point_source)
-            b = nearest_sun_grid<MIXED>(S, st, ps, cs, xs, ys);
-        else
-            b = nearest<MIXED>(S, st, ps, cs);
+        (void)xs;
+        (void)ys;
+        const int b = nearest<MIXED>(S, st, ps, cs);
         h = (b >= 0) ? uint32_t(b + 1) : 0u;
         hit_elem[i] = h;
     }
@@ -342,39 +396,76 @@ __global__ void __launch_bounds__(kProbeBlock) k_probe(SceneDev S, uint64_t s0, 
     if (threadIdx.x == 0) block_counts[blockIdx.x] = uint32_t(c);
 }
 
-// Probe specialised to generated sun rays on a first stage culled by the sun-plane grid
-// (no BVH or explicit-ray code, so fewer registers and more resident warps).
+// Probe of generated sun rays on a first stage culled by the sun-plane grid, in two
+// kernels so that the double-precision work runs in full warps:
+//   k_sun_candidates (one thread per sun ray, few registers): draws the sun-plane point
+//     and runs the float pre-tests of its grid cell; a ray with no passing entry is a miss
+//     (its hit_elem is written here), the others are appended to a candidate list;
+//   k_sun_resolve (one thread per listed ray): redraws the point and runs the serial
+//     nearest-element search of the reference's loop over the first stage, writing
+//     hit_elem and the per-kProbeBlock hit counts.
+// On a heliostat field most sun rays miss every footprint and never reach the second
+// kernel, whose warps are then fully occupied by rays that need the element tests.
 template <int MIXED, int MINB>
-__global__ void __launch_bounds__(kProbeBlock, MINB) k_probe_grid(SceneDev S, uint64_t s0, uint32_t n,
-                                                                   uint32_t *hit_elem, uint32_t *block_counts,
-                                                                   const RunState *rs) {
-    const uint32_t i = blockIdx.x * kProbeBlock + threadIdx.x;
-    uint32_t h = 0;
-    if (rs->reached) {
-        if (threadIdx.x == 0) block_counts[blockIdx.x] = 0;
-        return;
+__global__ void __launch_bounds__(kResolveBlock, MINB) k_sun_resolve(SceneDev S, uint64_t s0, uint32_t *hit_elem,
+                                                                     uint32_t *block_counts, const uint32_t *cand,
+                                                                     const uint32_t *cand_count, const RunState *rs) {
+    if (rs->reached) return;
+    const uint32_t nc = *cand_count;
+    const SunDev &sun = S.sun;
+    for (uint32_t c = blockIdx.x * kResolveBlock + threadIdx.x; c < nc; c += gridDim.x * kResolveBlock) {
+        const uint32_t i = cand[c];
+        RayRng rng;
+        rng.init(S.seed, s0 + i, 0);
+        const double xs = sun.xmin + (sun.xmax - sun.xmin) * rng.u();
+        const double ys = sun.ymin + (sun.ymax - sun.ymin) * rng.u();
+        const int b = nearest_sun_grid_lazy<MIXED>(S, S.stages[0], xs, ys);
+        hit_elem[i] = (b >= 0) ? uint32_t(b + 1) : 0u;
+        if (b >= 0) {
+            // one atomic per distinct count slot among the warp's hitting lanes
+            const unsigned mask = __activemask();
+            const uint32_t slot = i / kProbeBlock;
+            const unsigned peers = __match_any_sync(mask, slot);
+            if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&block_counts[slot], uint32_t(__popc(peers)));
+        }
     }
+}
+
+#ifdef ST_COMMON_KERNELS
+// first kernel of the grid probe (above): misses written, candidates listed
+__global__ void __launch_bounds__(kProbeBlock) k_sun_candidates(SceneDev S, uint64_t s0, uint32_t n,
+                                                                uint32_t *hit_elem, uint32_t *block_counts,
+                                                                uint32_t *cand, uint32_t *cand_count,
+                                                                const RunState *rs) {
+    if (threadIdx.x == 0) block_counts[blockIdx.x] = 0;
+    if (rs->reached) return;  // the requested hits are numbered: this batch is surplus
+    const uint32_t i = blockIdx.x * kProbeBlock + threadIdx.x;
+    bool listed = false;
     if (i < n) {
         RayRng rng;
         rng.init(S.seed, s0 + i, 0);
         const SunDev &sun = S.sun;
         const double xs = sun.xmin + (sun.xmax - sun.xmin) * rng.u();
         const double ys = sun.ymin + (sun.ymax - sun.ymin) * rng.u();
-        const double psun[3] = {xs, ys, -10000.0}, csun[3] = {0.0, 0.0, 1.0};
-        double pst[3], cst[3], pg[3], cg[3], ps[3], cs[3];
-        to_ref(sun.Rsun, sun.pos_sun_stage, psun, csun, pst, cst);
-        const StageRec &st = S.stages[0];
-        to_ref(st.R, st.o, pst, cst, pg, cg);
-        to_local(st.R, st.o, pg, cg, ps, cs);
-        const int b = nearest_sun_grid<MIXED>(S, st, ps, cs, xs, ys);
-        h = (b >= 0) ? uint32_t(b + 1) : 0u;
-        hit_elem[i] = h;
+        const int2 range = sun_cell(sun, xs, ys);
+        const float fx = float(xs), fy = float(ys);
+        for (int k = range.x; k < range.y; ++k)
+            if (sun_entry_pass(sun, k, fx, fy)) {
+                listed = true;
+                break;
+            }
+        if (!listed) hit_elem[i] = 0;
     }
-    const int c = __syncthreads_count(h != 0);
-    if (threadIdx.x == 0) block_counts[blockIdx.x] = uint32_t(c);
+    const unsigned bal = __ballot_sync(0xffffffffu, listed);
+    if (bal != 0) {
+        const int lane = threadIdx.x & 31, leader = __ffs(bal) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(cand_count, uint32_t(__popc(bal)));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (listed) cand[base + __popc(bal & ((1u << lane) - 1u))] = i;
+    }
 }
 
-#ifdef ST_COMMON_KERNELS
 // exclusive scan of the per-block counts (one block; counts fit in 32 bits per batch)
 __global__ void __launch_bounds__(1024) k_offsets(const uint32_t *counts, uint32_t nb, uint32_t *offsets,
                                                    uint32_t *total) {
@@ -521,14 +612,21 @@ __global__ void __launch_bounds__(kTraceBlock, MINB) k_trace(SceneDev S, const u
         int first_elem0 = -1;  // the ray's first first-stage element (global index)
         for (int si = 0; si < S.n_stages; ++si) {
             const StageRec &st = S.stages[si];
-            atomicAdd(&sh_entries[si], 1ull);
-            atomicMax(&sh_max_enter[si], raynum);
+            {
+                const unsigned mask = __activemask();
+                const unsigned peers = __match_any_sync(mask, si);
+                const unsigned mx = __reduce_max_sync(peers, raynum);
+                if ((threadIdx.x & 31) == __ffs(peers) - 1) {
+                    atomicAdd(&sh_entries[si], (unsigned long long)__popc(peers));
+                    atomicMax(&sh_max_enter[si], mx);
+                }
+            }
             double ps[3], cs[3];
             to_local(st.R, st.o, pg, cg, ps, cs);
-            int hits = 0;
+            int hits = 0, last_j = -1;
             bool absorbed = false;
             for (;;) {
-                int j = (hits == 0 && known >= 0) ? known : nearest<MIXED>(S, st, ps, cs);
+                int j = (hits == 0 && known >= 0) ? known : nearest<MIXED>(S, st, ps, cs, last_j);
                 known = -1;
                 if (j < 0) break;
                 const ElemRec &e = S.elems[st.first_elem + j];
@@ -538,7 +636,7 @@ __global__ void __launch_bounds__(kTraceBlock, MINB) k_trace(SceneDev S, const u
                 if (!element_test<MIXED>(S, e, ps, cs, pl, &h)) break;
                 ++hits;
                 if (hits == 1) {
-                    atomicAdd(&O.first_hits[st.first_elem + j], 1ull);
+                    warp_count(O.first_hits, st.first_elem + j);
                     if (si == 0) first_elem0 = st.first_elem + j;
                 }
                 double pout[3], cout[3];
@@ -599,11 +697,20 @@ __global__ void __launch_bounds__(kTraceBlock, MINB) k_trace(SceneDev S, const u
                 }
                 if (S.n_flux) bin_flux<MIXED>(S, si, j, absorbed, h.pe);
                 if (absorbed) {
-                    atomicAdd(&O.absorbed[st.first_elem + j], 1ull);
-                    if (si == S.n_stages - 1 && first_elem0 >= 0) atomicAdd(&O.delivered[first_elem0], 1ull);
+                    warp_count(O.absorbed, st.first_elem + j);
+                    if (si == S.n_stages - 1 && first_elem0 >= 0) warp_count(O.delivered, first_elem0);
                     break;
                 }
                 to_ref(e.R, e.o, pout, cout, ps, cs);
+                // A flat element cannot meet the ray leaving it: the next test's 1e-5 nudge moves
+                // the origin 1e-5 |cz| off the plane, behind the ray.  Skipped only when that
+                // offset exceeds the round-off of the local z (1e-13 of the coordinates,
+                // hundreds of ulps), so the skipped test is one that fails.
+                last_j = (e.stype == kSurfFlat &&
+                          1e-5 * fabs(cout[2]) >
+                              1e-13 * (1.0 + fabs(e.o[0]) + fabs(e.o[1]) + fabs(e.o[2]) + fabs(pout[0]) + fabs(pout[1])))
+                             ? j
+                             : -1;
                 if (!st.multihit) break;
                 if (hits >= kMaxHitsPerStage) {
                     atomicOr(&sh_flags, unsigned(kFlagHitCap));
