@@ -516,8 +516,9 @@ double accept_radius(const Elem &e) {
             rap = std::max(fabs(e.p[0]), fabs(e.p[1]));
             break;
         case 'l':
-            // x1 = x2 = 0 leaves x unbounded (intersect.cpp applies no x limit then)
-            if (e.p[0] == 0.0 && e.p[1] == 0.0) return -1.0;
+            // x1 = x2 = 0 leaves x unbounded (intersect.cpp applies no x limit then): only the
+            // closed cylinder and torus below stay bounded
+            if (e.p[0] == 0.0 && e.p[1] == 0.0 && e.stype != 2 && e.stype != 10) return -1.0;
             rap = sqrt(sq(std::max(fabs(e.p[0]), fabs(e.p[1]))) + sq(e.p[2] / 2.0));
             break;
         case 'i':
@@ -604,6 +605,86 @@ bool local_box(const Elem &e, double &x0, double &x1, double &y0, double &y1, do
         hz = 0.5 * std::max(fabs(e.vcx), fabs(e.vcy)) * rxy2 * (1.0 + 1e-9) + 1e-9;
     else
         hz = std::max(fabs(e.zap), 0.0) * (1.0 + 1e-9) + 1e-9;
+    return true;
+}
+
+// Ground grid of a stage whose elements are spread over its x-y plane in a thin z band
+// (z extent at most a quarter of the x-y extent, every element bounded).  Cells are about
+// one element radius wide; an enabled element is listed in every cell its bounding disc,
+// padded by 1e-3 of a cell plus 1e-6 of the coordinates (float traversal), overlaps, with
+// its float bounding sphere beside it so that the walk reads one entry per element.  The z
+// band and the grid box carry the same padding.  Returns false (grid off) otherwise.
+bool build_ground_grid(const std::vector<Elem> &els, const float4 *sphere, StageRec &sr, std::vector<int2> &cells,
+                       std::vector<float4> &ent_sphere, std::vector<int> &ent_elem) {
+    const size_t n = els.size();
+    std::vector<double> rad(n);
+    double xlo = 1e300, xhi = -1e300, ylo = 1e300, yhi = -1e300, zlo = 1e300, zhi = -1e300;
+    for (size_t j = 0; j < n; ++j) {
+        const double r = accept_radius(els[j]);
+        if (r < 0) return false;
+        rad[j] = r;
+        const double *c = els[j].origin;
+        xlo = std::min(xlo, c[0] - r);
+        xhi = std::max(xhi, c[0] + r);
+        ylo = std::min(ylo, c[1] - r);
+        yhi = std::max(yhi, c[1] + r);
+        zlo = std::min(zlo, c[2] - r);
+        zhi = std::max(zhi, c[2] + r);
+    }
+    const double ext = std::max(xhi - xlo, yhi - ylo);
+    if (!(ext > 0) || (zhi - zlo) > 0.25 * ext) return false;
+    std::vector<double> rs = rad;
+    std::nth_element(rs.begin(), rs.begin() + n / 2, rs.end());
+    double cell = std::max(rs[n / 2], ext / 4096.0);
+    if (!(cell > 0)) return false;
+    const double big = std::max(std::max(fabs(xlo), fabs(xhi)), std::max(fabs(ylo), fabs(yhi)));
+    double gx0, gy0;
+    int nx, ny;
+    for (;;) {
+        const double m = 1e-3 * cell + 1e-6 * big + 1e-6 + 0.5 * cell;  // margin around the padded discs
+        gx0 = xlo - m;
+        gy0 = ylo - m;
+        nx = int(ceil((xhi - xlo + 2 * m) / cell)) + 1;
+        ny = int(ceil((yhi - ylo + 2 * m) / cell)) + 1;
+        if (double(nx) * ny <= 1.0e6) break;
+        cell *= 1.5;
+    }
+    std::vector<std::vector<int>> lists(size_t(nx) * ny);
+    for (size_t j = 0; j < n; ++j) {
+        if (!els[j].enabled) continue;
+        const double *c = els[j].origin;
+        const double pad = rad[j] * (1.0 + 1e-6) + 1e-3 * cell + 1e-6 * big + 1e-6;
+        const int x0 = std::max(0, int(floor((c[0] - pad - gx0) / cell)));
+        const int x1 = std::min(nx - 1, int(floor((c[0] + pad - gx0) / cell)));
+        const int y0 = std::max(0, int(floor((c[1] - pad - gy0) / cell)));
+        const int y1 = std::min(ny - 1, int(floor((c[1] + pad - gy0) / cell)));
+        for (int gy = y0; gy <= y1; ++gy)
+            for (int gx = x0; gx <= x1; ++gx) {
+                const double ax = gx0 + gx * cell, bx = ax + cell, ay = gy0 + gy * cell, by = ay + cell;
+                const double dx = std::max(std::max(ax - c[0], 0.0), c[0] - bx);
+                const double dy = std::max(std::max(ay - c[1], 0.0), c[1] - by);
+                if (dx * dx + dy * dy <= pad * pad) lists[size_t(gy) * nx + gx].push_back(int(j));
+            }
+    }
+    const double zpad = 1e-3 * (zhi - zlo) + 1e-3 + 1e-6 * std::max(fabs(zlo), fabs(zhi));
+    sr.grid_on = 1;
+    sr.gnx = nx;
+    sr.gny = ny;
+    sr.gcell_off = int(cells.size());
+    sr.gx0 = float(gx0);
+    sr.gy0 = float(gy0);
+    sr.gcell = float(cell);
+    sr.ginv = float(1.0 / cell);
+    sr.gzlo = float(zlo - zpad);
+    sr.gzhi = float(zhi + zpad);
+    for (const auto &l : lists) {
+        const int a = int(ent_elem.size());
+        for (int j : l) {
+            ent_elem.push_back(j);
+            ent_sphere.push_back(sphere[j]);
+        }
+        cells.push_back(int2{a, int(ent_elem.size())});
+    }
     return true;
 }
 
@@ -1040,6 +1121,10 @@ bool flatten(Context *cx, HostScene &hs) {
             }
             hs.elems.push_back(r);
         }
+        sr.grid_on = 0;
+        if (st.elems.size() >= 64)
+            build_ground_grid(st.elems, hs.elem_sphere.data() + sr.first_elem, sr, hs.stage_cells, hs.grid_sphere,
+                              hs.grid_elem);
         if (st.elems.size() >= 16) {
             sr.bvh_off = int(hs.bvh.size());
             sr.bvh_items_off = int(hs.bvh_items.size());

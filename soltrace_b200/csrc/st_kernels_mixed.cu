@@ -4,7 +4,7 @@
 
 namespace stb {
 // Register-budget variants (same code, different __launch_bounds__ minimum blocks per
-// SM): kProbeMinBlocks / kTraceMinBlocks in st_launch.h; the autotuner picks one.
+// SM): kProbeMinBlocks in st_launch.h; the autotuner picks one.
 template <int V>
 static void resolve_one(const SceneDev &S, uint64_t s0, uint32_t *hit_elem, uint32_t *block_counts,
                         const uint32_t *cand, const uint32_t *cand_count, const RunState *rs, cudaStream_t st) {
@@ -36,32 +36,10 @@ int launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit
     return 1;
 }
 
-template <int R, int V>
-static void trace_one(const SceneDev &S, const uint64_t *a, const uint32_t *b, const uint32_t *c, const uint32_t *t,
-                      RunState *rs, const TraceOut &O, uint32_t blocks, cudaStream_t st) {
-    k_trace<1, R, kTraceMinBlocks[V]><<<blocks, kTraceBlock, 0, st>>>(S, a, b, c, t, rs, O);
-}
-void launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
-                       const uint32_t *hit_idx, const uint32_t *total, RunState *rs, const TraceOut &O,
-                       uint32_t blocks, int variant, cudaStream_t st) {
-    using Fn = void (*)(const SceneDev &, const uint64_t *, const uint32_t *, const uint32_t *, const uint32_t *,
-                        RunState *, const TraceOut &, uint32_t, cudaStream_t);
-    static const Fn table[2][kTraceVariants] = {{trace_one<0, 0>, trace_one<0, 1>, trace_one<0, 2>},
-                                                 {trace_one<1, 0>, trace_one<1, 1>, trace_one<1, 2>}};
-    table[records ? 1 : 0][(variant >= 0 && variant < kTraceVariants) ? variant : 0](S, hit_sid, hit_el, hit_idx, total, rs,
-                                                                                    O, blocks, st);
-}
-
-// resident trace blocks per SM of a variant, from its register and shared-memory use
-int trace_blocks_per_sm_mixed(bool records, int variant) {
-    int nb = 0;
-    const void *k;
-    switch (variant) {
-        case 1: k = records ? (const void *)k_trace<1, 1, kTraceMinBlocks[1]> : (const void *)k_trace<1, 0, kTraceMinBlocks[1]>; break;
-        case 2: k = records ? (const void *)k_trace<1, 1, kTraceMinBlocks[2]> : (const void *)k_trace<1, 0, kTraceMinBlocks[2]>; break;
-        default: k = records ? (const void *)k_trace<1, 1, kTraceMinBlocks[0]> : (const void *)k_trace<1, 0, kTraceMinBlocks[0]>;
-    }
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kTraceBlock, 0);
-    return nb > 0 ? nb : 1;
+int launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
+                      const uint32_t *hit_idx, const uint32_t *total, const RunState *rs, const TraceOut &O,
+                      const WfState &W, const WfQueues &Q, cudaStream_t st) {
+    return records ? wf_launch<1, 1>(S, hit_sid, hit_el, hit_idx, total, rs, O, W, Q, st)
+                   : wf_launch<1, 0>(S, hit_sid, hit_el, hit_idx, total, rs, O, W, Q, st);
 }
 }  // namespace stb

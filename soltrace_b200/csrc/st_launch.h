@@ -14,8 +14,9 @@ constexpr int kTraceBlock = 128;
 // SM given to __launch_bounds__); all compute the same results
 constexpr int kProbeVariants = 3;
 constexpr int kProbeMinBlocks[kProbeVariants] = {4, 6, 8};
-constexpr int kTraceVariants = 3;
-constexpr int kTraceMinBlocks[kTraceVariants] = {1, 4, 5};
+// resident blocks per SM asked of the trace's shade and search kernels (register budget)
+constexpr int kWfShadeMinBlocks = 4;
+constexpr int kWfSearchMinBlocks = 6;
 
 enum RunFlags : unsigned {
     kFlagHitCap = 1u,         // a ray reached kMaxHitsPerStage in one stage
@@ -42,6 +43,28 @@ struct RunState {
     unsigned int cursor;           // trace work queue: next hit-list entry to hand out
 };
 
+// Per-ray state of the trace between its kernels, one slot per hit-list entry of a batch
+// (structure of arrays; component q of a vector at [q * cap + slot]).
+struct WfState {
+    uint64_t *sid;      // sun-ray index (random stream key)
+    uint32_t *raynum;
+    uint32_t *draw;     // next draw of the ray's random stream
+    int4 *meta;         // stage, hits in the stage, element left (flat, else -1), element to shade (-1)
+    int *fe0;           // the ray's first first-stage element (global index), -1 none
+    double *p, *c;      // position, direction: global while the stage has no hit yet, else stage frame
+    uint32_t cap;
+};
+
+// Queues of the trace: two search queues used in turn, one shade queue, and the counts
+// of every round (count 2r: search queue of round r, 2r + 1: its shade queue); the
+// launcher zeroes the counts.
+struct WfQueues {
+    uint32_t *search[2];
+    uint32_t *shade;
+    uint32_t *counts;  // 2 * rounds + 1 entries
+    int rounds;
+};
+
 struct TraceOut {
     RecordDev *recs;
     unsigned long long rec_cap;
@@ -63,14 +86,15 @@ int launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit
 // first kernel of the grid probe (shared by both precisions)
 void launch_sun_candidates(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
                            uint32_t *cand, uint32_t *cand_count, const RunState *rs, cudaStream_t st);
-// grid-stride trace over min(*total, target - hits_done) numbered rays; `blocks`
-// is the grid size (0 = enough blocks for `max_n` rays)
-void launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
-                       const uint32_t *hit_idx, const uint32_t *total, RunState *rs, const TraceOut &O,
-                       uint32_t blocks, int variant, cudaStream_t st);
-void launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
-                        const uint32_t *hit_idx, const uint32_t *total, RunState *rs, const TraceOut &O,
-                        uint32_t blocks, int variant, cudaStream_t st);
+// Trace of a batch's numbered rays (hit-list entries below the cut-off at the requested
+// hit count): the first kernel, `Q.rounds` rounds of search and shade kernels, and the
+// finishing kernel.  Returns the number of kernels launched.
+int launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
+                      const uint32_t *hit_idx, const uint32_t *total, const RunState *rs, const TraceOut &O,
+                      const WfState &W, const WfQueues &Q, cudaStream_t st);
+int launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
+                       const uint32_t *hit_idx, const uint32_t *total, const RunState *rs, const TraceOut &O,
+                       const WfState &W, const WfQueues &Q, cudaStream_t st);
 // counting sort of the batch's hits by first-stage element (n_elem0 buckets)
 void launch_sort_by_element(const uint32_t *total, const uint64_t *hit_sid, const uint32_t *hit_el, uint32_t n_elem0,
                             uint32_t *elem_count, uint32_t *elem_cursor, uint32_t *scratch_total, uint64_t *s_sid,
@@ -80,6 +104,4 @@ void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uin
                     const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st);
 void launch_advance(const uint32_t *total, const uint64_t *hit_sid, uint64_t s0, uint32_t n, RunState *rs,
                     cudaStream_t st);
-int trace_blocks_per_sm_fp64(bool records, int variant);
-int trace_blocks_per_sm_mixed(bool records, int variant);
 }  // namespace stb

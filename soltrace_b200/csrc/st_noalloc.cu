@@ -103,6 +103,9 @@ extern "C" int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsig
     Carve cv{scratch};
     ElemRec *d_elems = cv.take<ElemRec>(hs.elems.size());
     float4 *d_sphere = cv.take<float4>(hs.elem_sphere.size());
+    int2 *d_scells = cv.take<int2>(hs.stage_cells.size());
+    float4 *d_gsph = cv.take<float4>(hs.grid_sphere.size());
+    int *d_gel = cv.take<int>(hs.grid_elem.size());
     double *d_surf = cv.take<double>(hs.surf_data.size());
     BvhNode *d_bvh = cv.take<BvhNode>(hs.bvh.size());
     int *d_bvh_items = cv.take<int>(hs.bvh_items.size());
@@ -124,6 +127,9 @@ extern "C" int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsig
     SceneDev S = hs.dev;
     S.elems = d_elems;
     S.elem_sphere = d_sphere;
+    S.stage_cells = d_scells;
+    S.grid_sphere = d_gsph;
+    S.grid_elem = d_gel;
     S.surf_data = d_surf;
     S.bvh = d_bvh;
     S.bvh_items = d_bvh_items;
@@ -141,6 +147,8 @@ extern "C" int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsig
     memset(&r0, 0, sizeof r0);
     r0.target = ~0ull;  // no cut-off: every hit of the range is listed
     if ((e = put(d_elems, hs.elems, st)) != cudaSuccess || (e = put(d_sphere, hs.elem_sphere, st)) != cudaSuccess ||
+        (e = put(d_scells, hs.stage_cells, st)) != cudaSuccess || (e = put(d_gsph, hs.grid_sphere, st)) != cudaSuccess ||
+        (e = put(d_gel, hs.grid_elem, st)) != cudaSuccess ||
         (e = put(d_surf, hs.surf_data, st)) != cudaSuccess ||
         (e = put(d_bvh, hs.bvh, st)) != cudaSuccess || (e = put(d_bvh_items, hs.bvh_items, st)) != cudaSuccess ||
         (e = put(d_cells, hs.cell_start, st)) != cudaSuccess || (e = put(d_cdisc, hs.cell_disc, st)) != cudaSuccess ||

@@ -56,18 +56,21 @@ cudaError_t upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s, uint64_t 
 struct Workspace {
     int device = -1;
     cudaStream_t stream = nullptr;
+    DevBuf stage_cells, grid_sphere, grid_elem;
     DevBuf elems, elem_sphere, optics, surf, tables, bvh, bvh_items, cell_start, cell_disc, cell_par, inv_cdf, expos,
         excos;
     DevBuf acc, ctr, rs, rec_count, hit_elem, counts, offsets, total, hit_sid, hit_el, recs;
     DevBuf cand;  // grid probe's candidate list: count, then one sun-ray index per entry
+    // trace state and queues (one slot per hit-list entry of a batch)
+    DevBuf wf_sid, wf_raynum, wf_draw, wf_meta, wf_fe0, wf_p, wf_c, wf_q0, wf_q1, wf_qs, wf_counts;
     DevBuf ecount, ecursor, etotal, s_sid, s_el, s_idx;
     std::vector<cudaEvent_t> events;
     // autotuned kernel variants per precision (FP64, mixed), chosen on the first run
     struct Tuning {
         bool done = false;
-        int probe = 0, trace = 0;
+        int probe = 0;
     } tune[2];
-    DevBuf tune_rs, tune_ctr, tune_acc;
+    DevBuf tune_rs;
     ~Workspace() {
         if (device >= 0) cudaSetDevice(device);
         for (auto e : events) cudaEventDestroy(e);
@@ -85,42 +88,28 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 
 }  // namespace
 
-// Autotuner: time every register-budget variant of the probe and of the trace kernel on
-// the same 2^21 sun rays (indices 0.., outputs discarded into scratch buffers) and keep
-// the fastest of each for this workspace and precision.  Variants share their arithmetic,
-// so the choice changes timing only.
-static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, uint64_t max_sun, int dev_sms,
-                            cudaStream_t st, DevBuf &hit_elem, DevBuf &counts, DevBuf &offsets, DevBuf &total,
-                            DevBuf &hit_sid, DevBuf &hit_el, DevBuf &ecount, DevBuf &ecursor, DevBuf &etotal,
-                            DevBuf &s_sid, DevBuf &s_el, DevBuf &s_idx, bool sort_hits, uint32_t n_elem0, size_t ne,
-                            int &launches) {
+// Autotuner: time every register-budget variant of the probe on the same 2^21 sun rays
+// (indices 0.., outputs discarded into scratch buffers) and keep the fastest for this
+// workspace and precision.  Variants share their arithmetic, so the choice changes
+// timing only.
+static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, uint64_t max_sun, cudaStream_t st,
+                            DevBuf &hit_elem, DevBuf &counts, int &launches) {
     Workspace::Tuning &tu = ws.tune[precision ? 1 : 0];
     const uint64_t n = std::min<uint64_t>(uint64_t(1) << 21, max_sun);
     if (n == 0) return cudaSuccess;
     const uint32_t nb = uint32_t((n + kProbeBlock - 1) / kProbeBlock);
     cudaError_t e;
-    if ((e = hit_elem.ensure(n * 4)) || (e = counts.ensure(size_t(nb) * 4)) || (e = offsets.ensure(size_t(nb) * 4)) ||
-        (e = total.ensure(8)) || (e = hit_sid.ensure(n * 8)) || (e = hit_el.ensure(n * 4)) ||
-        (e = ws.tune_rs.ensure(sizeof(RunState))) || (e = ws.tune_ctr.ensure(sizeof(RunCounters))) ||
-        (e = ws.tune_acc.ensure(std::max<size_t>(3 * ne, 1) * 8)) || (e = ws.cand.ensure((n + 1) * 4)))
+    if ((e = hit_elem.ensure(n * 4)) || (e = counts.ensure(size_t(nb) * 4)) ||
+        (e = ws.tune_rs.ensure(sizeof(RunState))) || (e = ws.cand.ensure((n + 1) * 4)))
         return e;
-    if (sort_hits && ((e = s_sid.ensure(n * 8)) || (e = s_el.ensure(n * 4)) || (e = s_idx.ensure(n * 4)))) return e;
     SceneDev S = S0;
     S.n_flux = 0;
     RunState r0;
     memset(&r0, 0, sizeof r0);
     r0.target = ~0ull;
     RunState *rs = ws.tune_rs.as<RunState>();
-    TraceOut O;
-    memset(&O, 0, sizeof O);
-    O.ctr = ws.tune_ctr.as<RunCounters>();
-    unsigned long long *acc = ws.tune_acc.as<unsigned long long>();
-    O.first_hits = acc;
-    O.absorbed = acc + ne;
-    O.delivered = acc + 2 * ne;
-    O.rec_count = nullptr;
     cudaMemcpyAsync(rs, &r0, sizeof r0, cudaMemcpyHostToDevice, st);
-    cudaEvent_t ev[2 * (kProbeVariants + kTraceVariants) + 2];
+    cudaEvent_t ev[2 * kProbeVariants];
     for (auto &x : ev) cudaEventCreate(&x);
     uint32_t *cand_count = ws.cand.as<uint32_t>(), *cand = cand_count + 1;
     auto probe = [&](int v) {
@@ -137,34 +126,6 @@ static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, ui
         probe(v);
         cudaEventRecord(ev[2 * v + 1], st);
     }
-    launch_offsets(counts.as<uint32_t>(), nb, offsets.as<uint32_t>(), total.as<uint32_t>(), st);
-    launch_compact(0, uint32_t(n), hit_elem.as<uint32_t>(), counts.as<uint32_t>(), offsets.as<uint32_t>(),
-                   hit_sid.as<uint64_t>(), hit_el.as<uint32_t>(), st);
-    launches += 2;
-    const uint64_t *t_sid = hit_sid.as<uint64_t>();
-    const uint32_t *t_el = hit_el.as<uint32_t>(), *t_idx = nullptr;
-    if (sort_hits) {
-        launch_sort_by_element(total.as<uint32_t>(), hit_sid.as<uint64_t>(), hit_el.as<uint32_t>(), n_elem0,
-                               ecount.as<uint32_t>(), ecursor.as<uint32_t>(), etotal.as<uint32_t>(),
-                               s_sid.as<uint64_t>(), s_el.as<uint32_t>(), s_idx.as<uint32_t>(), uint32_t(n), st);
-        launches += 3;
-        t_sid = s_sid.as<uint64_t>();
-        t_el = s_el.as<uint32_t>();
-        t_idx = s_idx.as<uint32_t>();
-    }
-    const int base = 2 * kProbeVariants;
-    for (int v = -1; v < kTraceVariants; ++v) {
-        const int vv = v < 0 ? 0 : v;  // v = -1 warms the caches
-        const int per_sm = precision ? trace_blocks_per_sm_mixed(false, vv) : trace_blocks_per_sm_fp64(false, vv);
-        cudaMemsetAsync(&rs->cursor, 0, sizeof(unsigned), st);
-        if (v >= 0) cudaEventRecord(ev[base + 2 * v], st);
-        if (precision)
-            launch_trace_mixed(false, S, t_sid, t_el, t_idx, total.as<uint32_t>(), rs, O, uint32_t(dev_sms * per_sm), vv, st);
-        else
-            launch_trace_fp64(false, S, t_sid, t_el, t_idx, total.as<uint32_t>(), rs, O, uint32_t(dev_sms * per_sm), vv, st);
-        launches++;
-        if (v >= 0) cudaEventRecord(ev[base + 2 * v + 1], st);
-    }
     e = cudaStreamSynchronize(st);
     if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) {
@@ -175,15 +136,6 @@ static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, ui
             if (ms < best * 0.98f) {
                 best = ms;
                 tu.probe = v;
-            }
-        }
-        best = 1e30f;
-        for (int v = 0; v < kTraceVariants; ++v) {
-            float ms = 0;
-            cudaEventElapsedTime(&ms, ev[base + 2 * v], ev[base + 2 * v + 1]);
-            if (ms < best * 0.98f) {
-                best = ms;
-                tu.trace = v;
             }
         }
         tu.done = true;
@@ -225,6 +177,9 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
            &d_inv_cdf = ws.inv_cdf, &d_expos = ws.expos, &d_excos = ws.excos;
     CK(upload(d_elems, hs.elems, st, out.h2d_bytes));
     CK(upload(ws.elem_sphere, hs.elem_sphere, st, out.h2d_bytes));
+    CK(upload(ws.stage_cells, hs.stage_cells, st, out.h2d_bytes));
+    CK(upload(ws.grid_sphere, hs.grid_sphere, st, out.h2d_bytes));
+    CK(upload(ws.grid_elem, hs.grid_elem, st, out.h2d_bytes));
     CK(upload(d_optics, hs.optics, st, out.h2d_bytes));
     CK(upload(d_surf, hs.surf_data, st, out.h2d_bytes));
     CK(upload(d_tables, hs.tables, st, out.h2d_bytes));
@@ -240,6 +195,9 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     SceneDev S = hs.dev;
     S.elems = d_elems.as<ElemRec>();
     S.elem_sphere = ws.elem_sphere.as<float4>();
+    S.stage_cells = ws.stage_cells.as<int2>();
+    S.grid_sphere = ws.grid_sphere.as<float4>();
+    S.grid_elem = ws.grid_elem.as<int>();
     S.optics = d_optics.as<OpticRec>();
     S.surf_data = d_surf.as<double>();
     S.tables = d_tables.as<double>();
@@ -290,15 +248,10 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     }
     unsigned long long rec_cap = 0;
     Workspace::Tuning &tu = ws.tune[rq.precision ? 1 : 0];
-    if (!tu.done && !explicit_mode)
-        CK(autotune(ws, S, rq.precision, rq.max_sun, dev_sms, st, d_hit_elem, d_counts, d_offsets, d_total, d_hit_sid,
-                    d_hit_el, d_ecount, d_ecursor, d_etotal, d_s_sid, d_s_el, d_s_idx, sort_hits, n_elem0, ne,
-                    out.gpu_launches));
+    if (!tu.done && !explicit_mode) CK(autotune(ws, S, rq.precision, rq.max_sun, st, d_hit_elem, d_counts, out.gpu_launches));
     out.probe_variant = tu.probe;
-    out.trace_variant = tu.trace;
-    const int per_sm = rq.precision ? trace_blocks_per_sm_mixed(rq.records, tu.trace)
-                                    : trace_blocks_per_sm_fp64(rq.records, tu.trace);
-    const uint32_t trace_grid = uint32_t(dev_sms * per_sm);
+    out.trace_variant = 0;
+    (void)dev_sms;
     CK(cudaStreamSynchronize(st));
     out.setup_ms = ms_since(t_setup);
 
@@ -433,17 +386,44 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                     t_el = d_s_el.as<uint32_t>();
                     t_idx = d_s_idx.as<uint32_t>();
                 }
+                // trace state and queues: one slot per hit-list entry (at most n)
+                CK(ws.wf_sid.ensure(n * 8));
+                CK(ws.wf_raynum.ensure(n * 4));
+                CK(ws.wf_draw.ensure(n * 4));
+                CK(ws.wf_meta.ensure(n * 16));
+                CK(ws.wf_fe0.ensure(n * 4));
+                CK(ws.wf_p.ensure(n * 24));
+                CK(ws.wf_c.ensure(n * 24));
+                CK(ws.wf_q0.ensure(n * 4));
+                CK(ws.wf_q1.ensure(n * 4));
+                CK(ws.wf_qs.ensure(n * 4));
+                WfQueues Q;
+                Q.rounds = 2 * nst;
+                CK(ws.wf_counts.ensure(sizeof(uint32_t) * (2 * Q.rounds + 1)));
+                Q.search[0] = ws.wf_q0.as<uint32_t>();
+                Q.search[1] = ws.wf_q1.as<uint32_t>();
+                Q.shade = ws.wf_qs.as<uint32_t>();
+                Q.counts = ws.wf_counts.as<uint32_t>();
+                WfState W;
+                W.sid = ws.wf_sid.as<uint64_t>();
+                W.raynum = ws.wf_raynum.as<uint32_t>();
+                W.draw = ws.wf_draw.as<uint32_t>();
+                W.meta = ws.wf_meta.as<int4>();
+                W.fe0 = ws.wf_fe0.as<int>();
+                W.p = ws.wf_p.as<double>();
+                W.c = ws.wf_c.as<double>();
+                W.cap = uint32_t(n);
                 CK(cudaEventRecord(p1, st));
                 if (rq.precision)
-                    launch_trace_mixed(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(), drs, O, trace_grid,
-                                       tu.trace, st);
+                    out.gpu_launches += launch_trace_mixed(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(),
+                                                           drs, O, W, Q, st);
                 else
-                    launch_trace_fp64(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(), drs, O, trace_grid,
-                                      tu.trace, st);
+                    out.gpu_launches += launch_trace_fp64(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(),
+                                                          drs, O, W, Q, st);
                 CK(cudaEventRecord(p2, st));
                 launch_advance(d_total.as<uint32_t>(), d_hit_sid.as<uint64_t>(), sun_next, uint32_t(n), drs, st);
                 CK(cudaGetLastError());
-                out.gpu_launches += 4;  // offsets, compact, trace, advance
+                out.gpu_launches += 3;  // offsets, compact, advance
                 probe_ev.push_back({p0, p1});
                 trace_ev.push_back({p1, p2});
                 queued += n;

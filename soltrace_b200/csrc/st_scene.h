@@ -73,7 +73,12 @@ struct StageRec {
     int virt, multihit, tracethrough;
     int bvh_off;   // first node in SceneDev::bvh, -1 when brute force is used
     int bvh_items_off;
-    int pad_;
+    // ground grid over the stage's x-y plane (stages spread in x, y within a thin z band,
+    // such as heliostat fields): cell (ix, iy) lists every enabled element whose padded
+    // bounding disc overlaps it; grid_on = 0 when not built
+    int grid_on;
+    int gnx, gny, gcell_off;  // cells, first cell in SceneDev::stage_cells
+    float gx0, gy0, gcell, ginv, gzlo, gzhi;
 };
 
 // BVH node over element bounding spheres in stage coordinates.  Leaf when
@@ -119,6 +124,9 @@ struct SceneDev {
     const double *tables;
     const BvhNode *bvh;
     const int *bvh_items;
+    const int2 *stage_cells;     // ground-grid cells of every stage: [start, end) of the entries
+    const float4 *grid_sphere;   // ground-grid entries: element bounding sphere (stage coordinates)
+    const int *grid_elem;        // ground-grid entries: element index within the stage
     StageRec stages[kMaxStages];
     int n_stages;
     SunDev sun;

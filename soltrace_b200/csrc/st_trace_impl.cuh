@@ -134,9 +134,107 @@ __device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const d
     return best;
 }
 
+// Nearest element through the stage's ground grid: a 2-D DDA walk over the cells the ray
+// crosses inside the stage's z band, in order of distance.  Entries pass a float test
+// against their padded bounding sphere; the few that pass are collected and given the
+// double-precision element test after the walk (or when the list fills, after which the
+// walk stops at the first cell beyond the nearest hit).  Every element a hit can come
+// from is listed in a visited cell (the padded discs absorb the float rounding of the
+// walk), and the choice among hits is the serial search's (shortest path, lower index on
+// ties), so the result is the brute-force search's.
+template <int MIXED>
+__device__ inline int nearest_grid(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3],
+                                   int from) {
+    const float ox = float(ps[0]), oy = float(ps[1]), oz = float(ps[2]);
+    const float dx = float(cs[0]), dy = float(cs[1]), dz = float(cs[2]);
+    // clip to the z band and the grid box
+    float t0 = 0.0f, t1 = 3.0e38f;
+    auto clip = [&](float o, float d, float lo, float hi) {
+        if (fabsf(d) > 1e-30f) {
+            const float a = (lo - o) / d, b = (hi - o) / d;
+            t0 = fmaxf(t0, fminf(a, b));
+            t1 = fminf(t1, fmaxf(a, b));
+        } else if (o < lo || o > hi) {
+            t1 = -1.0f;
+        }
+    };
+    clip(oz, dz, st.gzlo, st.gzhi);
+    clip(ox, dx, st.gx0, st.gx0 + st.gnx * st.gcell);
+    clip(oy, dy, st.gy0, st.gy0 + st.gny * st.gcell);
+    if (!(t0 <= t1)) return -1;
+    const float px = ox + t0 * dx, py = oy + t0 * dy;
+    int ix = min(max(int(floorf((px - st.gx0) * st.ginv)), 0), st.gnx - 1);
+    int iy = min(max(int(floorf((py - st.gy0) * st.ginv)), 0), st.gny - 1);
+    const int sx = dx > 0.0f ? 1 : -1, sy = dy > 0.0f ? 1 : -1;
+    const float inf = 3.0e38f;
+    float tmx = fabsf(dx) > 1e-30f ? (st.gx0 + (ix + (dx > 0.0f)) * st.gcell - ox) / dx : inf;
+    float tmy = fabsf(dy) > 1e-30f ? (st.gy0 + (iy + (dy > 0.0f)) * st.gcell - oy) / dy : inf;
+    const float tdx = fabsf(dx) > 1e-30f ? st.gcell / fabsf(dx) : inf;
+    const float tdy = fabsf(dy) > 1e-30f ? st.gcell / fabsf(dy) : inf;
+    const int2 *cells = S.stage_cells + st.gcell_off;
+    const float pad_o = 2e-6f * (fabsf(ox) + fabsf(oy) + fabsf(oz));
+    int best = -1;
+    double bp = 1e99;
+    constexpr int kCand = 8;
+    int cand[kCand];
+    int nc = 0;
+    auto flush = [&]() {
+        for (int c = 0; c < nc; ++c) {
+            const int j = cand[c];
+            double pl;
+            if (element_test<MIXED>(S, S.elems[st.first_elem + j], ps, cs, pl, nullptr) &&
+                (pl < bp || (pl == bp && j < best))) {
+                bp = pl;
+                best = j;
+            }
+        }
+        nc = 0;
+    };
+    int seen1 = -1, seen2 = -1, seen3 = -1;
+    float tin = t0;
+    for (;;) {
+        if (best >= 0 && double(tin) > bp * (1.0 + 1e-6) + 1e-3) break;
+        const int2 range = cells[iy * st.gnx + ix];
+        for (int k = range.x; k < range.y; ++k) {
+            const float4 bs = S.grid_sphere[k];
+            const float vx = bs.x - ox, vy = bs.y - oy, vz = bs.z - oz;
+            const float tc = vx * dx + vy * dy + vz * dz;
+            const float wx = vx - tc * dx, wy = vy - tc * dy, wz = vz - tc * dz;
+            // radius padded for the float rounding of centre, origin and direction
+            const float rr = bs.w + pad_o + 2e-6f * (fabsf(vx) + fabsf(vy) + fabsf(vz));
+            if (tc < -rr || wx * wx + wy * wy + wz * wz > rr * rr) continue;
+            const int j = S.grid_elem[k];
+            // the element the ray is leaving (when it certainly cannot be met again), and
+            // elements already collected from the last cells
+            if (j == from || j == seen1 || j == seen2 || j == seen3) continue;
+            seen3 = seen2;
+            seen2 = seen1;
+            seen1 = j;
+            if (nc == kCand) flush();
+            cand[nc++] = j;
+        }
+        // step to the next cell along the ray
+        if (tmx < tmy) {
+            tin = tmx;
+            ix += sx;
+            tmx += tdx;
+            if (ix < 0 || ix >= st.gnx) break;
+        } else {
+            tin = tmy;
+            iy += sy;
+            tmy += tdy;
+            if (iy < 0 || iy >= st.gny) break;
+        }
+        if (tin > t1) break;
+    }
+    flush();
+    return best;
+}
+
 template <int MIXED>
 __device__ __forceinline__ int nearest(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3],
                                        int from = -1) {
+    if (st.grid_on) return nearest_grid<MIXED>(S, st, ps, cs, from);
     return (st.bvh_off >= 0) ? nearest_bvh<MIXED>(S, st, ps, cs, from) : nearest_brute<MIXED>(S, st, ps, cs);
 }
 
@@ -561,27 +659,296 @@ __global__ void k_advance(const uint32_t *total, const uint64_t *hit_sid, uint64
 }
 #endif  // ST_COMMON_KERNELS
 
-template <int MIXED, int RECORDS, int MINB>
-__global__ void __launch_bounds__(kTraceBlock, MINB) k_trace(SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el,
-                                                        const uint32_t *hit_idx, const uint32_t *total,
-                                                        RunState *rs, TraceOut O) {
-    __shared__ unsigned long long sh_entries[kMaxStages];
-    __shared__ unsigned int sh_max_enter[kMaxStages], sh_max_tt[kMaxStages];
-    __shared__ unsigned int sh_flags, sh_warps_done;
-    if (threadIdx.x < kMaxStages) {
-        sh_entries[threadIdx.x] = 0;
-        sh_max_enter[threadIdx.x] = 0;
-        sh_max_tt[threadIdx.x] = 0;
-    }
-    if (threadIdx.x == 0) {
-        sh_flags = 0;
-        sh_warps_done = 0;
-    }
-    __syncthreads();
+// ------------------------------------------------------------------------------------
+// Trace: a wavefront over device-side ray queues.
+//
+// The per-ray state machine of raytrace.cpp:582-1040 is cut into two steps, each its own
+// kernel over a queue of rays: `shade` (the full hit on a known element: interaction,
+// random draws, records, flux and counters, then the outgoing ray) and `search` (the
+// nearest element of the current stage, or the stage exit).  Rays move between the
+// queues until they are absorbed or leave the last stage; the state they carry between
+// kernels is what the serial loop keeps in its locals.  Each kernel holds only the code of
+// its step, so it keeps few registers and many resident warps, and every warp does the
+// same step (a single trace kernel with both steps inlined was latency bound).  After a
+// fixed number of rounds a finishing kernel runs the remaining rays to the end one step
+// after the other.  Results do not depend on the queue order (per-ray random streams,
+// integer atomics, records ordered on the host by ray number and hit index).
+// ------------------------------------------------------------------------------------
+enum WfStatus : int { kWfDone = 0, kWfShade = 1, kWfSearch = 2 };
 
-    // rays of this batch to trace: the cut-off at the requested hit count (k_advance
-    // applies the same rule after this kernel)
-    // (entries may be sorted by element: hit_idx gives each entry's sun-order index)
+struct WfRay {
+    uint64_t sid;
+    uint32_t raynum, draw;
+    int si, hits, last_j, next_j, fe0;
+    double p[3], c[3];  // global while hits == 0 in stage si, stage coordinates after
+    bool moved;         // p, c changed since loaded
+};
+
+struct WfBlockCtr {
+    unsigned long long entries[kMaxStages];
+    unsigned int max_enter[kMaxStages], max_tt[kMaxStages];
+    unsigned int flags;
+};
+
+__device__ __forceinline__ void wf_ctr_init(WfBlockCtr &c) {
+    if (threadIdx.x < kMaxStages) {
+        c.entries[threadIdx.x] = 0;
+        c.max_enter[threadIdx.x] = 0;
+        c.max_tt[threadIdx.x] = 0;
+    }
+    if (threadIdx.x == 0) c.flags = 0;
+    __syncthreads();
+}
+
+__device__ __forceinline__ void wf_ctr_flush(WfBlockCtr &c, const SceneDev &S, const TraceOut &O) {
+    __syncthreads();
+    if (threadIdx.x < S.n_stages) {
+        const int s = threadIdx.x;
+        if (c.entries[s]) {
+            atomicAdd(&O.ctr->stage_entries[s], c.entries[s]);
+            atomicMax(&O.ctr->max_enter[s], c.max_enter[s]);
+        }
+        if (c.max_tt[s]) atomicMax(&O.ctr->max_ttmiss[s], c.max_tt[s]);
+    }
+    if (threadIdx.x == 0 && c.flags) atomicOr(&O.ctr->flags, c.flags);
+}
+
+__device__ __forceinline__ WfRay wf_load(const WfState &W, uint32_t i) {
+    WfRay r;
+    r.sid = W.sid[i];
+    r.raynum = W.raynum[i];
+    r.draw = W.draw[i];
+    const int4 m = W.meta[i];
+    r.si = m.x;
+    r.hits = m.y;
+    r.last_j = m.z;
+    r.next_j = m.w;
+    r.fe0 = W.fe0[i];
+    for (int q = 0; q < 3; ++q) {
+        r.p[q] = W.p[size_t(q) * W.cap + i];
+        r.c[q] = W.c[size_t(q) * W.cap + i];
+    }
+    r.moved = false;
+    return r;
+}
+
+__device__ __forceinline__ void wf_store(const WfState &W, uint32_t i, const WfRay &r, bool all) {
+    if (all) {
+        W.sid[i] = r.sid;
+        W.raynum[i] = r.raynum;
+    }
+    W.draw[i] = r.draw;
+    W.meta[i] = make_int4(r.si, r.hits, r.last_j, r.next_j);
+    W.fe0[i] = r.fe0;
+    if (all || r.moved)
+        for (int q = 0; q < 3; ++q) {
+            W.p[size_t(q) * W.cap + i] = r.p[q];
+            W.c[size_t(q) * W.cap + i] = r.c[q];
+        }
+}
+
+// append `slot` to a queue for every active lane with `want`; one atomic per warp
+__device__ __forceinline__ void wf_push(uint32_t *queue, uint32_t *count, uint32_t slot, bool want) {
+    const unsigned mask = __activemask();
+    const unsigned bal = __ballot_sync(mask, want);
+    if (bal == 0) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(bal) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(count, uint32_t(__popc(bal)));
+    base = __shfl_sync(mask, base, leader);
+    if (want) queue[base + __popc(bal & ((1u << lane) - 1u))] = slot;
+}
+
+// a ray enters stage si: entry count and largest ray number (raytrace.cpp:617-623)
+__device__ __forceinline__ void wf_stage_enter(WfBlockCtr &c, int si, uint32_t raynum) {
+    const unsigned mask = __activemask();
+    const unsigned peers = __match_any_sync(mask, si);
+    const unsigned mx = __reduce_max_sync(peers, raynum);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) {
+        atomicAdd(&c.entries[si], (unsigned long long)__popc(peers));
+        atomicMax(&c.max_enter[si], mx);
+    }
+}
+
+// the ray leaves stage si (no further hit there): a miss is recorded with element 0 and
+// ends the ray unless the stage is trace-through (raytrace.cpp:800-826; the one miss the
+// reference does not record is removed on the host from max_ttmiss); otherwise the ray
+// goes on, in global coordinates, to the next stage
+template <int RECORDS>
+__device__ __forceinline__ int wf_exit_stage(const SceneDev &S, const TraceOut &O, WfBlockCtr &c, WfRay &r,
+                                             const double ps[3], const double cs[3]) {
+    const StageRec &st = S.stages[r.si];
+    if (r.hits == 0) {
+        if (r.si == 0) return kWfDone;  // cannot happen: first-stage rays are numbered hits
+        if (RECORDS) {
+            const unsigned long long slot = warp_reserve(O.rec_count);
+            if (slot < O.rec_cap) {
+                RecordDev rec;
+                to_local(st.R, st.o, r.p, r.c, rec.pos, rec.cos);
+                rec.element = 0;
+                rec.stage = r.si + 1;
+                rec.raynum = r.raynum;
+                rec.seq = 0;
+                O.recs[slot] = rec;
+            }
+        }
+        if (!st.tracethrough) return kWfDone;
+        atomicMax(&c.max_tt[r.si], r.raynum);
+        // global ray unchanged
+    } else {
+        to_ref(st.R, st.o, ps, cs, r.p, r.c);
+        r.moved = true;
+    }
+    if (r.si + 1 >= S.n_stages) return kWfDone;
+    r.si += 1;
+    r.hits = 0;
+    r.last_j = -1;
+    r.next_j = -1;
+    wf_stage_enter(c, r.si, r.raynum);
+    return kWfSearch;
+}
+
+// the ray's position/direction in its stage's coordinates
+__device__ __forceinline__ void wf_stage_ray(const SceneDev &S, const WfRay &r, double ps[3], double cs[3]) {
+    if (r.hits == 0) {
+        const StageRec &st = S.stages[r.si];
+        to_local(st.R, st.o, r.p, r.c, ps, cs);
+    } else {
+        for (int q = 0; q < 3; ++q) {
+            ps[q] = r.p[q];
+            cs[q] = r.c[q];
+        }
+    }
+}
+
+// search step: nearest element of the current stage (raytrace.cpp:698-770)
+template <int MIXED, int RECORDS>
+__device__ __forceinline__ int wf_search(const SceneDev &S, const TraceOut &O, WfBlockCtr &c, WfRay &r) {
+    double ps[3], cs[3];
+    wf_stage_ray(S, r, ps, cs);
+    const int j = nearest<MIXED>(S, S.stages[r.si], ps, cs, r.last_j);
+    if (j < 0) return wf_exit_stage<RECORDS>(S, O, c, r, ps, cs);
+    r.next_j = j;
+    return kWfShade;
+}
+
+// shade step: the hit on element next_j and what the ray does there (raytrace.cpp:830-1000)
+template <int MIXED, int RECORDS>
+__device__ __forceinline__ int wf_shade(const SceneDev &S, const TraceOut &O, WfBlockCtr &c, WfRay &r) {
+    const int si = r.si;
+    const StageRec &st = S.stages[si];
+    double ps[3], cs[3];
+    wf_stage_ray(S, r, ps, cs);
+    const int j = r.next_j;
+    r.next_j = -1;
+    const ElemRec &e = S.elems[st.first_elem + j];
+    Hit h;
+    double pl;
+    // re-test the chosen element for the full hit (same arithmetic as the search)
+    if (!element_test<MIXED>(S, e, ps, cs, pl, &h)) return wf_exit_stage<RECORDS>(S, O, c, r, ps, cs);
+    const int hits = ++r.hits;
+    if (hits == 1) {
+        warp_count(O.first_hits, st.first_elem + j);
+        if (si == 0) r.fe0 = st.first_elem + j;
+    }
+    RayRng rng;
+    rng.init(S.seed, r.sid, r.draw);
+    bool absorbed = false;
+    double pout[3], cout[3];
+    if (st.virt) {
+        for (int q = 0; q < 3; ++q) {
+            pout[q] = h.pe[q];
+            cout[q] = h.ce[q];
+        }
+    } else {
+        if (e.interaction != 1 && e.interaction != 2) {
+            atomicOr(&c.flags, unsigned(kFlagBadInteraction));
+            absorbed = true;
+        } else {
+            const OpticRec &op = S.optics[h.back ? e.opt_back : e.opt_front];
+            const double tv = test_value<MIXED>(S, op, e.interaction, h.ce, h.n);
+            if (tv <= rng.u()) absorbed = true;
+            if (!absorbed) {
+                double cin[3] = {h.ce[0], h.ce[1], h.ce[2]};
+                if (S.sunshape_on && si == 0 && hits == 1) {
+                    double c2[3];
+                    error_sample<MIXED>(S, S.sun.shape, S.sun.sigma / 1000.0, cin, rng, false, h.n, c2);
+                    for (int q = 0; q < 3; ++q) cin[q] = c2[q];
+                }
+                double nrm[3] = {h.n[0], h.n[1], h.n[2]};
+                if (S.errors_on) {
+                    double n2[3];
+                    const int d = op.dist;
+                    const int dd = (d == 'g' || d == 'G' || d == 'p' || d == 'P') ? d : 0;
+                    error_sample<MIXED>(S, dd, op.slope / 1000.0, nrm, rng, false, nrm, n2);
+                    for (int q = 0; q < 3; ++q) nrm[q] = n2[q];
+                }
+                if (e.interaction == 1)
+                    refract<MIXED>(op, cin, nrm, rng, cout);
+                else
+                    reflect(cin, nrm, cout);
+                if (S.errors_on) {
+                    const bool diffuse = (op.dist == 'f' || op.dist == 'F');
+                    double axis[3], c3[3];
+                    for (int q = 0; q < 3; ++q) axis[q] = diffuse ? nrm[q] : cout[q];
+                    error_sample<MIXED>(S, op.dist, op.spec / 1000.0, axis, rng, e.interaction == 2, nrm, c3);
+                    for (int q = 0; q < 3; ++q) cout[q] = c3[q];
+                }
+                for (int q = 0; q < 3; ++q) pout[q] = h.pe[q];
+            }
+        }
+    }
+    r.draw = rng.k;
+    if (RECORDS) {
+        const unsigned long long slot = warp_reserve(O.rec_count);
+        if (slot < O.rec_cap) {
+            RecordDev rec;
+            to_ref(e.R, e.o, h.pe, h.ce, rec.pos, rec.cos);
+            rec.element = absorbed ? -(j + 1) : (j + 1);
+            rec.stage = si + 1;
+            rec.raynum = r.raynum;
+            rec.seq = uint32_t(hits - 1);
+            O.recs[slot] = rec;
+        }
+    }
+    if (S.n_flux) bin_flux<MIXED>(S, si, j, absorbed, h.pe);
+    if (absorbed) {
+        warp_count(O.absorbed, st.first_elem + j);
+        if (si == S.n_stages - 1 && r.fe0 >= 0) warp_count(O.delivered, r.fe0);
+        return kWfDone;
+    }
+    to_ref(e.R, e.o, pout, cout, ps, cs);
+    // A flat element cannot meet the ray leaving it: the next test's 1e-5 nudge moves the
+    // origin 1e-5 |cz| off the plane, behind the ray.  Skipped only when that offset exceeds
+    // the round-off of the local z (1e-13 of the coordinates, hundreds of ulps), so the
+    // skipped test is one that fails.
+    r.last_j = (e.stype == kSurfFlat &&
+                1e-5 * fabs(cout[2]) >
+                    1e-13 * (1.0 + fabs(e.o[0]) + fabs(e.o[1]) + fabs(e.o[2]) + fabs(pout[0]) + fabs(pout[1])))
+                   ? j
+                   : -1;
+    for (int q = 0; q < 3; ++q) {
+        r.p[q] = ps[q];
+        r.c[q] = cs[q];
+    }
+    r.moved = true;
+    if (!st.multihit) return wf_exit_stage<RECORDS>(S, O, c, r, ps, cs);
+    if (hits >= kMaxHitsPerStage) {
+        atomicOr(&c.flags, unsigned(kFlagHitCap));
+        return wf_exit_stage<RECORDS>(S, O, c, r, ps, cs);
+    }
+    return kWfSearch;
+}
+
+// First kernel: the batch's numbered rays (hit-list entries below the cut-off at the
+// requested hit count; k_advance applies the same rule after the trace) enter the first
+// stage and are shaded on the element the probe found.
+template <int MIXED, int RECORDS>
+__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_first(
+    SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx, const uint32_t *total,
+    const RunState *rs, TraceOut O, WfState W, uint32_t *q_search, uint32_t *n_search) {
+    __shared__ WfBlockCtr c;
+    wf_ctr_init(c);
     uint32_t n = 0, take = 0, raynum_base = 0;
     if (!rs->reached) {
         const unsigned long long left = rs->target - rs->hits_done;
@@ -590,182 +957,139 @@ __global__ void __launch_bounds__(kTraceBlock, MINB) k_trace(SceneDev S, const u
         raynum_base = uint32_t(rs->hits_done);
     }
     if (!hit_idx) n = take;
-    // warps take 32 consecutive entries at a time from the queue: consecutive entries
-    // share their first element once sorted, and no warp waits for another
-    const int lane = threadIdx.x & 31;
-    for (;;) {
-        __syncwarp();
-        uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&rs->cursor, 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= n) break;
-        const uint32_t i = base + lane;
-        const uint32_t idx = (i < n) ? (hit_idx ? hit_idx[i] : i) : 0xffffffffu;
-        if (i >= n || idx >= take) continue;  // past the list, or beyond the requested hit count
-        const uint64_t sid = hit_sid[i];
-        const uint32_t raynum = raynum_base + idx + 1;
-        RayRng rng;
-        rng.init(S.seed, sid, 0);
-        double pg[3], cg[3], xs, ys;
-        make_ray(S, sid, rng, pg, cg, xs, ys);
-        int known = int(hit_el[i]);
-        int first_elem0 = -1;  // the ray's first first-stage element (global index)
-        for (int si = 0; si < S.n_stages; ++si) {
-            const StageRec &st = S.stages[si];
-            {
-                const unsigned mask = __activemask();
-                const unsigned peers = __match_any_sync(mask, si);
-                const unsigned mx = __reduce_max_sync(peers, raynum);
-                if ((threadIdx.x & 31) == __ffs(peers) - 1) {
-                    atomicAdd(&sh_entries[si], (unsigned long long)__popc(peers));
-                    atomicMax(&sh_max_enter[si], mx);
-                }
-            }
-            double ps[3], cs[3];
-            to_local(st.R, st.o, pg, cg, ps, cs);
-            int hits = 0, last_j = -1;
-            bool absorbed = false;
-            for (;;) {
-                int j = (hits == 0 && known >= 0) ? known : nearest<MIXED>(S, st, ps, cs, last_j);
-                known = -1;
-                if (j < 0) break;
-                const ElemRec &e = S.elems[st.first_elem + j];
-                Hit h;
-                double pl;
-                // re-test the chosen element for the full hit (same arithmetic as the search)
-                if (!element_test<MIXED>(S, e, ps, cs, pl, &h)) break;
-                ++hits;
-                if (hits == 1) {
-                    warp_count(O.first_hits, st.first_elem + j);
-                    if (si == 0) first_elem0 = st.first_elem + j;
-                }
-                double pout[3], cout[3];
-                if (st.virt) {
-                    for (int q = 0; q < 3; ++q) {
-                        pout[q] = h.pe[q];
-                        cout[q] = h.ce[q];
-                    }
-                } else {
-                    if (e.interaction != 1 && e.interaction != 2) {
-                        atomicOr(&sh_flags, unsigned(kFlagBadInteraction));
-                        absorbed = true;
-                    } else {
-                        const OpticRec &op = S.optics[h.back ? e.opt_back : e.opt_front];
-                        const double tv = test_value<MIXED>(S, op, e.interaction, h.ce, h.n);
-                        if (tv <= rng.u()) absorbed = true;
-                        if (!absorbed) {
-                            double cin[3] = {h.ce[0], h.ce[1], h.ce[2]};
-                            if (S.sunshape_on && si == 0 && hits == 1) {
-                                double c2[3];
-                                error_sample<MIXED>(S, S.sun.shape, S.sun.sigma / 1000.0, cin, rng, false, h.n, c2);
-                                for (int q = 0; q < 3; ++q) cin[q] = c2[q];
-                            }
-                            double nrm[3] = {h.n[0], h.n[1], h.n[2]};
-                            if (S.errors_on) {
-                                double n2[3];
-                                const int d = op.dist;
-                                const int dd = (d == 'g' || d == 'G' || d == 'p' || d == 'P') ? d : 0;
-                                error_sample<MIXED>(S, dd, op.slope / 1000.0, nrm, rng, false, nrm, n2);
-                                for (int q = 0; q < 3; ++q) nrm[q] = n2[q];
-                            }
-                            if (e.interaction == 1)
-                                refract<MIXED>(op, cin, nrm, rng, cout);
-                            else
-                                reflect(cin, nrm, cout);
-                            if (S.errors_on) {
-                                const bool diffuse = (op.dist == 'f' || op.dist == 'F');
-                                double axis[3], c3[3];
-                                for (int q = 0; q < 3; ++q) axis[q] = diffuse ? nrm[q] : cout[q];
-                                error_sample<MIXED>(S, op.dist, op.spec / 1000.0, axis, rng, e.interaction == 2, nrm, c3);
-                                for (int q = 0; q < 3; ++q) cout[q] = c3[q];
-                            }
-                            for (int q = 0; q < 3; ++q) pout[q] = h.pe[q];
-                        }
-                    }
-                }
-                if (RECORDS) {
-                    const unsigned long long slot = warp_reserve(O.rec_count);
-                    if (slot < O.rec_cap) {
-                        RecordDev r;
-                        to_ref(e.R, e.o, h.pe, h.ce, r.pos, r.cos);
-                        r.element = absorbed ? -(j + 1) : (j + 1);
-                        r.stage = si + 1;
-                        r.raynum = raynum;
-                        r.seq = uint32_t(hits - 1);
-                        O.recs[slot] = r;
-                    }
-                }
-                if (S.n_flux) bin_flux<MIXED>(S, si, j, absorbed, h.pe);
-                if (absorbed) {
-                    warp_count(O.absorbed, st.first_elem + j);
-                    if (si == S.n_stages - 1 && first_elem0 >= 0) warp_count(O.delivered, first_elem0);
-                    break;
-                }
-                to_ref(e.R, e.o, pout, cout, ps, cs);
-                // A flat element cannot meet the ray leaving it: the next test's 1e-5 nudge moves
-                // the origin 1e-5 |cz| off the plane, behind the ray.  Skipped only when that
-                // offset exceeds the round-off of the local z (1e-13 of the coordinates,
-                // hundreds of ulps), so the skipped test is one that fails.
-                last_j = (e.stype == kSurfFlat &&
-                          1e-5 * fabs(cout[2]) >
-                              1e-13 * (1.0 + fabs(e.o[0]) + fabs(e.o[1]) + fabs(e.o[2]) + fabs(pout[0]) + fabs(pout[1])))
-                             ? j
-                             : -1;
-                if (!st.multihit) break;
-                if (hits >= kMaxHitsPerStage) {
-                    atomicOr(&sh_flags, unsigned(kFlagHitCap));
-                    break;
-                }
-            }
-            if (absorbed) break;
-            if (hits == 0) {
-                // a miss (raytrace.cpp:800-826): trace-through stages carry the ray on
-                // unchanged; both record the incoming ray with element 0.  The one miss
-                // the reference does not record (the stage's last ray in a
-                // trace-through stage) is removed on the host from max_ttmiss.
-                if (si == 0) break;  // cannot happen: first-stage rays are numbered hits
-                if (RECORDS) {
-                    const unsigned long long slot = warp_reserve(O.rec_count);
-                    if (slot < O.rec_cap) {
-                        RecordDev r;
-                        to_local(st.R, st.o, pg, cg, r.pos, r.cos);
-                        r.element = 0;
-                        r.stage = si + 1;
-                        r.raynum = raynum;
-                        r.seq = 0;
-                        O.recs[slot] = r;
-                    }
-                }
-                if (!st.tracethrough) break;
-                atomicMax(&sh_max_tt[si], raynum);
-                continue;  // global ray unchanged
-            }
-            to_ref(st.R, st.o, ps, cs, pg, cg);
-        }
-    }
-    // the last warp of the block to finish flushes the block's counters (no barrier,
-    // so finished warps never wait for the block's slowest ray)
-    __syncwarp();
-    unsigned last = 0;
-    if (lane == 0) {
-        __threadfence_block();
-        last = (atomicAdd(&sh_warps_done, 1u) == (kTraceBlock / 32) - 1) ? 1u : 0u;
-    }
-    last = __shfl_sync(0xffffffffu, last, 0);
-    if (last) {
-        __threadfence_block();
-        for (int s2 = lane; s2 < S.n_stages; s2 += 32) {
-            const unsigned long long ent = atomicAdd(&sh_entries[s2], 0ull);
-            if (ent) {
-                atomicAdd(&O.ctr->stage_entries[s2], ent);
-                atomicMax(&O.ctr->max_enter[s2], atomicMax(&sh_max_enter[s2], 0u));
-                const unsigned tt = atomicMax(&sh_max_tt[s2], 0u);
-                if (tt) atomicMax(&O.ctr->max_ttmiss[s2], tt);
+    const uint32_t stride = gridDim.x * kTraceBlock;
+    const uint32_t n_round = (n + 31u) & ~31u;  // whole warps in the loop (warp collectives)
+    for (uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x; i < n_round; i += stride) {
+        bool live = false;
+        WfRay r;
+        if (i < n) {
+            const uint32_t idx = hit_idx ? hit_idx[i] : i;
+            live = idx < take;
+            if (live) {
+                r.sid = hit_sid[i];
+                r.raynum = raynum_base + idx + 1;
+                RayRng rng;
+                rng.init(S.seed, r.sid, 0);
+                double xs, ys;
+                make_ray(S, r.sid, rng, r.p, r.c, xs, ys);
+                r.draw = rng.k;
+                r.si = 0;
+                r.hits = 0;
+                r.last_j = -1;
+                r.next_j = int(hit_el[i]);
+                r.fe0 = -1;
+                r.moved = true;
             }
         }
-        const unsigned fl = atomicOr(&sh_flags, 0u);
-        if (lane == 0 && fl) atomicOr(&O.ctr->flags, fl);
+        int status = kWfDone;
+        if (live) {
+            wf_stage_enter(c, 0, r.raynum);
+            // (an entry without a known element is searched in the first round)
+            status = (r.next_j >= 0) ? wf_shade<MIXED, RECORDS>(S, O, c, r) : int(kWfSearch);
+            if (status != kWfDone) wf_store(W, i, r, true);
+        }
+        wf_push(q_search, n_search, i, status != kWfDone);
     }
+    wf_ctr_flush(c, S, O);
+}
+
+// Search kernel: rays queued for a search; those that find an element go to the shade
+// queue, those that move on to another stage back to the search queue of the next round.
+template <int MIXED, int RECORDS>
+__global__ void __launch_bounds__(kTraceBlock, kWfSearchMinBlocks) k_wf_search(
+    SceneDev S, TraceOut O, WfState W, const uint32_t *q_in, const uint32_t *n_in, uint32_t *q_shade,
+    uint32_t *n_shade, uint32_t *q_next, uint32_t *n_next) {
+    __shared__ WfBlockCtr c;
+    wf_ctr_init(c);
+    const uint32_t n = *n_in;
+    const uint32_t stride = gridDim.x * kTraceBlock;
+    const uint32_t n_round = (n + 31u) & ~31u;
+    for (uint32_t q = blockIdx.x * kTraceBlock + threadIdx.x; q < n_round; q += stride) {
+        int status = kWfDone;
+        uint32_t i = 0;
+        if (q < n) {
+            i = q_in[q];
+            WfRay r = wf_load(W, i);
+            status = wf_search<MIXED, RECORDS>(S, O, c, r);
+            if (status != kWfDone) wf_store(W, i, r, false);
+        }
+        wf_push(q_shade, n_shade, i, status == kWfShade);
+        wf_push(q_next, n_next, i, status == kWfSearch);
+    }
+    wf_ctr_flush(c, S, O);
+}
+
+// Shade kernel: rays with a known element; survivors go to the next round's search queue.
+template <int MIXED, int RECORDS>
+__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_shade(
+    SceneDev S, TraceOut O, WfState W, const uint32_t *q_in, const uint32_t *n_in, uint32_t *q_next,
+    uint32_t *n_next) {
+    __shared__ WfBlockCtr c;
+    wf_ctr_init(c);
+    const uint32_t n = *n_in;
+    const uint32_t stride = gridDim.x * kTraceBlock;
+    const uint32_t n_round = (n + 31u) & ~31u;
+    for (uint32_t q = blockIdx.x * kTraceBlock + threadIdx.x; q < n_round; q += stride) {
+        int status = kWfDone;
+        uint32_t i = 0;
+        if (q < n) {
+            i = q_in[q];
+            WfRay r = wf_load(W, i);
+            status = wf_shade<MIXED, RECORDS>(S, O, c, r);
+            if (status != kWfDone) wf_store(W, i, r, false);
+        }
+        wf_push(q_next, n_next, i, status != kWfDone);
+    }
+    wf_ctr_flush(c, S, O);
+}
+
+// Finishing kernel: every ray still queued runs to its end, one step after the other.
+template <int MIXED, int RECORDS>
+__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_finish(SceneDev S, TraceOut O, WfState W,
+                                                                              const uint32_t *q_in,
+                                                                              const uint32_t *n_in) {
+    __shared__ WfBlockCtr c;
+    wf_ctr_init(c);
+    const uint32_t n = *n_in;
+    for (uint32_t q = blockIdx.x * kTraceBlock + threadIdx.x; q < n; q += gridDim.x * kTraceBlock) {
+        WfRay r = wf_load(W, q_in[q]);
+        int status = (r.next_j >= 0) ? int(kWfShade) : int(kWfSearch);
+        while (status != kWfDone)
+            status = (status == kWfShade) ? wf_shade<MIXED, RECORDS>(S, O, c, r) : wf_search<MIXED, RECORDS>(S, O, c, r);
+    }
+    wf_ctr_flush(c, S, O);
+}
+
+// Host side of the trace launch (instantiated per precision in its translation unit).
+template <int MIXED, int RECORDS>
+static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx,
+                     const uint32_t *total, const RunState *rs, const TraceOut &O, const WfState &W,
+                     const WfQueues &Q, cudaStream_t st) {
+    // persistent grids: every block the kernels can keep resident on every SM
+    static int per_sm[4] = {0, 0, 0, 0};
+    if (per_sm[0] == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_wf_first<MIXED, RECORDS>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_wf_search<MIXED, RECORDS>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_wf_shade<MIXED, RECORDS>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[3], k_wf_finish<MIXED, RECORDS>, kTraceBlock, 0);
+        for (int &x : per_sm) x = x > 0 ? x : 1;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int R = Q.rounds;
+    cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * (2 * R + 1), st);
+    k_wf_first<MIXED, RECORDS><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs, O, W,
+                                                                          Q.search[0], Q.counts);
+    for (int r = 0; r < R; ++r) {
+        uint32_t *c = Q.counts + 2 * r;
+        k_wf_search<MIXED, RECORDS><<<sms * per_sm[1], kTraceBlock, 0, st>>>(
+            S, O, W, Q.search[r & 1], c, Q.shade, c + 1, Q.search[(r + 1) & 1], c + 2);
+        k_wf_shade<MIXED, RECORDS><<<sms * per_sm[2], kTraceBlock, 0, st>>>(S, O, W, Q.shade, c + 1,
+                                                                           Q.search[(r + 1) & 1], c + 2);
+    }
+    k_wf_finish<MIXED, RECORDS><<<sms * per_sm[3], kTraceBlock, 0, st>>>(S, O, W, Q.search[R & 1], Q.counts + 2 * R);
+    return 2 + 2 * R;
 }
 
 }  // namespace stb
