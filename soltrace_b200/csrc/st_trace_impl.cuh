@@ -468,7 +468,7 @@ __device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed
 // kernels
 // ------------------------------------------------------------------------------------
 template <int MIXED>
-__global__ void __launch_bounds__(kProbeBlock) k_probe(SceneDev S, uint64_t s0, uint32_t n, uint32_t *hit_elem,
+__global__ void __launch_bounds__(kProbeBlock) k_probe(const __grid_constant__ SceneDev S, uint64_t s0, uint32_t n, uint32_t *hit_elem,
                                                         uint32_t *block_counts, const RunState *rs) {
     const uint32_t i = blockIdx.x * kProbeBlock + threadIdx.x;
     uint32_t h = 0;
@@ -505,7 +505,7 @@ __global__ void __launch_bounds__(kProbeBlock) k_probe(SceneDev S, uint64_t s0, 
 // On a heliostat field most sun rays miss every footprint and never reach the second
 // kernel, whose warps are then fully occupied by rays that need the element tests.
 template <int MIXED, int MINB>
-__global__ void __launch_bounds__(kResolveBlock, MINB) k_sun_resolve(SceneDev S, uint64_t s0, uint32_t *hit_elem,
+__global__ void __launch_bounds__(kResolveBlock, MINB) k_sun_resolve(const __grid_constant__ SceneDev S, uint64_t s0, uint32_t *hit_elem,
                                                                      uint32_t *block_counts, const uint32_t *cand,
                                                                      const uint32_t *cand_count, const RunState *rs) {
     if (rs->reached) return;
@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(kResolveBlock, MINB) k_sun_resolve(SceneDev S,
 
 #ifdef ST_COMMON_KERNELS
 // first kernel of the grid probe (above): misses written, candidates listed
-__global__ void __launch_bounds__(kProbeBlock) k_sun_candidates(SceneDev S, uint64_t s0, uint32_t n,
+__global__ void __launch_bounds__(kProbeBlock) k_sun_candidates(const __grid_constant__ SceneDev S, uint64_t s0, uint32_t n,
                                                                 uint32_t *hit_elem, uint32_t *block_counts,
                                                                 uint32_t *cand, uint32_t *cand_count,
                                                                 const RunState *rs) {
@@ -554,14 +554,23 @@ __global__ void __launch_bounds__(kProbeBlock) k_sun_candidates(SceneDev S, uint
             }
         if (!listed) hit_elem[i] = 0;
     }
+    // one atomic on the shared count per block: warp counts, their prefix, one reservation
+    __shared__ uint32_t wn[kProbeBlock / 32], base;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned bal = __ballot_sync(0xffffffffu, listed);
-    if (bal != 0) {
-        const int lane = threadIdx.x & 31, leader = __ffs(bal) - 1;
-        uint32_t base = 0;
-        if (lane == leader) base = atomicAdd(cand_count, uint32_t(__popc(bal)));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (listed) cand[base + __popc(bal & ((1u << lane) - 1u))] = i;
+    if (lane == 0) wn[w] = __popc(bal);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int k = 0; k < kProbeBlock / 32; ++k) {
+            const uint32_t x = wn[k];
+            wn[k] = t;
+            t += x;
+        }
+        base = t ? atomicAdd(cand_count, t) : 0u;
     }
+    __syncthreads();
+    if (listed) cand[base + wn[w] + __popc(bal & ((1u << lane) - 1u))] = i;
 }
 
 // exclusive scan of the per-block counts (one block; counts fit in 32 bits per batch)
@@ -747,16 +756,39 @@ __device__ __forceinline__ void wf_store(const WfState &W, uint32_t i, const WfR
         }
 }
 
-// append `slot` to a queue for every active lane with `want`; one atomic per warp
-__device__ __forceinline__ void wf_push(uint32_t *queue, uint32_t *count, uint32_t slot, bool want) {
-    const unsigned mask = __activemask();
-    const unsigned bal = __ballot_sync(mask, want);
-    if (bal == 0) return;
-    const int lane = threadIdx.x & 31, leader = __ffs(bal) - 1;
-    uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(count, uint32_t(__popc(bal)));
-    base = __shfl_sync(mask, base, leader);
-    if (want) queue[base + __popc(bal & ((1u << lane) - 1u))] = slot;
+// Append `slot` to queue A for every thread with `want_a` and to queue B for every thread
+// with `want_b`, with one global atomic per queue and block (a queue's count is a single
+// address that every block of the grid updates).  Called by all threads of the block.
+struct WfPushSh {
+    uint32_t na[kTraceBlock / 32], nb[kTraceBlock / 32];
+    uint32_t base_a, base_b;
+};
+__device__ __forceinline__ void wf_block_push(WfPushSh &sh, uint32_t *qa, uint32_t *ca, bool want_a, uint32_t *qb,
+                                              uint32_t *cb, bool want_b, uint32_t slot) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned ba = __ballot_sync(0xffffffffu, want_a), bb = __ballot_sync(0xffffffffu, want_b);
+    if (lane == 0) {
+        sh.na[w] = __popc(ba);
+        sh.nb[w] = __popc(bb);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t ta = 0, tb = 0;
+        for (int k = 0; k < kTraceBlock / 32; ++k) {
+            const uint32_t a = sh.na[k], b = sh.nb[k];
+            sh.na[k] = ta;  // exclusive prefix over the warps
+            sh.nb[k] = tb;
+            ta += a;
+            tb += b;
+        }
+        sh.base_a = ta ? atomicAdd(ca, ta) : 0u;
+        sh.base_b = tb ? atomicAdd(cb, tb) : 0u;
+    }
+    __syncthreads();
+    const unsigned lt = (1u << lane) - 1u;
+    if (want_a) qa[sh.base_a + sh.na[w] + __popc(ba & lt)] = slot;
+    if (want_b) qb[sh.base_b + sh.nb[w] + __popc(bb & lt)] = slot;
+    __syncthreads();  // sh is reused by the next call
 }
 
 // a ray enters stage si: entry count and largest ray number (raytrace.cpp:617-623)
@@ -945,9 +977,10 @@ __device__ __forceinline__ int wf_shade(const SceneDev &S, const TraceOut &O, Wf
 // stage and are shaded on the element the probe found.
 template <int MIXED, int RECORDS>
 __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_first(
-    SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx, const uint32_t *total,
+    const __grid_constant__ SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx, const uint32_t *total,
     const RunState *rs, TraceOut O, WfState W, uint32_t *q_search, uint32_t *n_search) {
     __shared__ WfBlockCtr c;
+    __shared__ WfPushSh psh;
     wf_ctr_init(c);
     uint32_t n = 0, take = 0, raynum_base = 0;
     if (!rs->reached) {
@@ -958,7 +991,8 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_first(
     }
     if (!hit_idx) n = take;
     const uint32_t stride = gridDim.x * kTraceBlock;
-    const uint32_t n_round = (n + 31u) & ~31u;  // whole warps in the loop (warp collectives)
+    // whole blocks in the loop (block-wide queue appends)
+    const uint32_t n_round = (n + kTraceBlock - 1) / kTraceBlock * kTraceBlock;
     for (uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x; i < n_round; i += stride) {
         bool live = false;
         WfRay r;
@@ -988,7 +1022,7 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_first(
             status = (r.next_j >= 0) ? wf_shade<MIXED, RECORDS>(S, O, c, r) : int(kWfSearch);
             if (status != kWfDone) wf_store(W, i, r, true);
         }
-        wf_push(q_search, n_search, i, status != kWfDone);
+        wf_block_push(psh, q_search, n_search, status != kWfDone, q_search, n_search, false, i);
     }
     wf_ctr_flush(c, S, O);
 }
@@ -997,13 +1031,14 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_first(
 // queue, those that move on to another stage back to the search queue of the next round.
 template <int MIXED, int RECORDS>
 __global__ void __launch_bounds__(kTraceBlock, kWfSearchMinBlocks) k_wf_search(
-    SceneDev S, TraceOut O, WfState W, const uint32_t *q_in, const uint32_t *n_in, uint32_t *q_shade,
+    const __grid_constant__ SceneDev S, TraceOut O, WfState W, const uint32_t *q_in, const uint32_t *n_in, uint32_t *q_shade,
     uint32_t *n_shade, uint32_t *q_next, uint32_t *n_next) {
     __shared__ WfBlockCtr c;
+    __shared__ WfPushSh psh;
     wf_ctr_init(c);
     const uint32_t n = *n_in;
     const uint32_t stride = gridDim.x * kTraceBlock;
-    const uint32_t n_round = (n + 31u) & ~31u;
+    const uint32_t n_round = (n + kTraceBlock - 1) / kTraceBlock * kTraceBlock;
     for (uint32_t q = blockIdx.x * kTraceBlock + threadIdx.x; q < n_round; q += stride) {
         int status = kWfDone;
         uint32_t i = 0;
@@ -1013,8 +1048,7 @@ __global__ void __launch_bounds__(kTraceBlock, kWfSearchMinBlocks) k_wf_search(
             status = wf_search<MIXED, RECORDS>(S, O, c, r);
             if (status != kWfDone) wf_store(W, i, r, false);
         }
-        wf_push(q_shade, n_shade, i, status == kWfShade);
-        wf_push(q_next, n_next, i, status == kWfSearch);
+        wf_block_push(psh, q_shade, n_shade, status == kWfShade, q_next, n_next, status == kWfSearch, i);
     }
     wf_ctr_flush(c, S, O);
 }
@@ -1022,13 +1056,14 @@ __global__ void __launch_bounds__(kTraceBlock, kWfSearchMinBlocks) k_wf_search(
 // Shade kernel: rays with a known element; survivors go to the next round's search queue.
 template <int MIXED, int RECORDS>
 __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_shade(
-    SceneDev S, TraceOut O, WfState W, const uint32_t *q_in, const uint32_t *n_in, uint32_t *q_next,
+    const __grid_constant__ SceneDev S, TraceOut O, WfState W, const uint32_t *q_in, const uint32_t *n_in, uint32_t *q_next,
     uint32_t *n_next) {
     __shared__ WfBlockCtr c;
+    __shared__ WfPushSh psh;
     wf_ctr_init(c);
     const uint32_t n = *n_in;
     const uint32_t stride = gridDim.x * kTraceBlock;
-    const uint32_t n_round = (n + 31u) & ~31u;
+    const uint32_t n_round = (n + kTraceBlock - 1) / kTraceBlock * kTraceBlock;
     for (uint32_t q = blockIdx.x * kTraceBlock + threadIdx.x; q < n_round; q += stride) {
         int status = kWfDone;
         uint32_t i = 0;
@@ -1038,14 +1073,14 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_shade(
             status = wf_shade<MIXED, RECORDS>(S, O, c, r);
             if (status != kWfDone) wf_store(W, i, r, false);
         }
-        wf_push(q_next, n_next, i, status != kWfDone);
+        wf_block_push(psh, q_next, n_next, status != kWfDone, q_next, n_next, false, i);
     }
     wf_ctr_flush(c, S, O);
 }
 
 // Finishing kernel: every ray still queued runs to its end, one step after the other.
 template <int MIXED, int RECORDS>
-__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_finish(SceneDev S, TraceOut O, WfState W,
+__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_finish(const __grid_constant__ SceneDev S, TraceOut O, WfState W,
                                                                               const uint32_t *q_in,
                                                                               const uint32_t *n_in) {
     __shared__ WfBlockCtr c;
