@@ -26,8 +26,19 @@ void launch_advance(const uint32_t *total, const uint64_t *hit_sid, uint64_t s0,
 void launch_sort_by_element(const uint32_t *total, const uint64_t *hit_sid, const uint32_t *hit_el, uint32_t n_elem0,
                             uint32_t *elem_count, uint32_t *elem_cursor, uint32_t *scratch_total, uint64_t *s_sid,
                             uint32_t *s_el, uint32_t *s_idx, uint32_t max_n, cudaStream_t st) {
-    const uint32_t blocks = std::max(1u, std::min<uint32_t>((max_n + 255) / 256, 148u * 8u));
     cudaMemsetAsync(elem_count, 0, size_t(n_elem0) * 4, st);
+    if (n_elem0 <= uint32_t(kSortBins)) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const uint32_t blocks = std::max(1u, std::min<uint32_t>((max_n + 4095) / 4096, uint32_t(2 * sms)));
+        k_elem_hist_sh<<<blocks, kSortBlock, 0, st>>>(total, hit_el, n_elem0, elem_count);
+        k_offsets<<<1, 1024, 0, st>>>(elem_count, n_elem0, elem_cursor, scratch_total);
+        k_elem_scatter_sh<<<blocks, kSortBlock, 0, st>>>(total, hit_sid, hit_el, n_elem0, elem_cursor, s_sid, s_el,
+                                                          s_idx);
+        return;
+    }
+    const uint32_t blocks = std::max(1u, std::min<uint32_t>((max_n + 255) / 256, 148u * 8u));
     k_elem_hist<<<blocks, 256, 0, st>>>(total, hit_el, elem_count);
     k_offsets<<<1, 1024, 0, st>>>(elem_count, n_elem0, elem_cursor, scratch_total);
     k_elem_scatter<<<blocks, 256, 0, st>>>(total, hit_sid, hit_el, elem_cursor, s_sid, s_el, s_idx);

@@ -175,12 +175,15 @@ __device__ inline int nearest_grid(const SceneDev &S, const StageRec &st, const 
     const float pad_o = 2e-6f * (fabsf(ox) + fabsf(oy) + fabsf(oz));
     int best = -1;
     double bp = 1e99;
+    // the candidate list lives in shared memory, [slot][thread] (blocks have at most 256
+    // threads), so that it neither takes registers nor goes to local memory
     constexpr int kCand = 8;
-    int cand[kCand];
+    __shared__ int cand_sh[kCand * 256];
+    int *cand = cand_sh + threadIdx.x;
     int nc = 0;
     auto flush = [&]() {
         for (int c = 0; c < nc; ++c) {
-            const int j = cand[c];
+            const int j = cand[256 * c];
             double pl;
             if (element_test<MIXED>(S, S.elems[st.first_elem + j], ps, cs, pl, nullptr) &&
                 (pl < bp || (pl == bp && j < best))) {
@@ -211,7 +214,7 @@ __device__ inline int nearest_grid(const SceneDev &S, const StageRec &st, const 
             seen2 = seen1;
             seen1 = j;
             if (nc == kCand) flush();
-            cand[nc++] = j;
+            cand[256 * nc++] = j;
         }
         // step to the next cell along the ray
         if (tmx < tmy) {
@@ -646,6 +649,51 @@ __global__ void __launch_bounds__(256) k_elem_scatter(const uint32_t *total, con
     for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
         const uint32_t e = hit_el[i];
         const uint32_t pos = atomicAdd(&elem_cursor[e], 1u);
+        s_sid[pos] = hit_sid[i];
+        s_el[pos] = e;
+        s_idx[pos] = i;
+    }
+}
+
+// The same counting sort for first stages of at most kSortBins elements, with the counts
+// kept per block in shared memory: each block takes a contiguous chunk of the hit list,
+// counts its elements there and adds its non-zero counts to the global ones (hist), or
+// reserves one range per element in the output with a single global atomic and hands out
+// the places in it from shared memory (scatter).  Global atomics: one per block and
+// element present, instead of one per hit.
+constexpr int kSortBins = 11264;
+constexpr int kSortBlock = 1024;
+__global__ void __launch_bounds__(kSortBlock) k_elem_hist_sh(const uint32_t *total, const uint32_t *hit_el,
+                                                             uint32_t n_elem, uint32_t *elem_count) {
+    __shared__ uint32_t h[kSortBins];
+    const uint32_t n = *total;
+    const uint32_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const uint32_t a = min(n, blockIdx.x * chunk), b = min(n, a + chunk);
+    for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock) h[e] = 0;
+    __syncthreads();
+    for (uint32_t i = a + threadIdx.x; i < b; i += kSortBlock) atomicAdd(&h[hit_el[i]], 1u);
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock)
+        if (h[e]) atomicAdd(&elem_count[e], h[e]);
+}
+__global__ void __launch_bounds__(kSortBlock) k_elem_scatter_sh(const uint32_t *total, const uint64_t *hit_sid,
+                                                                const uint32_t *hit_el, uint32_t n_elem,
+                                                                uint32_t *elem_cursor, uint64_t *s_sid, uint32_t *s_el,
+                                                                uint32_t *s_idx) {
+    __shared__ uint32_t h[kSortBins];
+    const uint32_t n = *total;
+    const uint32_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const uint32_t a = min(n, blockIdx.x * chunk), b = min(n, a + chunk);
+    for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock) h[e] = 0;
+    __syncthreads();
+    for (uint32_t i = a + threadIdx.x; i < b; i += kSortBlock) atomicAdd(&h[hit_el[i]], 1u);
+    __syncthreads();
+    for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock)
+        if (h[e]) h[e] = atomicAdd(&elem_cursor[e], h[e]);
+    __syncthreads();
+    for (uint32_t i = a + threadIdx.x; i < b; i += kSortBlock) {
+        const uint32_t e = hit_el[i];
+        const uint32_t pos = atomicAdd(&h[e], 1u);
         s_sid[pos] = hit_sid[i];
         s_el[pos] = e;
         s_idx[pos] = i;
