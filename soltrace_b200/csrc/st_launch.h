@@ -16,7 +16,7 @@ constexpr int kProbeVariants = 3;
 constexpr int kProbeMinBlocks[kProbeVariants] = {4, 6, 8};
 // resident blocks per SM asked of the trace's shade and search kernels (register budget)
 constexpr int kWfShadeMinBlocks = 4;
-constexpr int kWfSearchMinBlocks = 6;
+constexpr int kWfSearchMinBlocks = 4;
 
 enum RunFlags : unsigned {
     kFlagHitCap = 1u,         // a ray reached kMaxHitsPerStage in one stage
