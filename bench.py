@@ -40,6 +40,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 from soltrace_b200 import flops_model as fm  # noqa: E402
+from soltrace_b200 import parallel  # noqa: E402
 from soltrace_b200 import scenes  # noqa: E402
 
 METRIC = "ray-stage intersections/s on 1 B200, mixed vs FP64, at <=0.5% flux-map L2 error"
@@ -197,6 +198,20 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------------------------------
+def traffic_per_unit() -> dict:
+    """{group: DRAM bytes per unit} from the table in profiles/traffic.md."""
+    out = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.md")) as f:
+            for line in f:
+                cells = [c.strip() for c in line.strip().strip("|").split("|")]
+                if len(cells) >= 3 and cells[0] in ("probe group", "trace group"):
+                    out[cells[0]] = float(cells[1])
+    except (OSError, ValueError):
+        pass
+    return out
+
+
 # B200 arm
 # ---------------------------------------------------------------------------------------
 def main():
@@ -238,7 +253,7 @@ def main():
         st["flux"] = api.flux(ctx, 0, FLUX_MAP[3], FLUX_MAP[4])
         return st
 
-    seed0 = args.seed + 1000 * rank
+    seed0 = parallel.rank_seed(args.seed, rank)
     for k in range(args.warmup):
         step(1, seed0 + k)
 
@@ -268,16 +283,10 @@ def main():
     l2 = [float(np.linalg.norm(runs[k]["flux"].astype(float) - runs64[k]["flux"].astype(float)) /
                 max(np.linalg.norm(runs64[k]["flux"].astype(float)), 1e-30)) for k in range(n64)]
 
-    flux_sum = runs[-1]["flux"].astype(np.int64)
-    if dist:
-        t = torch.tensor([units, wall_ms], dtype=torch.float64, device="cuda")
-        tmax = torch.tensor([dev_ms, wall_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        units, dev_ms, wall_ms = t[0].item(), tmax[0].item(), tmax[1].item()
-        fx = torch.from_numpy(flux_sum).cuda()
-        dist.all_reduce(fx, op=dist.ReduceOp.SUM)  # combined receiver map of all ranks
-        flux_sum = fx.cpu().numpy()
+    # whole-job totals: units summed, device and wall times max over ranks, the receiver
+    # flux maps of all ranks summed (one NCCL all-reduce each; no-ops on one rank)
+    units, dev_ms, wall_ms, flux_sum = parallel.combine(units, dev_ms, wall_ms, runs[-1]["flux"],
+                                                        device="cuda" if dist else "cpu")
     if rank != 0:
         api.st_free_context(ctx)
         if dist:
@@ -300,18 +309,25 @@ def main():
     probe_tflops = pf / (probe_ms / 1e3) / 1e12
     trace_tflops = tf / (trace_ms / 1e3) / 1e12
     dominant = "k_probe" if probe_ms >= trace_ms else "k_trace"
+    # DRAM bytes per unit of each launch group, from the ncu captures summarised in
+    # profiles/traffic.md, scaled to this step's units
     traffic = None
-    try:
-        traffic = json.load(open(os.path.join(ROOT, "profiles", "traffic.json"))).get(dominant)
-    except (OSError, ValueError):
-        pass
+    per_unit = traffic_per_unit()
+    if dominant == "k_probe" and "probe group" in per_unit:
+        traffic = per_unit["probe group"] * sun_rays / len(runs)
+    elif dominant == "k_trace" and "trace group" in per_unit:
+        traffic = per_unit["trace group"] * hits / len(runs)
     if dominant == "k_probe":
         ach, pk = probe_tflops, fm.NOMINAL_FP64_TFLOPS
         hbm_ach = fm.probe_bytes(sun_rays, hits) / (probe_ms / 1e3) / 1e9
     else:
         ach, pk = trace_tflops, fm.NOMINAL_FP64_TFLOPS
         hbm_ach = fm.trace_bytes(hits) / (trace_ms / 1e3) / 1e9
-    roofline = {"bound": "fp64", "kernel": dominant, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+    group = {"k_probe": "probe group (k_sun_candidates, k_sun_resolve, k_offsets, k_compact, element sort)",
+             "k_trace": "trace group (k_wf_first, k_wf_search, k_wf_shade, k_wf_finish)"}[dominant]
+    roofline = {"bound": "fp64", "kernel": group, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                "scope": "per step: the group's launches of every batch, timed by CUDA events around them",
+                "traffic_unit": "DRAM bytes per step (ncu per-unit figures scaled)",
                 "frac": ach / pk, "peak_source": "nominal (148 SMs x 64 FP64 lanes x 2 x 1965 MHz); "
                                                  "no measured FP64 vector peak on this pool",
                 "traffic": traffic,
@@ -340,6 +356,7 @@ def main():
         "autotuned_variants": {"probe": runs[-1]["probe_variant"], "trace": runs[-1]["trace_variant"],
                                "fp64_trace": runs64[-1]["trace_variant"]},
         "units_per_step": units / len(runs), "sun_rays_per_step": sun_rays / len(runs),
+        "receiver_flux_counts_all_ranks": int(flux_sum.sum()),
         "roofline": roofline, "clocks": clk.summary(), "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)

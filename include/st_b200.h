@@ -41,10 +41,16 @@ int st_b200_set_device(st_context_t pcxt, int device);
 int st_b200_explicit_rays(st_context_t pcxt, st_uint_t n, const double *pos, const double *cos);
 
 /* Flux maps binned on the device at every intersection with (stage, element)
- * (1-based, as in the records).  kind 0: element-local x in [x0,x1) by y in [y0,y1);
- * kind 1: cylinder, angle atan2(x, z - x1) + pi over [0, 2 pi) (x1 is the
- * radius) by axial y in [y0,y1).  absorbed_only selects absorbed intersections.
- * Returns the map index. */
+ * (1-based, as in the records), in element-local coordinates (x, y, z).
+ *   kind 0: x in [x0,x1) by y in [y0,y1), bins [lower, upper) (pysoltrace's flat map,
+ *           pysoltrace.py:1926-1929);
+ *   kind 1: cylinder of radius x1: angle atan2(x, z - x1) + pi over [0, 2 pi) by y in
+ *           [y0,y1) (pysoltrace's cylinder map, pysoltrace.py:1937-1942; x0 unused);
+ *   kind 2: flat, the GUI's rule (app/src/project.cpp:1392-1403): bins (lower, upper]
+ *           over [x0,x1] by [y0,y1];
+ *   kind 3: full cylinder of radius x1, the GUI's unwrapped arc length over
+ *           [-pi x1, pi x1] (project.cpp:1370-1378) by y, bins (lower, upper].
+ * absorbed_only selects absorbed intersections.  Returns the map index. */
 int st_b200_add_flux_map(st_context_t pcxt, int stage, int element, int kind, int nx, int ny, double x0, double x1,
                          double y0, double y1, int absorbed_only);
 int st_b200_clear_flux_maps(st_context_t pcxt);
@@ -65,8 +71,25 @@ typedef struct st_b200_stats {
     unsigned long long h2d_bytes;         /* host -> device bytes copied by the run */
     unsigned long long d2h_bytes;         /* device -> host bytes copied by the run */
     int probe_variant, trace_variant;     /* autotuned kernel variants used */
+    unsigned long long intersections;     /* records of the run by the reference's rules,
+                                             counted on the device when records are off */
 } st_b200_stats;
 int st_b200_run_stats(st_context_t pcxt, st_b200_stats *out);
+
+/* Flux statistics of map `map` after a run, as the SolTrace GUI reports them for an element
+ * (app/src/project.cpp:1139-1288), for direct normal irradiance `dni` (W/m2):
+ * power per ray = dni x sun-box area / SunRayCount; flux of a bin = its count x power per
+ * ray / bin area (W/m2); peak and minimum over the bins (the first in x-major order on
+ * ties), mean, population standard deviation, uniformity = sigma / mean, and the Monte-
+ * Carlo uncertainties 100/sqrt(rays in the peak bin) and 100/sqrt(run intersections), in %.
+ * Bin areas: (x1-x0)/nx x (y1-y0)/ny, with 2 pi x1 / nx across a cylinder. */
+typedef struct st_b200_flux_stats_t {
+    double peak_flux, min_flux, ave_flux, sigma_flux, uniformity;
+    double peak_flux_uncertainty, ave_flux_uncertainty;
+    double power_per_ray, bin_area;
+    unsigned long long rays_binned, rays_in_peak_bin, rays_in_min_bin;
+} st_b200_flux_stats_t;
+int st_b200_flux_stats(st_context_t pcxt, int map, double dni, st_b200_flux_stats_t *out);
 
 /* Per-element ray accounting of the last run for a stage (1-based): first_hits[e]
  * counts rays whose first intersection in that stage was element e+1; absorbed[e]

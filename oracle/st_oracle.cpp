@@ -2503,12 +2503,34 @@ int st_oracle_explicit_rays(void *p, st_uint_t n, const double *pos, const doubl
 // kind 0: planar bins over element-local x in [x0,x1), y in [y0,y1);
 // kind 1: cylinder bins, angle atan2(x, z - r) + pi over [0, 2 pi) x axial y in [y0, y1)
 //          with r = x1 (the cylinder radius).  absorbed_only selects element == -target.
+// GUI statistics binning (app/src/project.cpp:1367-1403): bin g is the smallest g >= -1
+// with vmin + (g+1) b >= v, counted only when 0 <= g < n; a full cylinder unwraps x to
+// the arc length R asin(x/R) on the front half, +-(pi R/2 + R acos(|x|/R)) behind it.
+static int oracle_gui_bin(double v, double vmin, double b, int n) {
+    if (!(v > vmin - b) || !(v <= vmin + (n + 1) * b)) return -1;
+    int g = -1;
+    while (g + 1 <= n && vmin + (g + 1) * b < v) g++;
+    return (g >= 0 && g < n) ? g : -1;
+}
+static double oracle_gui_arc(double x, double z, double R) {
+    if (z <= R) return R * asin(x / R);
+    return (x < 0) ? -(kPi * R / 2.0 + R * acos(fabs(x) / R)) : kPi * R / 2.0 + R * acos(x / R);
+}
+
 int st_oracle_flux(void *p, int stage, int element, int kind, int nx, int ny, double x0, double x1, double y0,
                    double y1, int absorbed_only, unsigned long long *bins) {
     CTX(p, -1);
     for (const Record &r : cx->all) {
         if (r.stage != stage) continue;
         if (absorbed_only ? r.element != -element : (r.element != element && r.element != -element)) continue;
+        if (kind >= 2) {
+            const int ix = kind == 2 ? oracle_gui_bin(r.loc[0], x0, (x1 - x0) / nx, nx)
+                                     : oracle_gui_bin(oracle_gui_arc(r.loc[0], r.loc[2], x1), -kPi * x1,
+                                                      2.0 * kPi * x1 / nx, nx);
+            const int iy = oracle_gui_bin(r.loc[1], y0, (y1 - y0) / ny, ny);
+            if (ix >= 0 && iy >= 0) bins[size_t(iy) * nx + ix]++;
+            continue;
+        }
         double u, v, u0, u1;
         if (kind == 0) {
             u = r.loc[0];

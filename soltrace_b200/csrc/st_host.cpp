@@ -1291,6 +1291,7 @@ int run(Context *cx, unsigned seed) {
     if (cx->want_records) assemble_records(cx, rr);
     S.readback_ms = rr.readback_ms + std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
     S.records = cx->records.size();
+    S.intersections = cx->want_records ? uint64_t(cx->records.size()) : rr.intersections;
     return int(cx->records.size());
 }
 
@@ -1803,7 +1804,8 @@ int st_b200_explicit_rays(st_context_t p, st_uint_t n, const double *pos, const 
 int st_b200_add_flux_map(st_context_t p, int stage, int element, int kind, int nx, int ny, double x0, double x1,
                          double y0, double y1, int absorbed_only) {
     CTX(p, -1);
-    if (cx->flux.size() >= size_t(kMaxFluxMaps) || nx <= 0 || ny <= 0 || stage < 1 || element < 1 || (kind != 0 && kind != 1)) {
+    if (cx->flux.size() >= size_t(kMaxFluxMaps) || nx <= 0 || ny <= 0 || stage < 1 || element < 1 || kind < 0 ||
+        kind > 3 || !(x1 > x0 || kind == 1 || kind == 3) || !(y1 > y0) || ((kind == 1 || kind == 3) && !(x1 > 0))) {
         cx->log("invalid flux map request");
         return -1;
     }
@@ -1823,6 +1825,63 @@ int st_b200_flux_counts(st_context_t p, int map, unsigned long long *counts) {
     const auto &c = cx->flux[map].counts;
     const size_t n = size_t(cx->flux[map].req.nx) * cx->flux[map].req.ny;
     for (size_t i = 0; i < n; ++i) counts[i] = i < c.size() ? c[i] : 0ull;
+    return 1;
+}
+// Flux statistics of a map, as the GUI computes them for an element
+// (app/src/project.cpp:1139-1288): power per ray from the sun box and SunRayCount, flux =
+// count x power per ray / bin area, peak and minimum (first bin in x-major order on ties),
+// mean, population standard deviation, uniformity = sigma / mean, and the Monte-Carlo
+// uncertainties 100/sqrt(rays in the peak bin) and 100/sqrt(intersections of the run), %.
+int st_b200_flux_stats(st_context_t p, int map, double dni, st_b200_flux_stats_t *out) {
+    CTX(p, -1);
+    if (map < 0 || size_t(map) >= cx->flux.size() || !out) return -1;
+    const FluxMap &fm = cx->flux[map];
+    const FluxMapReq &q = fm.req;
+    const size_t nb = size_t(q.nx) * q.ny;
+    if (fm.counts.size() != nb || cx->sun_rays == 0) {
+        cx->log("flux statistics need a completed run");
+        return -1;
+    }
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    const double bx = (q.kind == 1 || q.kind == 3) ? two_pi * q.x1 / q.nx : (q.x1 - q.x0) / q.nx;
+    const double by = (q.y1 - q.y0) / q.ny;
+    st_b200_flux_stats_t r;
+    memset(&r, 0, sizeof r);
+    r.power_per_ray = dni * (cx->sun.xmax - cx->sun.xmin) * (cx->sun.ymax - cx->sun.ymin) / double(cx->sun_rays);
+    r.bin_area = bx * by;
+    const double zs = r.power_per_ray / r.bin_area;
+    double sum = 0, sum2 = 0, peak = 0, mn = 1e99;
+    unsigned long long npeak = 0, nmin = 0, binned = 0;
+    bool have_peak = false;
+    for (int ix = 0; ix < q.nx; ++ix)
+        for (int iy = 0; iy < q.ny; ++iy) {
+            const unsigned long long c = fm.counts[size_t(iy) * q.nx + ix];
+            const double z = double(c) * zs;
+            binned += c;
+            sum += z;
+            sum2 += z * z;
+            if (z > peak) {
+                peak = z;
+                npeak = c;
+                have_peak = true;
+            }
+            if (z < mn) {
+                mn = z;
+                nmin = c;
+            }
+        }
+    const double n = double(nb);
+    r.peak_flux = peak;
+    r.min_flux = mn;
+    r.ave_flux = sum / n;
+    r.sigma_flux = sqrt((n * sum2 - sum * sum) / (n * n));
+    r.uniformity = r.sigma_flux / r.ave_flux;
+    r.peak_flux_uncertainty = have_peak ? 100.0 / sqrt(double(npeak)) : INFINITY;
+    r.ave_flux_uncertainty = cx->stats.intersections ? 100.0 / sqrt(double(cx->stats.intersections)) : INFINITY;
+    r.rays_binned = binned;
+    r.rays_in_peak_bin = npeak;
+    r.rays_in_min_bin = nmin;
+    *out = r;
     return 1;
 }
 int st_b200_run_stats(st_context_t p, st_b200_stats *out) {

@@ -62,6 +62,7 @@ struct RunResult {
     double probe_ms = 0, trace_ms = 0, setup_ms = 0, readback_ms = 0;
     int batches = 0, gpu_launches = 0;
     unsigned flags = 0;
+    uint64_t intersections = 0;  // records of the run by the reference's rules, kept or not
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
     int probe_variant = 0, trace_variant = 0;
 };

@@ -503,6 +503,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             out.max_ttmiss[s] = c.max_ttmiss[s];
         }
         out.flags = c.flags;
+        out.intersections = c.records;
         out.first_hits.assign(accv.begin(), accv.begin() + ne);
         out.absorbed.assign(accv.begin() + ne, accv.begin() + 2 * ne);
         out.delivered.assign(accv.begin() + 2 * ne, accv.begin() + 3 * ne);

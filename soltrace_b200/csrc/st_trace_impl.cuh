@@ -426,6 +426,26 @@ __device__ __forceinline__ void warp_count(unsigned long long *base, int idx) {
     if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&base[idx], (unsigned long long)__popc(peers));
 }
 
+// Bin of value v on n bins of width b from vmin, by the GUI's rule: the smallest g >= -1
+// with vmin + (g + 1) b >= v (app/src/project.cpp:1392-1396; bins are (lower, upper]);
+// -1 when v is outside.
+__host__ __device__ inline int gui_bin(double v, double vmin, double b, int n) {
+    const double q = (v - vmin) / b;
+    if (!(q > -1.0) || !(q <= double(n) + 1.0)) return -1;  // outside (and NaN)
+    int g = int(ceil(q)) - 1;
+    if (g < -1) g = -1;
+    while (g + 1 <= n && vmin + (g + 1) * b < v) ++g;
+    while (g >= 0 && !(vmin + g * b < v)) --g;
+    return (g >= 0 && g < n) ? g : -1;
+}
+
+// The GUI's unwrapped arc length of a point on a full cylinder of radius R about the local
+// y axis (app/src/project.cpp:1370-1378).
+__host__ __device__ inline double gui_cyl_arc(double x, double z, double R) {
+    if (z <= R) return R * asin(x / R);
+    return (x < 0) ? -(kPiD * R / 2.0 + R * acos(fabs(x) / R)) : kPiD * R / 2.0 + R * acos(x / R);
+}
+
 template <int MIXED>
 __device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed, const double pe[3]) {
     for (int m = 0; m < S.n_flux; ++m) {
@@ -433,7 +453,15 @@ __device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed
         if (f.stage != si || f.elem != ej) continue;
         if (f.absorbed_only && !absorbed) continue;
         int ix, iy;
-        if (MIXED) {
+        if (f.kind >= 2) {  // the GUI's statistics rules, in double
+            if (f.kind == 2) {
+                ix = gui_bin(pe[0], f.x0, (f.x1 - f.x0) / f.nx, f.nx);
+            } else {
+                const double R = f.x1;
+                ix = gui_bin(gui_cyl_arc(pe[0], pe[2], R), -kPiD * R, 2.0 * kPiD * R / f.nx, f.nx);
+            }
+            iy = gui_bin(pe[1], f.y0, (f.y1 - f.y0) / f.ny, f.ny);
+        } else if (MIXED) {
             float u, u0, u1;
             if (f.kind == 0) {
                 u = float(pe[0]);
@@ -743,6 +771,7 @@ struct WfRay {
 
 struct WfBlockCtr {
     unsigned long long entries[kMaxStages];
+    unsigned long long intersections;  // records the reference would write (hits and misses)
     unsigned int max_enter[kMaxStages], max_tt[kMaxStages];
     unsigned int flags;
 };
@@ -753,7 +782,10 @@ __device__ __forceinline__ void wf_ctr_init(WfBlockCtr &c) {
         c.max_enter[threadIdx.x] = 0;
         c.max_tt[threadIdx.x] = 0;
     }
-    if (threadIdx.x == 0) c.flags = 0;
+    if (threadIdx.x == 0) {
+        c.flags = 0;
+        c.intersections = 0;
+    }
     __syncthreads();
 }
 
@@ -768,6 +800,13 @@ __device__ __forceinline__ void wf_ctr_flush(WfBlockCtr &c, const SceneDev &S, c
         if (c.max_tt[s]) atomicMax(&O.ctr->max_ttmiss[s], c.max_tt[s]);
     }
     if (threadIdx.x == 0 && c.flags) atomicOr(&O.ctr->flags, c.flags);
+    if (threadIdx.x == 0 && c.intersections) atomicAdd(&O.ctr->records, c.intersections);
+}
+
+// one more intersection record (counted whether or not records are kept)
+__device__ __forceinline__ void wf_count_record(WfBlockCtr &c) {
+    const unsigned mask = __activemask();
+    if ((threadIdx.x & 31) == __ffs(mask) - 1) atomicAdd(&c.intersections, (unsigned long long)__popc(mask));
 }
 
 __device__ __forceinline__ WfRay wf_load(const WfState &W, uint32_t i) {
@@ -860,6 +899,7 @@ __device__ __forceinline__ int wf_exit_stage(const SceneDev &S, const TraceOut &
     const StageRec &st = S.stages[r.si];
     if (r.hits == 0) {
         if (r.si == 0) return kWfDone;  // cannot happen: first-stage rays are numbered hits
+        wf_count_record(c);
         if (RECORDS) {
             const unsigned long long slot = warp_reserve(O.rec_count);
             if (slot < O.rec_cap) {
@@ -979,6 +1019,7 @@ __device__ __forceinline__ int wf_shade(const SceneDev &S, const TraceOut &O, Wf
         }
     }
     r.draw = rng.k;
+    wf_count_record(c);
     if (RECORDS) {
         const unsigned long long slot = warp_reserve(O.rec_count);
         if (slot < O.rec_cap) {

@@ -37,7 +37,16 @@ class Stats(C.Structure):
         ("d2h_bytes", C.c_ulonglong),
         ("probe_variant", C.c_int),
         ("trace_variant", C.c_int),
+        ("intersections", C.c_ulonglong),
     ]
+
+
+class FluxStats(C.Structure):
+    """st_b200_flux_stats_t: the GUI's element flux statistics of one flux map."""
+    _fields_ = [(k, C.c_double) for k in ("peak_flux", "min_flux", "ave_flux", "sigma_flux", "uniformity",
+                                          "peak_flux_uncertainty", "ave_flux_uncertainty", "power_per_ray",
+                                          "bin_area")] + \
+               [(k, C.c_ulonglong) for k in ("rays_binned", "rays_in_peak_bin", "rays_in_min_bin")]
 
 
 _u64p = C.POINTER(C.c_ulonglong)
@@ -52,6 +61,7 @@ EXTENSIONS = {
     "st_b200_flux_counts": (C.c_int, [C.c_void_p, C.c_int, _u64p]),
     "st_b200_run_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "st_b200_element_counts": (C.c_int, [C.c_void_p, C.c_int, _u64p, _u64p, _u64p]),
+    "st_b200_flux_stats": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.POINTER(FluxStats)]),
 }
 
 
@@ -69,6 +79,13 @@ class B200Api(StApi):
         if rc < 0:
             raise RuntimeError("st_b200_flux_counts failed")
         return out.reshape(ny, nx)
+
+    def flux_stats(self, ctx, idx: int, dni: float) -> dict:
+        """Peak/min/mean flux, sigma, uniformity and uncertainties of flux map `idx`."""
+        s = FluxStats()
+        if self.st_b200_flux_stats(ctx, idx, dni, C.byref(s)) < 0:
+            raise RuntimeError("st_b200_flux_stats failed: " + "; ".join(self.messages(ctx)))
+        return {k: getattr(s, k) for k, _ in FluxStats._fields_}
 
     def element_counts(self, ctx, stage: int, n: int):
         a = np.zeros(n, dtype=np.uint64)
