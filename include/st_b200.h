@@ -99,6 +99,16 @@ int st_b200_flux_stats(st_context_t pcxt, int map, double dni, st_b200_flux_stat
 int st_b200_element_counts(st_context_t pcxt, int stage, unsigned long long *first_hits,
                            unsigned long long *absorbed, unsigned long long *delivered);
 
+/* File front end of the SolTrace CLI (coretrace/strace/main.cpp:78-483) as library calls.
+ * st_b200_load_stinput reads a .stinput system file (sun, optical property pairs, stages
+ * and elements; surface files named in it are read relative to the working directory)
+ * into the context, replacing its optics and stages; 1 on success, -1 with the line and
+ * the reason in st_message() otherwise.  st_b200_write_rays writes the last run's
+ * intersection records in the CLI's .rays text format (sun box, SunRayCount, count, then
+ * one line per record in readback order); 1 on success, -1 otherwise. */
+int st_b200_load_stinput(st_context_t pcxt, const char *path);
+int st_b200_write_rays(st_context_t pcxt, const char *path);
+
 /* First-stage probe without device allocation.  No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc: code running inside a framework that owns

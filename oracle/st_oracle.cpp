@@ -2053,6 +2053,12 @@ int run_trace(Context *cx, unsigned seed) {
     if ((i) >= st->elements.size()) return -1;                      \
     Element *e = st->elements[i];
 
+// message hook of the product's .stinput reader, when the tests compile it into the oracle
+extern "C" void st_input_report(void *p, const char *msg) {
+    Context *cx = reinterpret_cast<Context *>(p);
+    if (cx) cx->log("%s", msg ? msg : "");
+}
+
 extern "C" {
 
 void *st_create_context() { return new Context; }
@@ -2402,6 +2408,24 @@ int st_sun_xyz(void *p, double x, double y, double z) {
     cx->sun.origin[0] = x;
     cx->sun.origin[1] = y;
     cx->sun.origin[2] = z;
+    return 1;
+}
+// solar position from latitude, day of year and solar hour (stapi.cpp:500-527): the
+// declination and hour angle give elevation and azimuth; returns the unit vector toward
+// the sun with x west, y zenith, z north.  Same arithmetic order as the reference.
+int st_sun_position(void *, double lat, double day, double hour, double *x, double *y, double *z) {
+    const double decl = 180 / kPi * asin(0.39795 * cos(0.98563 * kPi / 180 * (day - 173)));
+    const double ha = 15 * (hour - 12);
+    const double el = 180 / kPi * asin(sin(decl * kPi / 180) * sin(lat * kPi / 180) +
+                                       cos(decl * kPi / 180) * cos(ha * kPi / 180) * cos(lat * kPi / 180));
+    double az = 180 / kPi * acos((sin(kPi / 180 * decl) * cos(kPi / 180 * lat) -
+                                  cos(kPi / 180 * decl) * sin(kPi / 180 * lat) * cos(kPi / 180 * ha)) /
+                                     cos(kPi / 180 * el) +
+                                 0.0000000001);
+    if (sin(ha * kPi / 180) > 0.0) az = 360 - az;
+    if (x) *x = -sin(az * kPi / 180) * cos(el * kPi / 180);
+    if (y) *y = sin(el * kPi / 180);
+    if (z) *z = cos(az * kPi / 180) * cos(el * kPi / 180);
     return 1;
 }
 int st_sun_userdata(void *p, st_uint_t n, double angle[], double intensity[]) {

@@ -1,4 +1,4 @@
-"""Build coretrace_api.so (CUDA sm_100a + C++17) in-tree.
+"""Build coretrace_api.so (CUDA sm_100a + C++17) and the strace_b200 CLI in-tree.
 
     python -m soltrace_b200.build          # or: from soltrace_b200.build import build; build()
 
@@ -32,7 +32,9 @@ UNITS = {
     "st_kernels_mixed.cu": [],
     "st_kernels_common.cu": [],
     "st_noalloc.cu": [],
+    "st_stinput.cpp": [],
 }
+CLI = os.path.join(HERE, "strace_b200")  # command-line tracer (csrc/strace_main.cpp)
 HEADERS = ["st_scene.h", "st_device.cuh", "st_trace_impl.cuh", "st_host.h", "st_launch.h"]
 
 
@@ -72,6 +74,13 @@ def build(verbose: bool = False, force: bool = False) -> str:
             f.write(dig)
         objs.append(obj)
     cmd = [nvcc, *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    # the CLI links the library from its own directory
+    cli_src = os.path.join(CSRC, "strace_main.cpp")
+    cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++17", f"-I{INCLUDE}", cli_src, "-o", CLI, LIB,
+           "-Wl,-rpath,$ORIGIN"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)

@@ -1318,6 +1318,11 @@ void report(void *ctx, const std::string &msg) {
 }
 }  // namespace stb
 
+// message hook of the .stinput reader (st_stinput.cpp); not exported
+extern "C" __attribute__((visibility("hidden"))) void st_input_report(void *ctx, const char *msg) {
+    stb::report(ctx, msg ? msg : "");
+}
+
 namespace {
 StageM *stage_of(Context *cx, st_uint_t i) { return i < cx->stages.size() ? &cx->stages[i] : nullptr; }
 Elem *elem_of(Context *cx, st_uint_t s, st_uint_t i) {
