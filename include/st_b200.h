@@ -109,6 +109,32 @@ int st_b200_element_counts(st_context_t pcxt, int stage, unsigned long long *fir
 int st_b200_load_stinput(st_context_t pcxt, const char *path);
 int st_b200_write_rays(st_context_t pcxt, const char *path);
 
+/* Stage-data save and replay: the C form of the reference's st_sim_run_data
+ * (coretrace/stapi.cpp:680-728, raytrace.cpp:544-578 and 1044-1078), for loops that
+ * re-trace only the stages after the first (a receiver design over a fixed heliostat field).
+ *
+ * st_b200_set_save_stage_data(ctx, 1): st_sim_run then keeps (records must be on)
+ *   s0: every first-stage intersection record in ray order, 8 doubles each: position and
+ *       direction (stage frame, as in st_locations/st_cosines), element (negative when
+ *       absorbed), ray number;
+ *   s1: the second stage's input, 7 doubles each: global position, direction, ray number,
+ *       as the reference saves it: its array of the rays that entered the second stage, in
+ *       ray order, whose first positions were overwritten in place by the rays that left it.
+ * st_b200_stage_data_sizes / st_b200_stage_data read them back (caller-allocated arrays of
+ * 8 n0 and 7 n1 doubles).
+ * st_b200_sim_run_replay runs the scene from such data: s0 becomes the first stage's records,
+ * the s1 rays enter the second stage, SunRayCount is the ray number of the last s0 row, and
+ * the stages after the first are traced as by st_sim_run (the replayed rays draw from their
+ * own random streams).  Returns the record count, or -1 with a message. */
+int st_b200_set_save_stage_data(st_context_t pcxt, int on);
+int st_b200_stage_data_sizes(st_context_t pcxt, st_uint_t *n0, st_uint_t *n1);
+int st_b200_stage_data(st_context_t pcxt, double *s0, double *s1);
+int st_b200_sim_run_replay(st_context_t pcxt, unsigned int seed, st_uint_t n0, const double *s0, st_uint_t n1,
+                           const double *s1,
+                           int (*callback)(st_uint_t ntracedtotal, st_uint_t ntraced, st_uint_t ntotrace,
+                                           st_uint_t curstage, st_uint_t nstages, void *data),
+                           void *cbdata);
+
 /* First-stage probe without device allocation.  No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc: code running inside a framework that owns

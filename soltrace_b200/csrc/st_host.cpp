@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <climits>
 #include <numeric>
 #include <string>
 #include <strings.h>
@@ -100,6 +101,11 @@ struct Context {
     int (*cb)(unsigned long, unsigned long, unsigned long, unsigned long, unsigned long, void *) = nullptr;
     void *cbdata = nullptr;
     double last_hit_rate = 0.0;  // batch planning hint carried between runs of a context
+    // stage data (st_b200_set_save_stage_data / st_b200_sim_run_replay, stapi.cpp:680-728)
+    bool save_stage_data = false;
+    std::vector<double> stage_s0, stage_s1;  // saved: 8 doubles per stage-1 record, 7 per ray
+    bool replaying = false;
+    std::vector<double> replay_s0, replay_s1;
     Workspace *ws = nullptr;     // device buffers reused by every run of this context
     ~Context() {
         if (ws) workspace_destroy(ws);
@@ -1140,13 +1146,15 @@ bool flatten(Context *cx, HostScene &hs) {
 
 // reference record order: per stage sorted by (ray number, hit index), then the
 // block merge of TRayData::Merge (types.cpp:311-355)
-void assemble_records(Context *cx, RunResult &rr) {
+void assemble_records(Context *cx, RunResult &rr, bool replay) {
     const int nst = int(cx->stages.size());
     std::vector<RecordDev> &recs = rr.records;
     const uint32_t N = uint32_t(rr.ray_hits);
     // the reference traces no later stage when the only ray carried out of the first
-    // stage is the last numbered one (raytrace.cpp:786-797 never marks it)
-    const bool drop_later = nst > 1 && rr.stage_entries.size() > 1 && rr.stage_entries[1] == 1 && rr.max_enter[1] == N;
+    // stage is the last numbered one (raytrace.cpp:786-797 never marks it); a replay does
+    // not trace the first stage
+    const bool drop_later = !replay && nst > 1 && rr.stage_entries.size() > 1 && rr.stage_entries[1] == 1 &&
+                            rr.max_enter[1] == N;
     std::vector<std::vector<RecordDev>> per(nst);
     for (const RecordDev &r : recs) {
         const int s = r.stage - 1;
@@ -1208,10 +1216,38 @@ void assemble_records(Context *cx, RunResult &rr) {
     recs.shrink_to_fit();
 }
 
+// Saved second-stage input as the reference leaves it (raytrace.cpp:1064-1078): the stage's
+// ray array at the end of stage 2 holds, in ray order, the rays that left stage 2 in its
+// first positions (written back in place as they were produced) and the rays that entered
+// it in the rest.  `in` and `out` are unordered rows of 7 doubles (ray number last).
+std::vector<double> saved_second_stage(std::vector<double> in, std::vector<double> out) {
+    auto by_ray = [](std::vector<double> &rows) {
+        const size_t n = rows.size() / 7;
+        std::vector<size_t> idx(n);
+        std::iota(idx.begin(), idx.end(), size_t(0));
+        std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return rows[7 * a + 6] < rows[7 * b + 6]; });
+        std::vector<double> o(rows.size());
+        for (size_t k = 0; k < n; ++k) std::copy(rows.begin() + 7 * idx[k], rows.begin() + 7 * idx[k] + 7, o.begin() + 7 * k);
+        rows.swap(o);
+    };
+    by_ray(in);
+    by_ray(out);
+    const size_t n = in.size() / 7, w = std::min(out.size() / 7, n);
+    std::vector<double> s1(in);
+    std::copy(out.begin(), out.begin() + 7 * w, s1.begin());
+    return s1;
+}
+
 int run(Context *cx, unsigned seed) {
     cx->records.clear();
     memset(&cx->stats, 0, sizeof cx->stats);
-    if (cx->ex_pos.empty() && cx->raycount < 1) {
+    cx->stage_s0.clear();
+    cx->stage_s1.clear();
+    if (cx->save_stage_data && !cx->want_records) {
+        cx->log("saving stage data needs the intersection records (st_b200_set_records)");
+        return -1;
+    }
+    if (cx->ex_pos.empty() && !cx->replaying && cx->raycount < 1) {
         cx->log("invalid number of rays: %d", cx->raycount);
         return -1;
     }
@@ -1236,6 +1272,32 @@ int run(Context *cx, unsigned seed) {
     rq.callback = cx->cb;
     rq.cbdata = cx->cbdata;
     rq.hit_rate_hint = cx->last_hit_rate;
+    rq.save_stage_data = cx->save_stage_data;
+    if (cx->replaying) {
+        // rays enter stage 2 from the saved rows; each row's first first-stage element from
+        // the saved stage-1 records of its ray number (the first one), for the per-element
+        // delivered counts
+        rq.replay = true;
+        rq.replay_rows = cx->replay_s1;
+        const size_t n0 = cx->replay_s0.size() / 8, n1 = cx->replay_s1.size() / 7;
+        std::vector<std::pair<double, int>> first;  // (ray number, element) of each ray's first record
+        for (size_t k = 0; k < n0; ++k) {
+            const double rn = cx->replay_s0[8 * k + 7];
+            if (first.empty() || first.back().first != rn) first.push_back({rn, int(fabs(cx->replay_s0[8 * k + 6]))});
+        }
+        std::sort(first.begin(), first.end(), [](const std::pair<double, int> &a, const std::pair<double, int> &b) {
+            return a.first < b.first;
+        });
+        rq.replay_fe0.assign(n1, -1);
+        const int f0 = hs.dev.stages[0].first_elem, m0 = hs.dev.stages[0].n_elem;
+        for (size_t k = 0; k < n1; ++k) {
+            const double rn = cx->replay_s1[7 * k + 6];
+            auto it = std::lower_bound(first.begin(), first.end(), std::make_pair(rn, INT_MIN));
+            if (it != first.end() && it->first == rn && it->second >= 1 && it->second <= m0)
+                rq.replay_fe0[k] = f0 + it->second - 1;
+        }
+        rq.replay_sun_rays = n0 ? uint64_t(cx->replay_s0[8 * (n0 - 1) + 7]) : 0;
+    }
     RunResult rr;
     const double host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (!cx->ws) cx->ws = workspace_create();
@@ -1248,7 +1310,29 @@ int run(Context *cx, unsigned seed) {
     if (rr.sun_rays > 0 && cx->ex_pos.empty()) cx->last_hit_rate = double(rr.ray_hits) / double(rr.sun_rays);
     const int nst = int(cx->stages.size());
     const uint32_t N = uint32_t(rr.ray_hits);
-    const bool drop_later = nst > 1 && rr.stage_entries[1] == 1 && rr.max_enter[1] == N;
+    const bool drop_later = !cx->replaying && nst > 1 && rr.stage_entries[1] == 1 && rr.max_enter[1] == N;
+    if (cx->replaying) {
+        // the saved stage-1 records are the replay's stage-1 records (raytrace.cpp:554-565)
+        const size_t n0 = cx->replay_s0.size() / 8;
+        double last = -1;
+        uint32_t seq = 0;
+        for (size_t k = 0; k < n0; ++k) {
+            const double *row = cx->replay_s0.data() + 8 * k;
+            RecordDev r;
+            memset(&r, 0, sizeof r);
+            for (int q = 0; q < 3; ++q) {
+                r.pos[q] = row[q];
+                r.cos[q] = row[3 + q];
+            }
+            r.element = int(row[6]);
+            r.stage = 1;
+            r.raynum = uint32_t(row[7]);
+            seq = (row[7] == last) ? seq + 1 : 0;
+            last = row[7];
+            r.seq = seq;
+            rr.records.push_back(r);
+        }
+    }
     // flux maps and per-element counts
     for (size_t m = 0; m < cx->flux.size(); ++m) {
         cx->flux[m].counts = rr.flux[m];
@@ -1288,7 +1372,18 @@ int run(Context *cx, unsigned seed) {
     S.trace_variant = rr.trace_variant;
     if (rr.flags & 1u) cx->log("warning: a ray reached the limit of intersections per stage; it was stopped there");
     const auto ta = std::chrono::steady_clock::now();
-    if (cx->want_records) assemble_records(cx, rr);
+    if (cx->want_records) assemble_records(cx, rr, cx->replaying);
+    if (cx->save_stage_data) {
+        // stage-1 records in ray order (the records of stage 1 keep that order in the merged
+        // readback) and the second stage's input as the reference saves it
+        for (const RecordDev &r : cx->records)
+            if (r.stage == 1) {
+                const double row[8] = {r.pos[0], r.pos[1], r.pos[2], r.cos[0], r.cos[1], r.cos[2], double(r.element),
+                                       double(r.raynum)};
+                cx->stage_s0.insert(cx->stage_s0.end(), row, row + 8);
+            }
+        if (nst >= 2) cx->stage_s1 = saved_second_stage(rr.saved[0], rr.saved[1]);
+    }
     S.readback_ms = rr.readback_ms + std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
     S.records = cx->records.size();
     S.intersections = cx->want_records ? uint64_t(cx->records.size()) : rr.intersections;
@@ -1888,6 +1983,60 @@ int st_b200_flux_stats(st_context_t p, int map, double dni, st_b200_flux_stats_t
     r.rays_in_min_bin = nmin;
     *out = r;
     return 1;
+}
+int st_b200_set_save_stage_data(st_context_t p, int on) {
+    CTX(p, -1);
+    cx->save_stage_data = on != 0;
+    return 1;
+}
+int st_b200_stage_data_sizes(st_context_t p, st_uint_t *n0, st_uint_t *n1) {
+    CTX(p, -1);
+    if (n0) *n0 = st_uint_t(cx->stage_s0.size() / 8);
+    if (n1) *n1 = st_uint_t(cx->stage_s1.size() / 7);
+    return 1;
+}
+int st_b200_stage_data(st_context_t p, double *s0, double *s1) {
+    CTX(p, -1);
+    if (s0) std::copy(cx->stage_s0.begin(), cx->stage_s0.end(), s0);
+    if (s1) std::copy(cx->stage_s1.begin(), cx->stage_s1.end(), s1);
+    return 1;
+}
+int st_b200_sim_run_replay(st_context_t p, unsigned int seed, st_uint_t n0, const double *s0, st_uint_t n1,
+                           const double *s1, int (*cb)(st_uint_t, st_uint_t, st_uint_t, st_uint_t, st_uint_t, void *),
+                           void *data) {
+    CTX(p, -1);
+    if ((n0 && !s0) || (n1 && !s1)) return -1;
+    if (n0 == 0 || n1 == 0) {
+        // the reference loads saved data only when both parts are non-empty; otherwise it
+        // traces from the sun, for as many rays as s1 has rows when it has any
+        // (stapi.cpp:700-703, raytrace.cpp:159-163)
+        const int keep = cx->raycount;
+        if (n1) cx->raycount = int(n1);
+        cx->cb = cb;
+        cx->cbdata = data;
+        const int rc = run(cx, seed);
+        cx->raycount = keep;
+        return rc;
+    }
+    if (cx->stages.size() < 2) {
+        cx->log("a replay needs at least two stages");
+        return -1;
+    }
+    cx->replay_s0.assign(s0, s0 + 8 * n0);
+    cx->replay_s1.assign(s1, s1 + 7 * n1);
+    for (st_uint_t k = 0; k < n1; ++k)
+        if (!(s1[7 * k + 6] >= 1 && s1[7 * k + 6] < 4294967296.0)) {
+            cx->log("replay ray %lu has an invalid ray number", (unsigned long)k);
+            return -1;
+        }
+    cx->cb = cb;
+    cx->cbdata = data;
+    cx->replaying = true;
+    const int rc = run(cx, seed);
+    cx->replaying = false;
+    cx->replay_s0.clear();
+    cx->replay_s1.clear();
+    return rc;
 }
 int st_b200_run_stats(st_context_t p, st_b200_stats *out) {
     CTX(p, -1);

@@ -46,6 +46,11 @@ struct RunRequest {
     int (*callback)(unsigned long, unsigned long, unsigned long, unsigned long, unsigned long, void *) = nullptr;
     void *cbdata = nullptr;
     double hit_rate_hint = 0.0;  // expected first-stage hits per sun ray (0 = measure with a pilot batch)
+    bool save_stage_data = false;       // keep the rays leaving stages 1 and 2 (RunResult::saved)
+    bool replay = false;                // rays enter stage 2 from replay_rows instead of the sun
+    std::vector<double> replay_rows;    // 7 doubles per ray: global position, direction, ray number
+    std::vector<int> replay_fe0;        // per ray: global index of its first first-stage element, -1
+    uint64_t replay_sun_rays = 0;       // SunRayCount of a replay (the last saved stage-1 ray number)
 };
 
 struct RunResult {
@@ -63,6 +68,7 @@ struct RunResult {
     int batches = 0, gpu_launches = 0;
     unsigned flags = 0;
     uint64_t intersections = 0;  // records of the run by the reference's rules, kept or not
+    std::vector<double> saved[2];  // rays leaving stage 1 and stage 2 (7 doubles per ray), unordered
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
     int probe_variant = 0, trace_variant = 0;
 };

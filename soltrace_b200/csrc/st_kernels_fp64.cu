@@ -40,8 +40,8 @@ int launch_probe_fp64(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_
 
 int launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
                       const uint32_t *hit_idx, const uint32_t *total, const RunState *rs, const TraceOut &O,
-                      const WfState &W, const WfQueues &Q, cudaStream_t st) {
-    return records ? wf_launch<0, 1>(S, hit_sid, hit_el, hit_idx, total, rs, O, W, Q, st)
-                   : wf_launch<0, 0>(S, hit_sid, hit_el, hit_idx, total, rs, O, W, Q, st);
+                      const WfState &W, const WfQueues &Q, const ReplayIn *replay, cudaStream_t st) {
+    return records ? wf_launch<0, 1>(S, hit_sid, hit_el, hit_idx, total, rs, O, W, Q, replay, st)
+                   : wf_launch<0, 0>(S, hit_sid, hit_el, hit_idx, total, rs, O, W, Q, replay, st);
 }
 }  // namespace stb

@@ -73,6 +73,20 @@ struct TraceOut {
     unsigned long long *first_hits;  // per global element index
     unsigned long long *absorbed;
     unsigned long long *delivered;   // per global element index (first-stage elements)
+    // stage-data saving (st_b200_set_save_stage_data): rays leaving stage 1 and stage 2
+    // (global position, direction, ray number: 7 doubles per row), null when off
+    double *save_rows[2];
+    unsigned long long *save_count[2];
+    unsigned long long save_cap;
+};
+
+// Rays entering the second stage from saved stage data (replay, st_b200_sim_run_replay):
+// 7 doubles per row (global position, direction, ray number) and the global index of each
+// ray's first first-stage element (-1 unknown).
+struct ReplayIn {
+    const double *rows;
+    const int *fe0;
+    uint32_t n;
 };
 
 
@@ -89,12 +103,14 @@ void launch_sun_candidates(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t 
 // Trace of a batch's numbered rays (hit-list entries below the cut-off at the requested
 // hit count): the first kernel, `Q.rounds` rounds of search and shade kernels, and the
 // finishing kernel.  Returns the number of kernels launched.
+// With `replay` (non-null) the rays enter the second stage from saved rows instead of the
+// hit list (the hit-list arguments are then unused).
 int launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
                       const uint32_t *hit_idx, const uint32_t *total, const RunState *rs, const TraceOut &O,
-                      const WfState &W, const WfQueues &Q, cudaStream_t st);
+                      const WfState &W, const WfQueues &Q, const ReplayIn *replay, cudaStream_t st);
 int launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
                        const uint32_t *hit_idx, const uint32_t *total, const RunState *rs, const TraceOut &O,
-                       const WfState &W, const WfQueues &Q, cudaStream_t st);
+                       const WfState &W, const WfQueues &Q, const ReplayIn *replay, cudaStream_t st);
 // counting sort of the batch's hits by first-stage element (n_elem0 buckets)
 void launch_sort_by_element(const uint32_t *total, const uint64_t *hit_sid, const uint32_t *hit_el, uint32_t n_elem0,
                             uint32_t *elem_count, uint32_t *elem_cursor, uint32_t *scratch_total, uint64_t *s_sid,

@@ -63,6 +63,7 @@ struct Workspace {
     DevBuf cand;  // grid probe's candidate list: count, then one sun-ray index per entry
     // trace state and queues (one slot per hit-list entry of a batch)
     DevBuf wf_sid, wf_raynum, wf_draw, wf_meta, wf_fe0, wf_p, wf_c, wf_q0, wf_q1, wf_qs, wf_counts;
+    DevBuf save_rows[2], save_count, replay_rows, replay_fe0;  // stage-data save / replay
     DevBuf ecount, ecursor, etotal, s_sid, s_el, s_idx;
     std::vector<cudaEvent_t> events;
     // autotuned kernel variants per precision (FP64, mixed), chosen on the first run
@@ -142,6 +143,32 @@ static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, ui
     }
     for (auto &x : ev) cudaEventDestroy(x);
     return e;
+}
+
+// trace state and queues for up to `cap` rays
+static cudaError_t wf_buffers(Workspace &ws, uint64_t cap, int nst, WfState &W, WfQueues &Q) {
+    cudaError_t e;
+    cap = std::max<uint64_t>(cap, 1);
+    if ((e = ws.wf_sid.ensure(cap * 8)) || (e = ws.wf_raynum.ensure(cap * 4)) || (e = ws.wf_draw.ensure(cap * 4)) ||
+        (e = ws.wf_meta.ensure(cap * 16)) || (e = ws.wf_fe0.ensure(cap * 4)) || (e = ws.wf_p.ensure(cap * 24)) ||
+        (e = ws.wf_c.ensure(cap * 24)) || (e = ws.wf_q0.ensure(cap * 4)) || (e = ws.wf_q1.ensure(cap * 4)) ||
+        (e = ws.wf_qs.ensure(cap * 4)))
+        return e;
+    Q.rounds = 2 * nst;
+    if ((e = ws.wf_counts.ensure(sizeof(uint32_t) * (2 * Q.rounds + 1)))) return e;
+    Q.search[0] = ws.wf_q0.as<uint32_t>();
+    Q.search[1] = ws.wf_q1.as<uint32_t>();
+    Q.shade = ws.wf_qs.as<uint32_t>();
+    Q.counts = ws.wf_counts.as<uint32_t>();
+    W.sid = ws.wf_sid.as<uint64_t>();
+    W.raynum = ws.wf_raynum.as<uint32_t>();
+    W.draw = ws.wf_draw.as<uint32_t>();
+    W.meta = ws.wf_meta.as<int4>();
+    W.fe0 = ws.wf_fe0.as<int>();
+    W.p = ws.wf_p.as<double>();
+    W.c = ws.wf_c.as<double>();
+    W.cap = uint32_t(cap);
+    return cudaSuccess;
 }
 
 #define CK(x)                                                                                 \
@@ -246,9 +273,9 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
         CK(d_ecursor.ensure(size_t(n_elem0) * 4));
         CK(d_etotal.ensure(8));
     }
-    unsigned long long rec_cap = 0;
+    unsigned long long rec_cap = 0, save_cap = 0;
     Workspace::Tuning &tu = ws.tune[rq.precision ? 1 : 0];
-    if (!tu.done && !explicit_mode) CK(autotune(ws, S, rq.precision, rq.max_sun, st, d_hit_elem, d_counts, out.gpu_launches));
+    if (!tu.done && !explicit_mode && !rq.replay) CK(autotune(ws, S, rq.precision, rq.max_sun, st, d_hit_elem, d_counts, out.gpu_launches));
     out.probe_variant = tu.probe;
     out.trace_variant = 0;
     (void)dev_sms;
@@ -301,7 +328,51 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
 
         // Batches are queued without host round trips unless records are kept (each
         // batch's records are copied out) or a progress callback is installed.
-        const bool sync_each = rq.records || rq.callback != nullptr;
+        const bool sync_each = rq.records || rq.callback != nullptr || rq.save_stage_data;
+        out.saved[0].clear();
+        out.saved[1].clear();
+        // stage-data saving: room for every numbered ray of a batch in each of the two lists
+        O.save_rows[0] = O.save_rows[1] = nullptr;
+        O.save_count[0] = O.save_count[1] = nullptr;
+        O.save_cap = 0;
+        auto save_setup = [&](uint64_t rays) -> cudaError_t {
+            if (!rq.save_stage_data) return cudaSuccess;
+            cudaError_t e;
+            const uint64_t cap =
+                std::max<uint64_t>(save_cap, std::min<uint64_t>(rays, explicit_mode || rq.replay ? rays : rq.n_hits) + 16);
+            for (int k = 0; k < 2; ++k)
+                if ((e = ws.save_rows[k].ensure(cap * 7 * sizeof(double)))) return e;
+            if ((e = ws.save_count.ensure(16)) || (e = cudaMemsetAsync(ws.save_count.p, 0, 16, st))) return e;
+            for (int k = 0; k < 2; ++k) {
+                O.save_rows[k] = ws.save_rows[k].as<double>();
+                O.save_count[k] = ws.save_count.as<unsigned long long>() + k;
+            }
+            O.save_cap = cap;
+            return cudaSuccess;
+        };
+        // after a synchronised batch: append its saved rays (overflow: re-run with more room)
+        auto save_collect = [&](bool &overflow) -> cudaError_t {
+            overflow = false;
+            if (!rq.save_stage_data) return cudaSuccess;
+            unsigned long long cnt[2] = {0, 0};
+            cudaError_t e = cudaMemcpy(cnt, ws.save_count.p, 16, cudaMemcpyDeviceToHost);
+            if (e) return e;
+            for (int k = 0; k < 2; ++k)
+                if (cnt[k] > O.save_cap) {
+                    save_cap = cnt[k] + cnt[k] / 4 + 1024;
+                    overflow = true;
+                    return cudaSuccess;
+                }
+            for (int k = 0; k < 2; ++k) {
+                const size_t old = out.saved[k].size();
+                out.saved[k].resize(old + size_t(cnt[k]) * 7);
+                if (cnt[k] && (e = cudaMemcpy(out.saved[k].data() + old, O.save_rows[k],
+                                              size_t(cnt[k]) * 7 * sizeof(double), cudaMemcpyDeviceToHost)))
+                    return e;
+                out.d2h_bytes += 8 + cnt[k] * 7 * sizeof(double);
+            }
+            return cudaSuccess;
+        };
         uint64_t sun_next = 0;
         double p_est = rq.hit_rate_hint > 0 ? rq.hit_rate_hint : 0.0;
         RunState rs = rs0;
@@ -318,6 +389,57 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
         cudaEvent_t t_first = new_event(), t_last = new_event();
         CK(cudaEventRecord(t_first, st));
         bool done = false;
+        if (rq.replay) {
+            // saved stage data: the rays enter the second stage directly (no sun rays, no probe)
+            const uint64_t n1 = rq.replay_rows.size() / 7;
+            CK(upload(ws.replay_rows, rq.replay_rows, st, out.h2d_bytes));
+            CK(upload(ws.replay_fe0, rq.replay_fe0, st, out.h2d_bytes));
+            if (rq.records) {
+                if (rec_cap == 0) rec_cap = std::max<uint64_t>(n1, 1) * uint64_t(nst) * 2 + 4096;
+                CK(d_recs.ensure(rec_cap * sizeof(RecordDev)));
+                CK(cudaMemsetAsync(d_rec_count.p, 0, 8, st));
+            }
+            O.recs = rq.records ? d_recs.as<RecordDev>() : nullptr;
+            O.rec_cap = rq.records ? rec_cap : 0;
+            WfState W;
+            WfQueues Q;
+            CK(wf_buffers(ws, n1, nst, W, Q));
+            CK(save_setup(n1));
+            ReplayIn rin;
+            rin.rows = ws.replay_rows.as<double>();
+            rin.fe0 = rq.replay_fe0.empty() ? nullptr : ws.replay_fe0.as<int>();
+            rin.n = uint32_t(n1);
+            cudaEvent_t p1 = new_event(), p2 = new_event();
+            CK(cudaEventRecord(p1, st));
+            if (rq.precision)
+                out.gpu_launches +=
+                    launch_trace_mixed(rq.records, S, nullptr, nullptr, nullptr, nullptr, drs, O, W, Q, &rin, st);
+            else
+                out.gpu_launches +=
+                    launch_trace_fp64(rq.records, S, nullptr, nullptr, nullptr, nullptr, drs, O, W, Q, &rin, st);
+            CK(cudaEventRecord(p2, st));
+            CK(cudaGetLastError());
+            trace_ev.push_back({p1, p2});
+            out.batches = 1;
+            unsigned long long nrec = 0;
+            if (rq.records) CK(cudaMemcpyAsync(&nrec, d_rec_count.p, 8, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            if (rq.records && nrec > rec_cap) {
+                rec_cap = nrec + nrec / 4 + 4096;
+                continue;
+            }
+            bool save_over = false;
+            CK(save_collect(save_over));
+            if (save_over) continue;
+            if (nrec) {
+                out.records.resize(nrec);
+                out.d2h_bytes += nrec * sizeof(RecordDev);
+                CK(cudaMemcpy(out.records.data(), d_recs.p, nrec * sizeof(RecordDev), cudaMemcpyDeviceToHost));
+            }
+            rs.hits_done = rs.sun_rays = rq.replay_sun_rays;
+            rs.reached = 1;
+            done = true;
+        }
         while (!done) {
             // plan the next group of batches
             uint64_t want;
@@ -387,39 +509,17 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                     t_idx = d_s_idx.as<uint32_t>();
                 }
                 // trace state and queues: one slot per hit-list entry (at most n)
-                CK(ws.wf_sid.ensure(n * 8));
-                CK(ws.wf_raynum.ensure(n * 4));
-                CK(ws.wf_draw.ensure(n * 4));
-                CK(ws.wf_meta.ensure(n * 16));
-                CK(ws.wf_fe0.ensure(n * 4));
-                CK(ws.wf_p.ensure(n * 24));
-                CK(ws.wf_c.ensure(n * 24));
-                CK(ws.wf_q0.ensure(n * 4));
-                CK(ws.wf_q1.ensure(n * 4));
-                CK(ws.wf_qs.ensure(n * 4));
-                WfQueues Q;
-                Q.rounds = 2 * nst;
-                CK(ws.wf_counts.ensure(sizeof(uint32_t) * (2 * Q.rounds + 1)));
-                Q.search[0] = ws.wf_q0.as<uint32_t>();
-                Q.search[1] = ws.wf_q1.as<uint32_t>();
-                Q.shade = ws.wf_qs.as<uint32_t>();
-                Q.counts = ws.wf_counts.as<uint32_t>();
                 WfState W;
-                W.sid = ws.wf_sid.as<uint64_t>();
-                W.raynum = ws.wf_raynum.as<uint32_t>();
-                W.draw = ws.wf_draw.as<uint32_t>();
-                W.meta = ws.wf_meta.as<int4>();
-                W.fe0 = ws.wf_fe0.as<int>();
-                W.p = ws.wf_p.as<double>();
-                W.c = ws.wf_c.as<double>();
-                W.cap = uint32_t(n);
+                WfQueues Q;
+                CK(wf_buffers(ws, n, nst, W, Q));
+                CK(save_setup(n));
                 CK(cudaEventRecord(p1, st));
                 if (rq.precision)
                     out.gpu_launches += launch_trace_mixed(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(),
-                                                           drs, O, W, Q, st);
+                                                           drs, O, W, Q, nullptr, st);
                 else
                     out.gpu_launches += launch_trace_fp64(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(),
-                                                          drs, O, W, Q, st);
+                                                          drs, O, W, Q, nullptr, st);
                 CK(cudaEventRecord(p2, st));
                 launch_advance(d_total.as<uint32_t>(), d_hit_sid.as<uint64_t>(), sun_next, uint32_t(n), drs, st);
                 CK(cudaGetLastError());
@@ -437,6 +537,12 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                     CK(cudaStreamSynchronize(st));
                     if (rq.records && nrec > rec_cap) {
                         rec_cap = nrec + nrec / 4 + 4096;  // re-run the whole job with room for it
+                        restart = true;
+                        break;
+                    }
+                    bool save_over = false;
+                    CK(save_collect(save_over));
+                    if (save_over) {
                         restart = true;
                         break;
                     }

@@ -893,6 +893,20 @@ __device__ __forceinline__ void wf_stage_enter(WfBlockCtr &c, int si, uint32_t r
 // ends the ray unless the stage is trace-through (raytrace.cpp:800-826; the one miss the
 // reference does not record is removed on the host from max_ttmiss); otherwise the ray
 // goes on, in global coordinates, to the next stage
+// a ray leaving stage 1 or 2 (0-based si 0 or 1) toward the next stage, kept when stage
+// data are saved (global position, direction, ray number)
+__device__ __forceinline__ void wf_save_ray(const TraceOut &O, const WfRay &r) {
+    if (r.si > 1 || !O.save_rows[r.si]) return;
+    const unsigned long long slot = atomicAdd(O.save_count[r.si], 1ull);
+    if (slot >= O.save_cap) return;
+    double *row = O.save_rows[r.si] + 7 * slot;
+    for (int q = 0; q < 3; ++q) {
+        row[q] = r.p[q];
+        row[3 + q] = r.c[q];
+    }
+    row[6] = double(r.raynum);
+}
+
 template <int RECORDS>
 __device__ __forceinline__ int wf_exit_stage(const SceneDev &S, const TraceOut &O, WfBlockCtr &c, WfRay &r,
                                              const double ps[3], const double cs[3]) {
@@ -919,6 +933,7 @@ __device__ __forceinline__ int wf_exit_stage(const SceneDev &S, const TraceOut &
         to_ref(st.R, st.o, ps, cs, r.p, r.c);
         r.moved = true;
     }
+    wf_save_ray(O, r);
     if (r.si + 1 >= S.n_stages) return kWfDone;
     r.si += 1;
     r.hits = 0;
@@ -1116,6 +1131,44 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_first(
     wf_ctr_flush(c, S, O);
 }
 
+// Replay entry: rays of saved stage data enter the second stage (raytrace.cpp:544-578
+// loads them in place of tracing the first stage).  Row i draws from its own stream
+// (key: bit 62 set, row index), as the replayed rays' first-stage draws are not known.
+template <int MIXED, int RECORDS>
+__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_replay(
+    const __grid_constant__ SceneDev S, TraceOut O, WfState W, ReplayIn in, uint32_t *q_search, uint32_t *n_search) {
+    __shared__ WfBlockCtr c;
+    __shared__ WfPushSh psh;
+    wf_ctr_init(c);
+    const uint32_t n = in.n;
+    const uint32_t stride = gridDim.x * kTraceBlock;
+    const uint32_t n_round = (n + kTraceBlock - 1) / kTraceBlock * kTraceBlock;
+    for (uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x; i < n_round; i += stride) {
+        const bool live = i < n && S.n_stages > 1;
+        if (live) {
+            WfRay r;
+            const double *row = in.rows + 7 * size_t(i);
+            for (int q = 0; q < 3; ++q) {
+                r.p[q] = row[q];
+                r.c[q] = row[3 + q];
+            }
+            r.raynum = uint32_t(row[6]);
+            r.sid = (1ull << 62) | i;
+            r.draw = 0;
+            r.si = 1;
+            r.hits = 0;
+            r.last_j = -1;
+            r.next_j = -1;
+            r.fe0 = in.fe0 ? in.fe0[i] : -1;
+            r.moved = true;
+            wf_stage_enter(c, 1, r.raynum);
+            wf_store(W, i, r, true);
+        }
+        wf_block_push(psh, q_search, n_search, live, q_search, n_search, false, i);
+    }
+    wf_ctr_flush(c, S, O);
+}
+
 // Search kernel: rays queued for a search; those that find an element go to the shade
 // queue, those that move on to another stage back to the search queue of the next round.
 template <int MIXED, int RECORDS>
@@ -1188,7 +1241,7 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_finish(co
 template <int MIXED, int RECORDS>
 static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx,
                      const uint32_t *total, const RunState *rs, const TraceOut &O, const WfState &W,
-                     const WfQueues &Q, cudaStream_t st) {
+                     const WfQueues &Q, const ReplayIn *replay, cudaStream_t st) {
     // persistent grids: every block the kernels can keep resident on every SM
     static int per_sm[4] = {0, 0, 0, 0};
     if (per_sm[0] == 0) {
@@ -1203,8 +1256,11 @@ static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t 
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int R = Q.rounds;
     cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * (2 * R + 1), st);
-    k_wf_first<MIXED, RECORDS><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs, O, W,
-                                                                          Q.search[0], Q.counts);
+    if (replay)
+        k_wf_replay<MIXED, RECORDS><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, O, W, *replay, Q.search[0], Q.counts);
+    else
+        k_wf_first<MIXED, RECORDS><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs, O,
+                                                                              W, Q.search[0], Q.counts);
     for (int r = 0; r < R; ++r) {
         uint32_t *c = Q.counts + 2 * r;
         k_wf_search<MIXED, RECORDS><<<sms * per_sm[1], kTraceBlock, 0, st>>>(

@@ -62,6 +62,13 @@ EXTENSIONS = {
     "st_b200_run_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
     "st_b200_element_counts": (C.c_int, [C.c_void_p, C.c_int, _u64p, _u64p, _u64p]),
     "st_b200_flux_stats": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.POINTER(FluxStats)]),
+    "st_b200_set_save_stage_data": (C.c_int, [C.c_void_p, C.c_int]),
+    "st_b200_stage_data_sizes": (C.c_int, [C.c_void_p, C.POINTER(st_uint_t), C.POINTER(st_uint_t)]),
+    "st_b200_stage_data": (C.c_int, [C.c_void_p, c_double_p, c_double_p]),
+    "st_b200_sim_run_replay": (C.c_int, [C.c_void_p, C.c_uint, st_uint_t, c_double_p, st_uint_t, c_double_p,
+                                         C.c_void_p, C.c_void_p]),
+    "st_b200_load_stinput": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "st_b200_write_rays": (C.c_int, [C.c_void_p, C.c_char_p]),
 }
 
 
@@ -86,6 +93,22 @@ class B200Api(StApi):
         if self.st_b200_flux_stats(ctx, idx, dni, C.byref(s)) < 0:
             raise RuntimeError("st_b200_flux_stats failed: " + "; ".join(self.messages(ctx)))
         return {k: getattr(s, k) for k, _ in FluxStats._fields_}
+
+    def stage_data(self, ctx):
+        """(s0, s1) of the last run with stage-data saving on: arrays (n0, 8) and (n1, 7)."""
+        n0, n1 = st_uint_t(), st_uint_t()
+        self.st_b200_stage_data_sizes(ctx, C.byref(n0), C.byref(n1))
+        s0 = np.zeros((n0.value, 8))
+        s1 = np.zeros((n1.value, 7))
+        self.st_b200_stage_data(ctx, s0.ctypes.data_as(c_double_p), s1.ctypes.data_as(c_double_p))
+        return s0, s1
+
+    def run_replay(self, ctx, seed: int, s0: np.ndarray, s1: np.ndarray) -> int:
+        """Trace the stages after the first from saved stage data (st_b200_sim_run_replay)."""
+        s0 = np.ascontiguousarray(s0, dtype=np.float64).reshape(-1, 8)
+        s1 = np.ascontiguousarray(s1, dtype=np.float64).reshape(-1, 7)
+        return self.st_b200_sim_run_replay(ctx, seed, len(s0), s0.ctypes.data_as(c_double_p), len(s1),
+                                           s1.ctypes.data_as(c_double_p), None, None)
 
     def element_counts(self, ctx, stage: int, n: int):
         a = np.zeros(n, dtype=np.uint64)
