@@ -74,6 +74,13 @@ struct Element {
     std::vector<double> poly;
     std::vector<double> spl_x, spl_y, spl_y2;
     std::vector<double> vshot;  // rows of 5
+    // finite-element surface (.fed): nodes (x, y, z) and the zone grid the reference's
+    // st_hash_tree builds over them (treemesh.cpp:353-535): 2^fe_nx x 2^fe_ny zones over
+    // the nodes' bounding box; per zone, the nodes of the 3 x 3 zones around it
+    std::vector<double> fe_nodes;
+    int fe_nx = 0, fe_ny = 0;
+    double fe_lim[4] = {0, 0, 0, 0};
+    std::vector<int> fe_start, fe_items;
     int vshot_rows = 0;
     int interaction = 0;
     std::string optic_name;
@@ -313,6 +320,221 @@ void vshot_slopes(const Element *e, double x, double y, double density, double *
 }
 
 // ------------------------------------------------------------------------------------
+// Finite-element surface (vshot.cpp:166-242, interpolate.cpp:5-238, treemesh.cpp)
+// ------------------------------------------------------------------------------------
+// zone index of (x, y): repeated halving of the bounding box, upper half when strictly
+// above the midpoint (st_hash_tree::pos_to_binary, treemesh.cpp:757-800)
+static int fe_zone(const Element *e, double x, double y) {
+    double x0 = e->fe_lim[0], x1 = e->fe_lim[1], y0 = e->fe_lim[2], y1 = e->fe_lim[3];
+    int ix = 0, iy = 0;
+    for (int k = 0; k < e->fe_nx; ++k) {
+        const double c = (x0 + x1) * 0.5;
+        if (x > c) {
+            x0 = c;
+            ix = 2 * ix + 1;
+        } else {
+            x1 = c;
+            ix = 2 * ix;
+        }
+    }
+    for (int k = 0; k < e->fe_ny; ++k) {
+        const double c = (y0 + y1) * 0.5;
+        if (y > c) {
+            y0 = c;
+            iy = 2 * iy + 1;
+        } else {
+            y1 = c;
+            iy = 2 * iy;
+        }
+    }
+    return iy * (1 << e->fe_nx) + ix;
+}
+
+// Build the zone grid of the nodes (input.cpp:510-557 -> st_hash_tree): zone size from
+// 1.5 sqrt(area per node), levels floor(log2(extent / size)) >= 1 per axis.  A zone's
+// candidate list: its own nodes, then those of its 8 neighbours (x offset outer loop, y
+// inner, treemesh.cpp:448-485); zones with no node in their 3 x 3 block have none.
+static void fe_build(Element *e) {
+    const size_t n = e->fe_nodes.size() / 3;
+    double xmin = 1.79769313486231570e308, ymin = xmin, xmax = -xmin, ymax = -xmin;
+    for (size_t i = 0; i < n; ++i) {
+        const double x = e->fe_nodes[3 * i], y = e->fe_nodes[3 * i + 1];
+        xmax = x > xmax ? x : xmax;
+        ymax = y > ymax ? y : ymax;
+        xmin = x < xmin ? x : xmin;
+        ymin = y < ymin ? y : ymin;
+    }
+    e->fe_lim[0] = xmin;
+    e->fe_lim[1] = xmax;
+    e->fe_lim[2] = ymin;
+    e->fe_lim[3] = ymax;
+    const double rap = 1.5 * sqrt(((xmax - xmin) * (ymax - ymin)) / (double)n);
+    const double l2i = 1. / log(2.);
+    e->fe_nx = (int)floor(log((xmax - xmin) / rap) * l2i);
+    e->fe_nx = e->fe_nx < 1 ? 1 : e->fe_nx;
+    e->fe_ny = (int)floor(log((ymax - ymin) / rap) * l2i);
+    e->fe_ny = e->fe_ny < 1 ? 1 : e->fe_ny;
+    const int nx = 1 << e->fe_nx, ny = 1 << e->fe_ny;
+    std::vector<std::vector<int>> zone(size_t(nx) * ny);
+    for (size_t i = 0; i < n; ++i) zone[fe_zone(e, e->fe_nodes[3 * i], e->fe_nodes[3 * i + 1])].push_back(int(i));
+    e->fe_start.assign(size_t(nx) * ny + 1, 0);
+    e->fe_items.clear();
+    for (int iy = 0; iy < ny; ++iy)
+        for (int ix = 0; ix < nx; ++ix) {
+            const int z = iy * nx + ix;
+            e->fe_start[z] = int(e->fe_items.size());
+            e->fe_items.insert(e->fe_items.end(), zone[z].begin(), zone[z].end());
+            for (int i = -1; i < 2; ++i)
+                for (int j = -1; j < 2; ++j) {
+                    if (i == 0 && j == 0) continue;
+                    const int jx = ix + i, jy = iy + j;
+                    if (jx < 0 || jx >= nx || jy < 0 || jy >= ny) continue;
+                    const auto &l = zone[size_t(jy) * nx + jx];
+                    e->fe_items.insert(e->fe_items.end(), l.begin(), l.end());
+                }
+        }
+    e->fe_start[size_t(nx) * ny] = int(e->fe_items.size());  // zone z: [fe_start[z], fe_start[z + 1])
+}
+
+// Kriging with a power-law variogram (Numerical Recipes 3rd ed. section 3.7.4, the Krig
+// and Powvargram structures, with an LU decomposition with implicit partial pivoting, section
+// 2.3), in the reference's arithmetic order (interpolate.cpp:5-238).
+struct FeKrig {
+    int n = 0;
+    double x[7][2], alph = 0, bet = 1.999;
+    double lu[8][8];
+    int indx[8];
+    double yvi[8];
+    double pvg(double r) const { return 0.0 + alph * pow(r, bet); }
+    static double sq(double a) { return a * a; }
+    double rdist(const double *a, const double *b) const {
+        double d = 0.;
+        for (int k = 0; k < 2; ++k) d += sq(a[k] - b[k]);
+        return sqrt(d);
+    }
+    void setup(const double (*px)[2], const double *py, int npt) {
+        n = npt;
+        for (int i = 0; i < n; ++i) {
+            x[i][0] = px[i][0];
+            x[i][1] = px[i][1];
+        }
+        double num = 0., denom = 0.;
+        for (int i = 0; i < n; i++)
+            for (int j = i + 1; j < n; j++) {
+                double rb = 0.;
+                for (int k = 0; k < 2; k++) rb += sq(x[i][k] - x[j][k]);
+                rb = pow(rb, 0.5 * bet);
+                num += rb * (0.5 * sq(py[i] - py[j]) - 0.0);
+                denom += sq(rb);
+            }
+        alph = num / denom;
+        const int m = n + 1;
+        for (int i = 0; i < n; i++) {
+            for (int j = i; j < n; j++) lu[i][j] = lu[j][i] = pvg(rdist(x[i], x[j]));
+            lu[i][n] = lu[n][i] = 1.;
+        }
+        lu[n][n] = 0.;
+        double y[8];
+        for (int i = 0; i < n; ++i) y[i] = py[i];
+        y[n] = 0.;
+        // decomposition
+        double vv[8];
+        for (int i = 0; i < m; i++) {
+            double big = 0.0, t;
+            for (int j = 0; j < m; j++)
+                if ((t = fabs(lu[i][j])) > big) big = t;
+            vv[i] = 1.0 / big;
+        }
+        for (int k = 0; k < m; k++) {
+            double big = 0.0, t;
+            int imax = k;
+            for (int i = k; i < m; i++) {
+                t = vv[i] * fabs(lu[i][k]);
+                if (t > big) {
+                    big = t;
+                    imax = i;
+                }
+            }
+            if (k != imax) {
+                for (int j = 0; j < m; j++) {
+                    t = lu[imax][j];
+                    lu[imax][j] = lu[k][j];
+                    lu[k][j] = t;
+                }
+                vv[imax] = vv[k];
+            }
+            indx[k] = imax;
+            if (lu[k][k] == 0.0) lu[k][k] = 1.0e-40;
+            for (int i = k + 1; i < m; i++) {
+                t = lu[i][k] /= lu[k][k];
+                for (int j = k + 1; j < m; j++) lu[i][j] -= t * lu[k][j];
+            }
+        }
+        // solve for the weights
+        int ii = 0;
+        for (int i = 0; i < m; i++) yvi[i] = y[i];
+        for (int i = 0; i < m; i++) {
+            const int ip = indx[i];
+            double sum = yvi[ip];
+            yvi[ip] = yvi[i];
+            if (ii != 0)
+                for (int j = ii - 1; j < i; j++) sum -= lu[i][j] * yvi[j];
+            else if (sum != 0.0)
+                ii = i + 1;
+            yvi[i] = sum;
+        }
+        for (int i = m - 1; i >= 0; i--) {
+            double sum = yvi[i];
+            for (int j = i + 1; j < m; j++) sum -= lu[i][j] * yvi[j];
+            yvi[i] = sum / lu[i][i];
+        }
+    }
+    double interp(const double *xs) const {
+        double v = 0.;
+        for (int i = 0; i < n; i++) v += yvi[i] * pvg(rdist(xs, x[i]));
+        v += yvi[n] * 1.;
+        return v;
+    }
+};
+
+static bool g_fe_failed = false;  // a finite-element query found fewer than 3 nodes
+
+// surface z and its finite-difference slopes at (X, Y): kriging on the 7 nearest candidate
+// nodes (FEInterpKD, vshot.cpp:166-215); false when fewer than 3 candidates
+static bool fe_interp(const Element *e, double X, double Y, double step, double *zr, double *zx, double *zy) {
+    const int z = fe_zone(e, X, Y);
+    const int a = e->fe_start[z], b = e->fe_start[z + 1];
+    if (b - a < 3) return false;
+    std::vector<std::pair<double, int>> nd;
+    for (int k = a; k < b; ++k) {
+        const double *v = &e->fe_nodes[3 * size_t(e->fe_items[k])];
+        nd.push_back({sqrt(pow(X - v[0], 2) + pow(Y - v[1], 2)), e->fe_items[k]});
+    }
+    std::sort(nd.begin(), nd.end(),
+              [](const std::pair<double, int> &p, const std::pair<double, int> &q) { return p.first < q.first; });
+    const int m = (int)nd.size() > 7 ? 7 : (int)nd.size();
+    double px[7][2], py[7];
+    for (int i = 0; i < m; ++i) {
+        const double *v = &e->fe_nodes[3 * size_t(nd[i].second)];
+        px[i][0] = v[0];
+        px[i][1] = v[1];
+        py[i] = v[2];
+    }
+    FeKrig gm;
+    gm.setup(px, py, m);
+    double xy[2] = {X, Y};
+    *zr = gm.interp(xy);
+    xy[0] += step;
+    const double za = gm.interp(xy);
+    xy[0] -= step;
+    xy[1] += step;
+    const double zb = gm.interp(xy);
+    *zx = (*zr - za) / step;
+    *zy = (*zr - zb) / step;
+    return true;
+}
+
+// ------------------------------------------------------------------------------------
 // Implicit surface F and grad F (surface.cpp:57-413); returns error flag.
 // May overwrite pos[2] with the surface z for data surfaces (surface.cpp:193,246,266,292,332).
 // ------------------------------------------------------------------------------------
@@ -347,6 +569,28 @@ int surface_eval(double pos[3], const Element *e, double *F, double dF[3]) {
             dfz = e->alpha[2];
             *F = dfx * X + dfy * Y + dfz * Z - e->alpha[3];
             break;
+        case 4: {  // finite-element data (surface.cpp:217-241)
+            if (X * X + Y * Y == 0.0) {
+                *F = Z;
+                dfz = 1;
+                break;
+            }
+            const double density = (double)(e->fe_nodes.size() / 3) / e->aperture_area;
+            const double delta = 0.001 / sqrt(density);
+            double zr = 0, zx = 0, zy = 0;
+            if (!fe_interp(e, X, Y, delta, &zr, &zx, &zy)) {
+                // the reference throws here and the run does not return
+                g_fe_failed = true;
+                err = 1;
+                break;
+            }
+            pos[2] = zr;
+            *F = Z - zr;
+            dfx = zx;
+            dfy = zy;
+            dfz = 1.0;
+            break;
+        }
         case 5: {
             if (X * X + Y * Y == 0.0) {
                 *F = Z;
@@ -1509,6 +1753,13 @@ void aperture_plane(Element *e) {  // apertureplane.cpp:57-491
             e->z_aperture = lastz;
             break;
         }
+        case 'e': {  // apertureplane.cpp:455-468 scans the nodes' second coordinate
+            double lastz = 0.0;
+            for (size_t i = 0; i + 2 < e->fe_nodes.size(); i += 3)
+                if (e->fe_nodes[i + 1] > lastz) lastz = e->fe_nodes[i + 1];
+            e->z_aperture = lastz;
+            break;
+        }
         default:
             break;
     }
@@ -1893,6 +2144,7 @@ void merge_records(Context *cx) {
 
 int run_trace(Context *cx, unsigned seed) {
     cx->all.clear();
+    g_fe_failed = false;
     cx->stage_records.assign(cx->stages.size(), {});
     if (!init_geometries(cx)) return -1;
     const bool explicit_rays = !cx->explicit_pos.empty();
@@ -2032,6 +2284,11 @@ int run_trace(Context *cx, unsigned seed) {
             carry.swap(next);
         }
     } catch (int) {
+        return -1;
+    }
+    if (g_fe_failed) {
+        g_fe_failed = false;
+        cx->log("Interpolation failed to find nearby nodes to ray hit in FEA surface.");
         return -1;
     }
     merge_records(cx);
@@ -2388,6 +2645,18 @@ int st_element_surface_file(void *p, st_uint_t s, st_uint_t i, const char *file)
             e->surface = 'i';
             e->surface_type = 9;
         }
+    } else if (ext == "fed") {  // input.cpp:510-561
+        rd();  // name line
+        rd();
+        const int np = atoi(line);
+        e->fe_nodes.assign(3 * size_t(np > 0 ? np : 0), 0.0);
+        for (int k = 0; k < np; ++k) {
+            rd();
+            sscanf(line, "%lg %lg %lg", &e->fe_nodes[3 * k], &e->fe_nodes[3 * k + 1], &e->fe_nodes[3 * k + 2]);
+        }
+        if (np > 0) fe_build(e);
+        e->surface = 'e';
+        e->surface_type = 4;
     } else {
         cx->log("Surface file type extension unknown: '%s'\n", ext.c_str());
         ok = false;

@@ -504,6 +504,179 @@ __device__ inline bool splint(const double *xa, const double *ya, const double *
     return true;
 }
 
+// ------------------------------------------------------------------------------------
+// Finite-element surface (vshot.cpp:166-242): kriging with a power-law variogram on the 7
+// nearest nodes among a query zone's candidates (Numerical Recipes 3rd ed. 3.7.4, Krig with
+// Powvargram; LU decomposition with implicit partial pivoting, 2.3), arithmetic in the
+// reference's order (interpolate.cpp:5-238).  Table layout: st_host.cpp fe_table.
+// ------------------------------------------------------------------------------------
+static __device__ unsigned int g_fe_fail = 0;  // a query found fewer than 3 candidate nodes
+
+struct FeKriging {
+    int n;
+    double x[7][2], alph;
+    double lu[8][8], yvi[8];
+    __device__ double pvg(double r) const { return 0.0 + alph * pow(r, 1.999); }
+    __device__ static double dist(double ax, double ay, double bx, double by) {
+        double d = 0.;
+        d += (ax - bx) * (ax - bx);
+        d += (ay - by) * (ay - by);
+        return sqrt(d);
+    }
+    __device__ void setup(const double *py) {
+        double num = 0., den = 0.;
+        for (int i = 0; i < n; i++)
+            for (int j = i + 1; j < n; j++) {
+                double rb = 0.;
+                rb += (x[i][0] - x[j][0]) * (x[i][0] - x[j][0]);
+                rb += (x[i][1] - x[j][1]) * (x[i][1] - x[j][1]);
+                rb = pow(rb, 0.5 * 1.999);
+                num += rb * (0.5 * ((py[i] - py[j]) * (py[i] - py[j])) - 0.0);
+                den += rb * rb;
+            }
+        alph = num / den;
+        const int m = n + 1;
+        for (int i = 0; i < n; i++) {
+            for (int j = i; j < n; j++) lu[i][j] = lu[j][i] = pvg(dist(x[i][0], x[i][1], x[j][0], x[j][1]));
+            lu[i][n] = lu[n][i] = 1.;
+        }
+        lu[n][n] = 0.;
+        double vv[8];
+        int indx[8];
+        for (int i = 0; i < m; i++) {
+            double big = 0.0;
+            for (int j = 0; j < m; j++) big = fabs(lu[i][j]) > big ? fabs(lu[i][j]) : big;
+            vv[i] = 1.0 / big;
+        }
+        for (int k = 0; k < m; k++) {
+            double big = 0.0;
+            int imax = k;
+            for (int i = k; i < m; i++) {
+                const double t = vv[i] * fabs(lu[i][k]);
+                if (t > big) {
+                    big = t;
+                    imax = i;
+                }
+            }
+            if (k != imax) {
+                for (int j = 0; j < m; j++) {
+                    const double t = lu[imax][j];
+                    lu[imax][j] = lu[k][j];
+                    lu[k][j] = t;
+                }
+                vv[imax] = vv[k];
+            }
+            indx[k] = imax;
+            if (lu[k][k] == 0.0) lu[k][k] = 1.0e-40;
+            for (int i = k + 1; i < m; i++) {
+                const double t = lu[i][k] /= lu[k][k];
+                for (int j = k + 1; j < m; j++) lu[i][j] -= t * lu[k][j];
+            }
+        }
+        for (int i = 0; i < n; i++) yvi[i] = py[i];
+        yvi[n] = 0.;
+        int ii = 0;
+        for (int i = 0; i < m; i++) {
+            const int ip = indx[i];
+            double sum = yvi[ip];
+            yvi[ip] = yvi[i];
+            if (ii != 0)
+                for (int j = ii - 1; j < i; j++) sum -= lu[i][j] * yvi[j];
+            else if (sum != 0.0)
+                ii = i + 1;
+            yvi[i] = sum;
+        }
+        for (int i = m - 1; i >= 0; i--) {
+            double sum = yvi[i];
+            for (int j = i + 1; j < m; j++) sum -= lu[i][j] * yvi[j];
+            yvi[i] = sum / lu[i][i];
+        }
+    }
+    __device__ double interp(double qx, double qy) const {
+        double v = 0.;
+        for (int i = 0; i < n; i++) v += yvi[i] * pvg(dist(qx, qy, x[i][0], x[i][1]));
+        v += yvi[n] * 1.;
+        return v;
+    }
+};
+
+// surface z at (X, Y) and the slopes of F = z_local - z (finite differences of step
+// 0.001/sqrt(nodes per aperture area)); 1 when the query zone has fewer than 3 candidates
+static __device__ __noinline__ int fe_eval(const ElemRec &e, const double *sd, double X, double Y, double &zr, double &fx,
+                                    double &fy) {
+    const double *h = sd + e.data_off;
+    const int nn = int(h[0]), lx = int(h[1]), ly = int(h[2]), nz = int(h[7]);
+    const double *starts = h + 8, *items = starts + nz + 1, *nodes = items + int(starts[nz]);
+    double x0 = h[3], x1 = h[4], y0 = h[5], y1 = h[6];
+    int ix = 0, iy = 0;
+    for (int k = 0; k < lx; ++k) {
+        const double c = (x0 + x1) * 0.5;
+        if (X > c) {
+            x0 = c;
+            ix = 2 * ix + 1;
+        } else {
+            x1 = c;
+            ix = 2 * ix;
+        }
+    }
+    for (int k = 0; k < ly; ++k) {
+        const double c = (y0 + y1) * 0.5;
+        if (Y > c) {
+            y0 = c;
+            iy = 2 * iy + 1;
+        } else {
+            y1 = c;
+            iy = 2 * iy;
+        }
+    }
+    const int zone = iy * (1 << lx) + ix;
+    const int a = int(starts[zone]), b = int(starts[zone + 1]);
+    if (b - a < 3) {
+        atomicOr(&g_fe_fail, 1u);
+        return 1;
+    }
+    // the 7 nearest candidates, nearest first (earlier candidates first on ties)
+    double br[7];
+    int bi[7], m = 0;
+    for (int k = a; k < b; ++k) {
+        const int j = int(items[k]);
+        const double dx = X - nodes[3 * j], dy = Y - nodes[3 * j + 1];
+        const double r = sqrt(dx * dx + dy * dy);
+        int p;
+        if (m < 7)
+            p = m++;
+        else if (r < br[6])
+            p = 6;
+        else
+            continue;
+        while (p > 0 && br[p - 1] > r) {
+            br[p] = br[p - 1];
+            bi[p] = bi[p - 1];
+            --p;
+        }
+        br[p] = r;
+        bi[p] = j;
+    }
+    (void)nn;
+    FeKriging g;
+    g.n = m;
+    double py[7];
+    for (int i = 0; i < m; ++i) {
+        g.x[i][0] = nodes[3 * bi[i]];
+        g.x[i][1] = nodes[3 * bi[i] + 1];
+        py[i] = nodes[3 * bi[i] + 2];
+    }
+    g.setup(py);
+    const double step = 0.001 / sqrt(double(nn) / e.area);
+    zr = g.interp(X, Y);
+    const double xa = X + step;
+    const double za = g.interp(xa, Y);
+    const double zb = g.interp(xa - step, Y + step);
+    fx = (zr - za) / step;
+    fy = (zr - zb) / step;
+    return 0;
+}
+
 // F and grad F; may replace pos[2] by the surface z for data surfaces.  0 = ok.
 __device__ inline int surface_eval(const ElemRec &e, const double *sd, double pos[3], double &F, double dF[3]) {
     const double X = pos[0], Y = pos[1], Z = pos[2];
@@ -534,6 +707,22 @@ __device__ inline int surface_eval(const ElemRec &e, const double *sd, double po
             dF[1] = 0.0;
             dF[2] = 1.0;
             return 0;
+        case kSurfFE: {  // surface.cpp:217-241
+            if (X * X + Y * Y == 0.0) {
+                F = Z;
+                dF[0] = dF[1] = 0.0;
+                dF[2] = 1.0;
+                return 0;
+            }
+            double zr, fx, fy;
+            if (fe_eval(e, sd, X, Y, zr, fx, fy)) return 1;
+            pos[2] = zr;
+            F = Z - zr;
+            dF[0] = fx;
+            dF[1] = fy;
+            dF[2] = 1.0;
+            return 0;
+        }
         case kSurfVshot: {
             if (X * X + Y * Y == 0.0) {
                 F = Z;

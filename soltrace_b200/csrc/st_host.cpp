@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <climits>
+#include <limits>
 #include <numeric>
 #include <string>
 #include <strings.h>
@@ -694,6 +695,66 @@ bool build_ground_grid(const std::vector<Elem> &els, const float4 *sphere, Stage
     return true;
 }
 
+// Zone table of a finite-element surface for the device (st_device.cuh fe_eval), the
+// neighbourhoods the reference's st_hash_tree gives its nodes (input.cpp:538-556,
+// treemesh.cpp:353-535): the nodes' bounding box halved floor(log2(extent / zone)) >= 1
+// times per axis, zone = 1.5 sqrt(area per node); a query in zone (ix, iy) considers the
+// nodes of that zone, then of its 8 neighbours (x offset outer, y inner).  Layout, in
+// doubles: N, levels x, levels y, xmin, xmax, ymin, ymax, zone count Z, Z + 1 list starts,
+// the lists (node indices), the nodes (x, y, z).
+void fe_table(const std::vector<double> &nodes, std::vector<double> &out) {
+    const size_t n = nodes.size() / 3;
+    double xmin = std::numeric_limits<double>::max(), ymin = xmin, xmax = -xmin, ymax = -xmin;
+    for (size_t i = 0; i < n; ++i) {
+        const double x = nodes[3 * i], y = nodes[3 * i + 1];
+        xmax = x > xmax ? x : xmax;
+        ymax = y > ymax ? y : ymax;
+        xmin = x < xmin ? x : xmin;
+        ymin = y < ymin ? y : ymin;
+    }
+    const double zone = 1.5 * sqrt(((xmax - xmin) * (ymax - ymin)) / (double)std::max<size_t>(n, 1));
+    const double inv_ln2 = 1. / log(2.);
+    const int lx = std::max(1, (int)floor(log((xmax - xmin) / zone) * inv_ln2));
+    const int ly = std::max(1, (int)floor(log((ymax - ymin) / zone) * inv_ln2));
+    const int nx = 1 << std::min(lx, 12), ny = 1 << std::min(ly, 12);
+    auto zone_of = [&](double x, double y) {
+        double x0 = xmin, x1 = xmax, y0 = ymin, y1 = ymax;
+        int ix = 0, iy = 0;
+        for (int k = 0; k < lx && k < 12; ++k) {
+            const double c = (x0 + x1) * 0.5;
+            if (x > c) x0 = c, ix = 2 * ix + 1;
+            else x1 = c, ix = 2 * ix;
+        }
+        for (int k = 0; k < ly && k < 12; ++k) {
+            const double c = (y0 + y1) * 0.5;
+            if (y > c) y0 = c, iy = 2 * iy + 1;
+            else y1 = c, iy = 2 * iy;
+        }
+        return iy * nx + ix;
+    };
+    std::vector<std::vector<int>> own(size_t(nx) * ny);
+    for (size_t i = 0; i < n; ++i) own[zone_of(nodes[3 * i], nodes[3 * i + 1])].push_back(int(i));
+    std::vector<double> starts, items;
+    for (int iy = 0; iy < ny; ++iy)
+        for (int ix = 0; ix < nx; ++ix) {
+            starts.push_back(double(items.size()));
+            for (int i : own[size_t(iy) * nx + ix]) items.push_back(i);
+            for (int dx = -1; dx < 2; ++dx)
+                for (int dy = -1; dy < 2; ++dy) {
+                    const int jx = ix + dx, jy = iy + dy;
+                    if ((dx == 0 && dy == 0) || jx < 0 || jx >= nx || jy < 0 || jy >= ny) continue;
+                    for (int i : own[size_t(jy) * nx + jx]) items.push_back(i);
+                }
+        }
+    starts.push_back(double(items.size()));
+    const double head[8] = {double(n), double(std::min(lx, 12)), double(std::min(ly, 12)), xmin, xmax, ymin, ymax,
+                            double(nx) * ny};
+    out.insert(out.end(), head, head + 8);
+    out.insert(out.end(), starts.begin(), starts.end());
+    out.insert(out.end(), items.begin(), items.end());
+    out.insert(out.end(), nodes.begin(), nodes.begin() + 3 * n);
+}
+
 // Median-split BVH over element bounding spheres (stage coordinates).
 void build_bvh(const std::vector<Elem> &els, std::vector<BvhNode> &nodes, std::vector<int> &items) {
     struct Item {
@@ -1069,10 +1130,6 @@ bool flatten(Context *cx, HostScene &hs) {
         sr.tracethrough = st.tracethrough;
         sr.bvh_off = -1;
         for (const Elem &e : st.elems) {
-            if (e.fe_surface) {
-                cx->log("finite-element surface files (.fed) are not supported by the B200 trace");
-                return false;
-            }
             ElemRec r;
             memset(&r, 0, sizeof r);
             for (int k = 0; k < 9; ++k) r.R[k] = e.R[k];
@@ -1121,6 +1178,9 @@ bool flatten(Context *cx, HostScene &hs) {
                     hs.surf_data.insert(hs.surf_data.end(), e.spl_y.begin(), e.spl_y.end());
                     hs.surf_data.insert(hs.surf_data.end(), e.spl_y2.begin(), e.spl_y2.end());
                     r.spl_n = int(e.spl_x.size());
+                    break;
+                case kSurfFE:
+                    fe_table(e.vshot, hs.surf_data);
                     break;
                 default:
                     break;

@@ -44,4 +44,15 @@ int launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, 
     return records ? wf_launch<0, 1>(S, hit_sid, hit_el, hit_idx, total, rs, O, W, Q, replay, st)
                    : wf_launch<0, 0>(S, hit_sid, hit_el, hit_idx, total, rs, O, W, Q, replay, st);
 }
+// finite-element queries of this precision's kernels that found too few nodes since the
+// last call (the flag is cleared)
+unsigned take_fe_failures_fp64() {
+    unsigned v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_fe_fail, sizeof v) != cudaSuccess) return 0;
+    if (v) {
+        const unsigned z = 0;
+        cudaMemcpyToSymbol(g_fe_fail, &z, sizeof z);
+    }
+    return v;
+}
 }  // namespace stb

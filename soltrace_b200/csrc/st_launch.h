@@ -115,6 +115,9 @@ int launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid,
 void launch_sort_by_element(const uint32_t *total, const uint64_t *hit_sid, const uint32_t *hit_el, uint32_t n_elem0,
                             uint32_t *elem_count, uint32_t *elem_cursor, uint32_t *scratch_total, uint64_t *s_sid,
                             uint32_t *s_el, uint32_t *s_idx, uint32_t max_n, cudaStream_t st);
+// finite-element interpolation failures flagged by the kernels since the last call
+unsigned take_fe_failures_fp64();
+unsigned take_fe_failures_mixed();
 void launch_offsets(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_t *total, cudaStream_t st);
 void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uint32_t *counts,
                     const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st);

@@ -618,6 +618,11 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             out.flux.emplace_back(accv.begin() + flux_off[m],
                                   accv.begin() + flux_off[m] + size_t(rq.flux[m].nx) * rq.flux[m].ny);
         out.readback_ms += ms_since(tr);
+        if (rq.precision ? take_fe_failures_mixed() : take_fe_failures_fp64()) {
+            // the reference throws at such a query (vshot.cpp:177-178) and returns no result
+            out.error = "Interpolation failed to find nearby nodes to ray hit in FEA surface.";
+            return false;
+        }
         if (out.flags & kFlagBadInteraction) {
             out.error = "Bad optical interaction type (only 1 = refraction and 2 = reflection are traced)";
             return false;

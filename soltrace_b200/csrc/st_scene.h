@@ -29,7 +29,7 @@ enum SurfType : int {
     kSurfConic = 1,      // conic of revolution / cone (g, s, p, o, c)
     kSurfCylinder = 2,   // 't'
     kSurfFlat = 3,       // 'f'
-    kSurfFE = 4,         // 'e' finite-element data (not supported on the device)
+    kSurfFE = 4,         // 'e' finite-element data
     kSurfVshot = 5,      // 'v'
     kSurfZernike = 6,    // 'm'
     kSurfSingleAxis = 7, // conic with one curvature (Cy = 0)

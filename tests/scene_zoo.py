@@ -75,6 +75,25 @@ def write_sht(path, focal=2.0, n=400, seed=5):
             f.write(f"{x:.6f} {y:.6f} {sx:.8f} {sy:.8f} 0\n")
 
 
+def write_fed(path, focal=2.0, half=3.5, side=30, seed=7):
+    # finite-element nodes of a paraboloid z = r^2/(4f) on a jittered square grid reaching well
+    # past the aperture, so that every zone of the nodes' bounding box has nodes around it
+    # (a query in a zone with fewer than 3 nodes nearby makes the reference throw)
+    rng = np.random.default_rng(seed)
+    c = 1.0 / (4.0 * focal)
+    g = np.linspace(-half, half, side)
+    pts = []
+    for x in g:
+        for y in g:
+            x1, y1 = x + rng.uniform(-0.2, 0.2) * (g[1] - g[0]), y + rng.uniform(-0.2, 0.2) * (g[1] - g[0])
+            pts.append((x1, y1, c * (x1 * x1 + y1 * y1)))
+    with open(path, "w") as f:
+        f.write("fe surface\n")
+        f.write(f"{len(pts)}\n")
+        for x, y, z in pts:
+            f.write(f"{float(x)!r} {float(y)!r} {float(z)!r}\n")
+
+
 def zoo(tmpdir: str) -> dict:
     """name -> Scene"""
     os.makedirs(tmpdir, exist_ok=True)
@@ -134,6 +153,9 @@ def zoo(tmpdir: str) -> dict:
     t = np.linspace(0, 20, 30)
     inten = np.where(t < 4.65, 1.0, 0.05 * np.exp(-(t - 4.65) / 4.0))
     dish = Element(aperture="c", aperture_params=(4.0,), surface="p", surface_params=(0.125, 0.125), **P)
+    fed = os.path.join(tmpdir, "dish.fed")
+    write_fed(fed)
+    S["fe_surface"] = _two_stage([Element(aperture="c", aperture_params=(4.0,), surface="e", surface_file=fed, **P)])
     S["sun_gauss"] = _two_stage([dish], sun=Sun("g", 2.5, (0.0, 0.0, 100.0)))
     S["sun_table"] = _two_stage([dish], sun=Sun("d", 0.0, (0.0, 0.0, 100.0), table=(t, inten)))
     S["sun_point"] = _two_stage([dish], sun=Sun("p", 4.65, (0.0, 0.0, 3.0), point_source=True), n=500)

@@ -43,7 +43,7 @@ ZOO_NAMES = ["sphere_circle", "sphere_line", "hyperboloid", "ellipsoid", "parabo
              "parabola_rect", "parabola_annulus", "parabola_irrtri", "parabola_quad", "trough_line", "cone",
              "general", "flat_circle", "torus", "torus_sector", "cylinder", "zernike", "poly", "spline", "vshot",
              "sun_gauss", "sun_table", "sun_point", "sun_oblique", "optics_pillbox", "optics_diffuse", "refl_table",
-             "refraction", "virtual_stage", "tracethrough", "no_multihit", "multi_element"]
+             "refraction", "virtual_stage", "tracethrough", "no_multihit", "multi_element", "fe_surface"]
 
 
 @pytest.mark.parametrize("name", ZOO_NAMES + list(_bench_scenes()))
@@ -53,7 +53,11 @@ def test_fp64_matches_oracle_ray_by_ray(product, oracle, zoo_scenes, name):
     b = run_scene(oracle, sc, 11, PHILOX)
     assert a[0] == b[0], (a[3], b[3])
     assert a[2] == b[2]  # sun box and SunRayCount
-    assert_same_records(a[1], b[1], pos_tol=1e-9, rel_tol=2e-12, dir_tol=1e-9)
+    # the finite-element surface interpolates with pow(), whose last bit differs between the
+    # device and the host library; the Newton iteration on it then stops a step earlier or
+    # later within its 1e-6 relative tolerance
+    tol = 1e-7 if name == "fe_surface" else 1e-9
+    assert_same_records(a[1], b[1], pos_tol=tol, rel_tol=2e-12, dir_tol=tol)
 
 
 def _explicit_setup(pos, cos):

@@ -44,7 +44,8 @@ def test_oracle_reproduces_reference_golden(oracle, zoo_scenes, name):
         assert msg == g["messages"]
 
 
-@pytest.mark.parametrize("name,seed", [("dish", 3), ("trough", 5), ("refraction", 7), ("spline", 9), ("torus", 13)])
+@pytest.mark.parametrize("name,seed", [("dish", 3), ("trough", 5), ("refraction", 7), ("spline", 9), ("torus", 13),
+                                       ("fe_surface", 15)])
 def test_oracle_matches_live_reference(oracle, reference, zoo_scenes, name, seed):
     if name == "dish":
         sc = scenes.dish_scene(5000)
