@@ -107,6 +107,11 @@ struct Context {
     std::vector<double> stage_s0, stage_s1;  // saved: 8 doubles per stage-1 record, 7 per ray
     bool replaying = false;
     std::vector<double> replay_s0, replay_s1;
+    // the flattened scene of the last run and a signature of the inputs it was built from:
+    // a run whose inputs are unchanged reuses it (geometry set-up, grids and lists skipped)
+    HostScene scene_cache;
+    uint64_t scene_sig = 0;
+    bool scene_valid = false;
     Workspace *ws = nullptr;     // device buffers reused by every run of this context
     ~Context() {
         if (ws) workspace_destroy(ws);
@@ -755,6 +760,114 @@ void fe_table(const std::vector<double> &nodes, std::vector<double> &out) {
     out.insert(out.end(), nodes.begin(), nodes.begin() + 3 * n);
 }
 
+// Outgoing-beam candidate lists of the first stage's flat elements (heliostat fields).
+//
+// A sun ray reflected by a flat element leaves it close to the mirror image of the sun
+// direction about the element's normal: sunshape, slope and specularity errors move it by
+// tens of milliradians at most.  For every flat element j of a first stage with a ground
+// grid and a directional sun, the list holds every element k whose padded bounding sphere
+// meets the volume swept by rays that start inside j's bounding sphere with a direction
+// within kBeamHalfAngle of that axis, up to where such rays leave the stage's z band.  A ray
+// leaving j inside the cone (checked per ray, in float with 1e-3 rad of margin in the
+// lists) is searched against the list; any other ray walks the ground grid.  Lists longer
+// than kBeamMaxList are not kept.
+constexpr double kBeamHalfAngle = 0.1;  // rad
+constexpr size_t kBeamMaxList = 256;
+
+void build_beam_lists(Context *cx, HostScene &hs) {
+    const size_t ne = hs.elems.size();
+    hs.beam_axis.assign(ne, float4{0.f, 0.f, 0.f, 2.f});
+    hs.beam_range.assign(ne, int2{0, 0});
+    hs.beam_elem.clear();
+    StageRec &sr = hs.dev.stages[0];
+    if (cx->sun.point_source || !sr.grid_on || !sr.multihit) return;
+    const StageM &st = cx->stages[0];
+    const double *Rs = hs.dev.sun.Rsun;
+    const double din[3] = {Rs[6], Rs[7], Rs[8]};  // sun-ray direction in the stage frame
+    const double th = kBeamHalfAngle + 1e-3, tan_th = tan(th);
+    const double zlo = sr.gzlo, zhi = sr.gzhi;
+    const size_t n = st.elems.size();
+    std::vector<double> rad(n);
+    for (size_t k = 0; k < n; ++k) {
+        const double r = accept_radius(st.elems[k]);
+        const double *c = st.elems[k].origin;
+        rad[k] = r < 0 ? -1.0 : r * (1.0 + 1e-6) + 1e-3 + 1e-6 * (fabs(c[0]) + fabs(c[1]) + fabs(c[2]));
+    }
+    // centres binned on an x-y grid, so that each list only examines elements within its
+    // reach; elements without a finite bound are examined by every list
+    double rmax = 0, xlo = 1e300, ylo = 1e300, xhi = -1e300, yhi = -1e300;
+    std::vector<int> unbounded;
+    for (size_t k = 0; k < n; ++k) {
+        if (rad[k] < 0) {
+            unbounded.push_back(int(k));
+            continue;
+        }
+        rmax = std::max(rmax, rad[k]);
+        xlo = std::min(xlo, st.elems[k].origin[0]);
+        xhi = std::max(xhi, st.elems[k].origin[0]);
+        ylo = std::min(ylo, st.elems[k].origin[1]);
+        yhi = std::max(yhi, st.elems[k].origin[1]);
+    }
+    const double bin = std::max(4.0 * rmax, std::max(xhi - xlo, yhi - ylo) / 1024.0) + 1e-9;
+    const int bnx = xhi >= xlo ? int((xhi - xlo) / bin) + 1 : 1, bny = yhi >= ylo ? int((yhi - ylo) / bin) + 1 : 1;
+    std::vector<std::vector<int>> bins(size_t(bnx) * bny);
+    for (size_t k = 0; k < n; ++k)
+        if (rad[k] >= 0)
+            bins[size_t(int((st.elems[k].origin[1] - ylo) / bin)) * bnx + int((st.elems[k].origin[0] - xlo) / bin)]
+                .push_back(int(k));
+    std::vector<int> list, cand;
+    for (size_t j = 0; j < n; ++j) {
+        const Elem &e = st.elems[j];
+        if (e.stype != 3 || !e.enabled || rad[j] < 0) continue;
+        const double nrm[3] = {e.R[6], e.R[7], e.R[8]};
+        const double dn = din[0] * nrm[0] + din[1] * nrm[1] + din[2] * nrm[2];
+        double a[3] = {din[0] - 2.0 * dn * nrm[0], din[1] - 2.0 * dn * nrm[1], din[2] - 2.0 * dn * nrm[2]};
+        const double la = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        if (!(la > 0)) continue;
+        for (double &v : a) v /= la;
+        // how far along the beam a ray can still be inside the z band
+        const double elev = asin(std::max(-1.0, std::min(1.0, a[2])));
+        const double *cj = e.origin;
+        double s_max = 1e300;
+        if (elev - th > 0) s_max = (zhi - (cj[2] - rad[j])) / sin(elev - th);
+        else if (elev + th < 0) s_max = ((cj[2] + rad[j]) - zlo) / sin(-(elev + th));
+        // elements whose centre is within reach of the beam's in-band part
+        cand.assign(unbounded.begin(), unbounded.end());
+        const double reach = s_max + 2.0 * rad[j] + rmax;
+        if (reach >= 1e299 || reach / bin > bnx + bny) {
+            for (size_t k = 0; k < n; ++k)
+                if (rad[k] >= 0) cand.push_back(int(k));
+        } else {
+            const int x0 = std::max(0, int((cj[0] - reach - xlo) / bin)), x1 = std::min(bnx - 1, int((cj[0] + reach - xlo) / bin));
+            const int y0 = std::max(0, int((cj[1] - reach - ylo) / bin)), y1 = std::min(bny - 1, int((cj[1] + reach - ylo) / bin));
+            for (int by = y0; by <= y1; ++by)
+                for (int bx = x0; bx <= x1; ++bx)
+                    for (int k : bins[size_t(by) * bnx + bx]) cand.push_back(k);
+        }
+        list.clear();
+        bool too_long = false;
+        for (size_t q = 0; q < cand.size() && !too_long; ++q) {
+            const size_t k = size_t(cand[q]);
+            if (k == j || !st.elems[k].enabled) continue;
+            const double rk = rad[k] < 0 ? 1e300 : rad[k];
+            const double *ck = st.elems[k].origin;
+            const double v[3] = {ck[0] - cj[0], ck[1] - cj[1], ck[2] - cj[2]};
+            const double t = v[0] * a[0] + v[1] * a[1] + v[2] * a[2];
+            if (t < -(rad[j] + rk) || t - rk > rad[j] + s_max) continue;
+            const double w[3] = {v[0] - t * a[0], v[1] - t * a[1], v[2] - t * a[2]};
+            const double p = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+            if (p > rk + rad[j] + (std::max(t, 0.0) + rk + rad[j]) * tan_th) continue;
+            list.push_back(int(k));
+            too_long = list.size() > kBeamMaxList;
+        }
+        if (too_long) continue;
+        const size_t g = size_t(sr.first_elem) + j;
+        hs.beam_axis[g] = float4{float(a[0]), float(a[1]), float(a[2]), float(cos(kBeamHalfAngle))};
+        hs.beam_range[g] = int2{int(hs.beam_elem.size()), int(hs.beam_elem.size() + list.size())};
+        hs.beam_elem.insert(hs.beam_elem.end(), list.begin(), list.end());
+    }
+}
+
 // Median-split BVH over element bounding spheres (stage coordinates).
 void build_bvh(const std::vector<Elem> &els, std::vector<BvhNode> &nodes, std::vector<int> &items) {
     struct Item {
@@ -1199,6 +1312,7 @@ bool flatten(Context *cx, HostScene &hs) {
         }
     }
     if (!sun_setup(cx, hs)) return false;
+    build_beam_lists(cx, hs);
     hs.dev.sunshape_on = cx->err_sun;
     hs.dev.errors_on = cx->err_opt;
     return true;
@@ -1298,6 +1412,101 @@ std::vector<double> saved_second_stage(std::vector<double> in, std::vector<doubl
     return s1;
 }
 
+// 64-bit FNV-1a signature of every input the flattened scene is built from: optics, stages
+// and elements (with their surface data), the sun and the error switches.
+struct SigHash {
+    uint64_t h = 1469598103934665603ull;
+    void bytes(const void *p, size_t n) {
+        const unsigned char *c = static_cast<const unsigned char *>(p);
+        for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
+    }
+    template <typename T>
+    void pod(const T &v) {
+        bytes(&v, sizeof v);
+    }
+    void vec(const std::vector<double> &v) {
+        pod(v.size());
+        if (!v.empty()) bytes(v.data(), v.size() * sizeof(double));
+    }
+    void str(const std::string &s) {
+        pod(s.size());
+        bytes(s.data(), s.size());
+    }
+};
+
+uint64_t scene_signature(const Context *cx) {
+    SigHash g;
+    g.pod(cx->err_sun);
+    g.pod(cx->err_opt);
+    const SunM &s = cx->sun;
+    g.pod(s.shape);
+    g.pod(s.sigma);
+    g.pod(s.point_source);
+    g.vec(s.ang);
+    g.vec(s.inten);
+    g.bytes(s.origin, sizeof s.origin);
+    g.pod(cx->optics.size());
+    for (const OpticSet &o : cx->optics) {
+        g.str(o.name);
+        for (const Face *f : {&o.front, &o.back}) {
+            g.pod(f->dist);
+            g.pod(f->optnum);
+            g.pod(f->apgr);
+            g.pod(f->order);
+            g.pod(f->refl);
+            g.pod(f->trans);
+            g.pod(f->slope);
+            g.pod(f->spec);
+            g.bytes(f->n, sizeof f->n);
+            g.bytes(f->ab12, sizeof f->ab12);
+            g.vec(f->refl_tab);
+            g.vec(f->trans_tab);
+            g.pod(f->use_refl);
+            g.pod(f->use_trans);
+        }
+    }
+    g.pod(cx->stages.size());
+    for (const StageM &st : cx->stages) {
+        g.pod(st.multihit);
+        g.pod(st.virt);
+        g.pod(st.tracethrough);
+        g.bytes(st.origin, sizeof st.origin);
+        g.bytes(st.aim, sizeof st.aim);
+        g.pod(st.zrot);
+        g.pod(st.elems.size());
+        for (const Elem &e : st.elems) {
+            g.pod(e.enabled);
+            g.bytes(e.origin, sizeof e.origin);
+            g.bytes(e.aim, sizeof e.aim);
+            g.pod(e.zrot);
+            g.pod(e.shape);
+            g.bytes(e.p, sizeof e.p);
+            g.pod(e.surface);
+            g.pod(e.stype);
+            g.pod(e.kappa);
+            g.bytes(e.alpha, sizeof e.alpha);
+            g.pod(e.vcx);
+            g.pod(e.vcy);
+            g.pod(e.ra);
+            g.pod(e.rs);
+            g.pod(e.cone);
+            g.pod(e.curv);
+            g.pod(e.fit_order);
+            g.vec(e.bcoef);
+            g.vec(e.poly);
+            g.vec(e.spl_x);
+            g.vec(e.spl_y);
+            g.vec(e.spl_y2);
+            g.vec(e.vshot);
+            g.pod(e.vshot_rows);
+            g.pod(e.fe_surface);
+            g.pod(e.interaction);
+            g.str(e.optic);
+        }
+    }
+    return g.h;
+}
+
 int run(Context *cx, unsigned seed) {
     cx->records.clear();
     memset(&cx->stats, 0, sizeof cx->stats);
@@ -1316,9 +1525,16 @@ int run(Context *cx, unsigned seed) {
         return -1;
     }
     const auto t0 = std::chrono::steady_clock::now();
-    if (!init_geometries(cx)) return -1;
-    HostScene hs;
-    if (!flatten(cx, hs)) return -1;
+    if (!cx->scene_valid || cx->scene_sig != scene_signature(cx)) {
+        cx->scene_valid = false;
+        if (!init_geometries(cx)) return -1;
+        cx->scene_cache = HostScene();
+        if (!flatten(cx, cx->scene_cache)) return -1;
+        // the set-up fills derived fields; the next run starts from this state
+        cx->scene_sig = scene_signature(cx);
+        cx->scene_valid = true;
+    }
+    const HostScene &hs = cx->scene_cache;
     RunRequest rq;
     rq.n_hits = uint64_t(cx->raycount);
     rq.max_sun = uint64_t(std::max(cx->raymax, 0));

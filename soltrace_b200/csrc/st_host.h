@@ -22,6 +22,9 @@ struct HostScene {
     std::vector<int2> stage_cells;    // ground-grid cells ([start, end) into the grid entries)
     std::vector<float4> grid_sphere;  // ground-grid entries: element bounding sphere
     std::vector<int> grid_elem;       // ground-grid entries: element index within the stage
+    std::vector<float4> beam_axis;    // per element: outgoing-beam axis and cosine limit (w > 1: none)
+    std::vector<int2> beam_range;     // per element: [start, end) in beam_elem
+    std::vector<int> beam_elem;       // outgoing-beam candidate lists (element index within the stage)
     std::vector<float4> elem_sphere;  // per element: origin (stage coordinates), padded bounding radius
     std::vector<float4> cell_disc;  // sun-plane grid entries: disc centre x, y, radius, element
     std::vector<float4> cell_par;   // sun-plane grid entries: footprint parallelogram (dual basis rows)

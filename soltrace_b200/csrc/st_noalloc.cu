@@ -130,6 +130,9 @@ extern "C" int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsig
     S.stage_cells = d_scells;
     S.grid_sphere = d_gsph;
     S.grid_elem = d_gel;
+    S.beam_axis = nullptr;  // the probe does not search from a known element
+    S.beam_range = nullptr;
+    S.beam_elem = nullptr;
     S.surf_data = d_surf;
     S.bvh = d_bvh;
     S.bvh_items = d_bvh_items;

@@ -56,7 +56,7 @@ cudaError_t upload(DevBuf &b, const std::vector<T> &v, cudaStream_t s, uint64_t 
 struct Workspace {
     int device = -1;
     cudaStream_t stream = nullptr;
-    DevBuf stage_cells, grid_sphere, grid_elem;
+    DevBuf stage_cells, grid_sphere, grid_elem, beam_axis, beam_range, beam_elem;
     DevBuf elems, elem_sphere, optics, surf, tables, bvh, bvh_items, cell_start, cell_disc, cell_par, inv_cdf, expos,
         excos;
     DevBuf acc, ctr, rs, rec_count, hit_elem, counts, offsets, total, hit_sid, hit_el, recs;
@@ -207,6 +207,9 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     CK(upload(ws.stage_cells, hs.stage_cells, st, out.h2d_bytes));
     CK(upload(ws.grid_sphere, hs.grid_sphere, st, out.h2d_bytes));
     CK(upload(ws.grid_elem, hs.grid_elem, st, out.h2d_bytes));
+    CK(upload(ws.beam_axis, hs.beam_axis, st, out.h2d_bytes));
+    CK(upload(ws.beam_range, hs.beam_range, st, out.h2d_bytes));
+    CK(upload(ws.beam_elem, hs.beam_elem, st, out.h2d_bytes));
     CK(upload(d_optics, hs.optics, st, out.h2d_bytes));
     CK(upload(d_surf, hs.surf_data, st, out.h2d_bytes));
     CK(upload(d_tables, hs.tables, st, out.h2d_bytes));
@@ -225,6 +228,9 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     S.stage_cells = ws.stage_cells.as<int2>();
     S.grid_sphere = ws.grid_sphere.as<float4>();
     S.grid_elem = ws.grid_elem.as<int>();
+    S.beam_axis = hs.beam_axis.empty() ? nullptr : ws.beam_axis.as<float4>();
+    S.beam_range = ws.beam_range.as<int2>();
+    S.beam_elem = ws.beam_elem.as<int>();
     S.optics = d_optics.as<OpticRec>();
     S.surf_data = d_surf.as<double>();
     S.tables = d_tables.as<double>();

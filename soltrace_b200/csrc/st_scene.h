@@ -127,6 +127,12 @@ struct SceneDev {
     const int2 *stage_cells;     // ground-grid cells of every stage: [start, end) of the entries
     const float4 *grid_sphere;   // ground-grid entries: element bounding sphere (stage coordinates)
     const int *grid_elem;        // ground-grid entries: element index within the stage
+    // outgoing-beam lists of flat first-stage elements: rays leaving element j with a
+    // direction d such that d . axis >= w (beam_axis[j] = axis, w; w > 1: no list) can only
+    // meet the elements beam_elem[beam_range[j].x .. beam_range[j].y) of the stage
+    const float4 *beam_axis;
+    const int2 *beam_range;
+    const int *beam_elem;
     StageRec stages[kMaxStages];
     int n_stages;
     SunDev sun;

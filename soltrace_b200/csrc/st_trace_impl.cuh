@@ -134,7 +134,9 @@ __device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const d
     return best;
 }
 
-// Nearest element through the stage's ground grid: a 2-D DDA walk over the cells the ray
+// Nearest element through the stage's ground grid (or, for a ray leaving a flat first-stage
+// element within its outgoing beam, through that element's beam list: see
+// build_beam_lists in st_host.cpp): a 2-D DDA walk over the cells the ray
 // crosses inside the stage's z band, in order of distance.  Entries pass a float test
 // against their padded bounding sphere; the few that pass are collected and given the
 // double-precision element test after the walk (or when the list fills, after which the
@@ -147,6 +149,17 @@ __device__ inline int nearest_grid(const SceneDev &S, const StageRec &st, const 
                                    int from) {
     const float ox = float(ps[0]), oy = float(ps[1]), oz = float(ps[2]);
     const float dx = float(cs[0]), dy = float(cs[1]), dz = float(cs[2]);
+    // a ray leaving a flat element within its outgoing beam: that element's list stands in
+    // for the walk (one pass of the loop below over the list)
+    int2 list = make_int2(0, 0);
+    bool list_mode = false;
+    if (from >= 0 && S.beam_axis) {
+        const float4 ax = S.beam_axis[st.first_elem + from];
+        if (dx * ax.x + dy * ax.y + dz * ax.z >= ax.w) {
+            list_mode = true;
+            list = S.beam_range[st.first_elem + from];
+        }
+    }
     // clip to the z band and the grid box
     float t0 = 0.0f, t1 = 3.0e38f;
     auto clip = [&](float o, float d, float lo, float hi) {
@@ -158,10 +171,12 @@ __device__ inline int nearest_grid(const SceneDev &S, const StageRec &st, const 
             t1 = -1.0f;
         }
     };
-    clip(oz, dz, st.gzlo, st.gzhi);
-    clip(ox, dx, st.gx0, st.gx0 + st.gnx * st.gcell);
-    clip(oy, dy, st.gy0, st.gy0 + st.gny * st.gcell);
-    if (!(t0 <= t1)) return -1;
+    if (!list_mode) {
+        clip(oz, dz, st.gzlo, st.gzhi);
+        clip(ox, dx, st.gx0, st.gx0 + st.gnx * st.gcell);
+        clip(oy, dy, st.gy0, st.gy0 + st.gny * st.gcell);
+        if (!(t0 <= t1)) return -1;
+    }
     const float px = ox + t0 * dx, py = oy + t0 * dy;
     int ix = min(max(int(floorf((px - st.gx0) * st.ginv)), 0), st.gnx - 1);
     int iy = min(max(int(floorf((py - st.gy0) * st.ginv)), 0), st.gny - 1);
@@ -197,16 +212,16 @@ __device__ inline int nearest_grid(const SceneDev &S, const StageRec &st, const 
     float tin = t0;
     for (;;) {
         if (best >= 0 && double(tin) > bp * (1.0 + 1e-6) + 1e-3) break;
-        const int2 range = cells[iy * st.gnx + ix];
+        const int2 range = list_mode ? list : cells[iy * st.gnx + ix];
         for (int k = range.x; k < range.y; ++k) {
-            const float4 bs = S.grid_sphere[k];
+            const float4 bs = list_mode ? S.elem_sphere[st.first_elem + S.beam_elem[k]] : S.grid_sphere[k];
             const float vx = bs.x - ox, vy = bs.y - oy, vz = bs.z - oz;
             const float tc = vx * dx + vy * dy + vz * dz;
             const float wx = vx - tc * dx, wy = vy - tc * dy, wz = vz - tc * dz;
             // radius padded for the float rounding of centre, origin and direction
             const float rr = bs.w + pad_o + 2e-6f * (fabsf(vx) + fabsf(vy) + fabsf(vz));
             if (tc < -rr || wx * wx + wy * wy + wz * wz > rr * rr) continue;
-            const int j = S.grid_elem[k];
+            const int j = list_mode ? S.beam_elem[k] : S.grid_elem[k];
             // the element the ray is leaving (when it certainly cannot be met again), and
             // elements already collected from the last cells
             if (j == from || j == seen1 || j == seen2 || j == seen3) continue;
@@ -216,6 +231,7 @@ __device__ inline int nearest_grid(const SceneDev &S, const StageRec &st, const 
             if (nc == kCand) flush();
             cand[256 * nc++] = j;
         }
+        if (list_mode) break;
         // step to the next cell along the ray
         if (tmx < tmy) {
             tin = tmx;

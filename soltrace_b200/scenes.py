@@ -117,6 +117,16 @@ def _face_args(f: OpticFace):
     return args, keep
 
 
+def push_optic(api: StApi, ctx, idx: int, o: OpticSet) -> None:
+    """Set both faces of optic `idx` (st_optic front, then back)."""
+    for fb, face in ((1, o.front), (2, o.back)):
+        args, keep = _face_args(face)
+        rc = api.st_optic(ctx, idx, fb, *args)
+        del keep
+        if rc is not None and rc < 0:
+            raise RuntimeError(f"st_optic failed ({rc}): {api.messages(ctx)}")
+
+
 def push(api: StApi, ctx, sc: Scene) -> None:
     """Send the scene through the C API setters; raises on any setter failure."""
 
@@ -126,10 +136,7 @@ def push(api: StApi, ctx, sc: Scene) -> None:
 
     for o in sc.optics:
         idx = api.st_add_optic(ctx, o.name.encode())
-        for fb, face in ((1, o.front), (2, o.back)):
-            args, keep = _face_args(face)
-            ok(api.st_optic(ctx, idx, fb, *args), "st_optic")
-            del keep
+        push_optic(api, ctx, idx, o)
     ok(api.st_sun(ctx, int(sc.sun.point_source), sc.sun.shape.encode()[:1], sc.sun.sigma), "st_sun")
     ok(api.st_sun_xyz(ctx, *map(float, sc.sun.xyz)), "st_sun_xyz")
     if sc.sun.table is not None:
