@@ -1090,6 +1090,27 @@ __device__ __forceinline__ bool element_test(const SceneDev &S, const ElemRec &e
     return true;
 }
 
+// element_test for a flat element (surface type 3), without the other surfaces' code: the
+// same arithmetic as element_test's flat branch, for kernels that only meet flat elements
+template <int MIXED>
+__device__ __forceinline__ bool element_test_flat(const ElemRec &e, const double ps[3], const double cs[3],
+                                                  double &plen) {
+    double pe[3], ce[3];
+    to_local(e.R, e.o, ps, cs, pe, ce);
+    pe[0] = pe[0] + 1.0e-5 * ce[0];
+    pe[1] = pe[1] + 1.0e-5 * ce[1];
+    pe[2] = pe[2] + 1.0e-5 * ce[2];
+    const double t = (0.0 - pe[2] != 0.0) ? (0.0 - pe[2]) / (ce[2] + 0.00000000001) : 0.0;
+    if (t < 0) return false;
+    const double ox = pe[0] + ce[0] * t, oy = pe[1] + ce[1] * t;
+    const int in = MIXED ? aperture_in<float>(e, float(ox), float(oy), false) : aperture_in<double>(e, ox, oy, false);
+    if (in != 1) return false;
+    const int s = e.surf | 0x20;
+    if (!(0.0 <= e.zap || s == 'm' || s == 'r')) return false;
+    plen = t;
+    return true;
+}
+
 // ------------------------------------------------------------------------------------
 // Error sampling (errors.cpp:60-226, surfacenormalerrors.cpp:58-167) with per-ray
 // inverse-CDF samplers: |theta| of a 2-D Gaussian is Rayleigh, a pillbox disc is

@@ -1300,6 +1300,8 @@ bool flatten(Context *cx, HostScene &hs) {
             }
             hs.elems.push_back(r);
         }
+        sr.flat_only = 1;
+        for (const Elem &e : st.elems) sr.flat_only &= (e.stype == 3) ? 1 : 0;
         sr.grid_on = 0;
         if (st.elems.size() >= 64)
             build_ground_grid(st.elems, hs.elem_sphere.data() + sr.first_elem, sr, hs.stage_cells, hs.grid_sphere,

@@ -7,9 +7,9 @@
 namespace stb {
 void launch_sun_candidates(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
                            uint32_t *cand, uint32_t *cand_count, const RunState *rs, cudaStream_t st) {
-    const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;
+    const uint32_t nblocks = (n + kCandRays - 1) / kCandRays;
     cudaMemsetAsync(cand_count, 0, sizeof(uint32_t), st);
-    k_sun_candidates<<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, cand, cand_count, rs);
+    k_sun_candidates<<<nblocks, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, cand, cand_count, rs);
 }
 void launch_offsets(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_t *total, cudaStream_t st) {
     k_offsets<<<1, 1024, 0, st>>>(counts, nb, offsets, total);

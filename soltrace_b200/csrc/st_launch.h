@@ -9,6 +9,8 @@ namespace stb {
 
 constexpr int kProbeBlock = 256;
 constexpr int kResolveBlock = 128;  // threads per block of the grid probe's element-test kernel
+constexpr int kCandPerThread = 4;   // sun rays per thread of the grid probe's pre-test kernel
+constexpr int kCandRays = kProbeBlock * kCandPerThread;
 constexpr int kTraceBlock = 128;
 // register-budget variants of the probe and trace kernels (minimum resident blocks per
 // SM given to __launch_bounds__); all compute the same results

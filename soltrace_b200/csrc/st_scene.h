@@ -78,6 +78,7 @@ struct StageRec {
     // bounding disc overlaps it; grid_on = 0 when not built
     int grid_on;
     int gnx, gny, gcell_off;  // cells, first cell in SceneDev::stage_cells
+    int flat_only;            // every element of the stage is flat (surface type 3)
     float gx0, gy0, gcell, ginv, gzlo, gzhi;
 };
 

@@ -292,7 +292,7 @@ __device__ __forceinline__ int2 sun_cell(const SunDev &sun, double xs, double ys
 
 // Sun-ray probe through the grid for one ray; the double-precision ray is built only once
 // a cell entry passes the float pre-test.
-template <int MIXED>
+template <int MIXED, int FLAT = 0>
 __device__ inline int nearest_sun_grid_lazy(const SceneDev &S, const StageRec &st, double xs, double ys) {
     const SunDev &sun = S.sun;
     const int2 range = sun_cell(sun, xs, ys);
@@ -311,7 +311,8 @@ __device__ inline int nearest_sun_grid_lazy(const SceneDev &S, const StageRec &s
             have_ray = true;
         }
         double pl;
-        if (element_test<MIXED>(S, e, ps, cs, pl, nullptr) && pl < bp) {
+        const bool hit = FLAT ? element_test_flat<MIXED>(e, ps, cs, pl) : element_test<MIXED>(S, e, ps, cs, pl, nullptr);
+        if (hit && pl < bp) {
             bp = pl;
             best = j;
         }
@@ -551,7 +552,7 @@ __global__ void __launch_bounds__(kProbeBlock) k_probe(const __grid_constant__ S
 //     hit_elem and the per-kProbeBlock hit counts.
 // On a heliostat field most sun rays miss every footprint and never reach the second
 // kernel, whose warps are then fully occupied by rays that need the element tests.
-template <int MIXED, int MINB>
+template <int MIXED, int MINB, int FLAT>
 __global__ void __launch_bounds__(kResolveBlock, MINB) k_sun_resolve(const __grid_constant__ SceneDev S, uint64_t s0, uint32_t *hit_elem,
                                                                      uint32_t *block_counts, const uint32_t *cand,
                                                                      const uint32_t *cand_count, const RunState *rs) {
@@ -564,7 +565,7 @@ __global__ void __launch_bounds__(kResolveBlock, MINB) k_sun_resolve(const __gri
         rng.init(S.seed, s0 + i, 0);
         const double xs = sun.xmin + (sun.xmax - sun.xmin) * rng.u();
         const double ys = sun.ymin + (sun.ymax - sun.ymin) * rng.u();
-        const int b = nearest_sun_grid_lazy<MIXED>(S, S.stages[0], xs, ys);
+        const int b = nearest_sun_grid_lazy<MIXED, FLAT>(S, S.stages[0], xs, ys);
         hit_elem[i] = (b >= 0) ? uint32_t(b + 1) : 0u;
         if (b >= 0) {
             // one atomic per distinct count slot among the warp's hitting lanes
@@ -582,30 +583,38 @@ __global__ void __launch_bounds__(kProbeBlock) k_sun_candidates(const __grid_con
                                                                 uint32_t *hit_elem, uint32_t *block_counts,
                                                                 uint32_t *cand, uint32_t *cand_count,
                                                                 const RunState *rs) {
-    if (threadIdx.x == 0) block_counts[blockIdx.x] = 0;
+    // a block takes kCandRays sun rays (kCandRays / kProbeBlock per thread, kProbeBlock apart)
+    const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;
+    if (threadIdx.x < kCandPerThread && blockIdx.x * kCandPerThread + threadIdx.x < nb)
+        block_counts[blockIdx.x * kCandPerThread + threadIdx.x] = 0;
     if (rs->reached) return;  // the requested hits are numbered: this batch is surplus
-    const uint32_t i = blockIdx.x * kProbeBlock + threadIdx.x;
-    bool listed = false;
-    if (i < n) {
-        RayRng rng;
-        rng.init(S.seed, s0 + i, 0);
-        const SunDev &sun = S.sun;
-        const double xs = sun.xmin + (sun.xmax - sun.xmin) * rng.u();
-        const double ys = sun.ymin + (sun.ymax - sun.ymin) * rng.u();
-        const int2 range = sun_cell(sun, xs, ys);
-        const float fx = float(xs), fy = float(ys);
-        for (int k = range.x; k < range.y; ++k)
-            if (sun_entry_pass(sun, k, fx, fy)) {
-                listed = true;
-                break;
-            }
-        if (!listed) hit_elem[i] = 0;
+    const SunDev &sun = S.sun;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned bal[kCandPerThread];
+    uint32_t mine = 0;
+    for (int m = 0; m < kCandPerThread; ++m) {
+        const uint32_t i = blockIdx.x * kCandRays + m * kProbeBlock + threadIdx.x;
+        bool listed = false;
+        if (i < n) {
+            RayRng rng;
+            rng.init(S.seed, s0 + i, 0);
+            const double xs = sun.xmin + (sun.xmax - sun.xmin) * rng.u();
+            const double ys = sun.ymin + (sun.ymax - sun.ymin) * rng.u();
+            const int2 range = sun_cell(sun, xs, ys);
+            const float fx = float(xs), fy = float(ys);
+            for (int k = range.x; k < range.y; ++k)
+                if (sun_entry_pass(sun, k, fx, fy)) {
+                    listed = true;
+                    break;
+                }
+            if (!listed) hit_elem[i] = 0;
+        }
+        bal[m] = __ballot_sync(0xffffffffu, listed);
+        mine += __popc(bal[m]);
     }
     // one atomic on the shared count per block: warp counts, their prefix, one reservation
     __shared__ uint32_t wn[kProbeBlock / 32], base;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const unsigned bal = __ballot_sync(0xffffffffu, listed);
-    if (lane == 0) wn[w] = __popc(bal);
+    if (lane == 0) wn[w] = mine;
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t t = 0;
@@ -617,7 +626,12 @@ __global__ void __launch_bounds__(kProbeBlock) k_sun_candidates(const __grid_con
         base = t ? atomicAdd(cand_count, t) : 0u;
     }
     __syncthreads();
-    if (listed) cand[base + wn[w] + __popc(bal & ((1u << lane) - 1u))] = i;
+    uint32_t at = base + wn[w];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int m = 0; m < kCandPerThread; ++m) {
+        if ((bal[m] >> lane) & 1u) cand[at + __popc(bal[m] & lt)] = blockIdx.x * kCandRays + m * kProbeBlock + threadIdx.x;
+        at += __popc(bal[m]);
+    }
 }
 
 // exclusive scan of the per-block counts (one block; counts fit in 32 bits per batch)
