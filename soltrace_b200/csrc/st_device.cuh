@@ -1094,7 +1094,7 @@ __device__ __forceinline__ bool element_test(const SceneDev &S, const ElemRec &e
 // same arithmetic as element_test's flat branch, for kernels that only meet flat elements
 template <int MIXED>
 __device__ __forceinline__ bool element_test_flat(const ElemRec &e, const double ps[3], const double cs[3],
-                                                  double &plen) {
+                                                  double &plen, Hit *full = nullptr) {
     double pe[3], ce[3];
     to_local(e.R, e.o, ps, cs, pe, ce);
     pe[0] = pe[0] + 1.0e-5 * ce[0];
@@ -1108,6 +1108,18 @@ __device__ __forceinline__ bool element_test_flat(const ElemRec &e, const double
     const int s = e.surf | 0x20;
     if (!(0.0 <= e.zap || s == 'm' || s == 'r')) return false;
     plen = t;
+    if (full) {
+        const int back = (ce[2] < 0) ? 0 : 1;
+        full->pe[0] = ox;
+        full->pe[1] = oy;
+        full->pe[2] = 0.0;
+        for (int q = 0; q < 3; ++q) full->ce[q] = ce[q];
+        full->n[0] = back ? -0.0 : 0.0;  // the flipped normal of element_test, signed zeros included
+        full->n[1] = back ? -0.0 : 0.0;
+        full->n[2] = back ? -1.0 : 1.0;
+        full->plen = t;
+        full->back = back;
+    }
     return true;
 }
 

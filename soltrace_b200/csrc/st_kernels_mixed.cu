@@ -6,8 +6,7 @@ namespace stb {
 // Register-budget variants (same code, different __launch_bounds__ minimum blocks per
 // SM): kProbeMinBlocks in st_launch.h; the autotuner picks one.
 template <int V, int FLAT>
-static void resolve_one(const SceneDev &S, uint64_t s0, uint32_t *hit_elem, uint32_t *block_counts,
-                        const uint32_t *cand, const uint32_t *cand_count, const RunState *rs, cudaStream_t st) {
+static void resolve_one(const SceneDev &S, uint64_t s0, const ProbeOut &o, const RunState *rs, cudaStream_t st) {
     // persistent grid: every resident block of the variant on every SM
     static int per_sm = 0;
     if (per_sm == 0) {
@@ -18,27 +17,26 @@ static void resolve_one(const SceneDev &S, uint64_t s0, uint32_t *hit_elem, uint
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    k_sun_resolve<1, kProbeMinBlocks[V], FLAT><<<sms * per_sm, kResolveBlock, 0, st>>>(S, s0, hit_elem, block_counts,
-                                                                                       cand, cand_count, rs);
+    k_sun_resolve<1, kProbeMinBlocks[V], FLAT><<<sms * per_sm, kResolveBlock, 0, st>>>(S, s0, o, rs);
 }
-int launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
-                  uint32_t *cand, uint32_t *cand_count, const RunState *rs, int variant, cudaStream_t st) {
+int launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, const ProbeOut &o, const RunState *rs, int variant,
+                       cudaStream_t st) {
     const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;
     if (S.sun.grid_on && !S.explicit_rays && !S.sun.point_source) {
-        launch_sun_candidates(S, s0, n, hit_elem, block_counts, cand, cand_count, rs, st);
+        launch_sun_candidates(S, s0, n, o, rs, st);
         // first stages of flat elements only (heliostat fields) take the flat-only variant
         const bool flat = S.stages[0].flat_only != 0;
         switch (variant * 2 + (flat ? 1 : 0)) {
-            case 1: resolve_one<0, 1>(S, s0, hit_elem, block_counts, cand, cand_count, rs, st); break;
-            case 2: resolve_one<1, 0>(S, s0, hit_elem, block_counts, cand, cand_count, rs, st); break;
-            case 3: resolve_one<1, 1>(S, s0, hit_elem, block_counts, cand, cand_count, rs, st); break;
-            case 4: resolve_one<2, 0>(S, s0, hit_elem, block_counts, cand, cand_count, rs, st); break;
-            case 5: resolve_one<2, 1>(S, s0, hit_elem, block_counts, cand, cand_count, rs, st); break;
-            default: resolve_one<0, 0>(S, s0, hit_elem, block_counts, cand, cand_count, rs, st);
+            case 1: resolve_one<0, 1>(S, s0, o, rs, st); break;
+            case 2: resolve_one<1, 0>(S, s0, o, rs, st); break;
+            case 3: resolve_one<1, 1>(S, s0, o, rs, st); break;
+            case 4: resolve_one<2, 0>(S, s0, o, rs, st); break;
+            case 5: resolve_one<2, 1>(S, s0, o, rs, st); break;
+            default: resolve_one<0, 0>(S, s0, o, rs, st);
         }
         return 2;
     }
-    k_probe<1><<<nb, kProbeBlock, 0, st>>>(S, s0, n, hit_elem, block_counts, rs);
+    k_probe<1><<<nb, kProbeBlock, 0, st>>>(S, s0, n, o, rs);
     return 1;
 }
 

@@ -19,6 +19,15 @@ constexpr int kProbeMinBlocks[kProbeVariants] = {4, 6, 8};
 // resident blocks per SM asked of the trace's shade and search kernels (register budget)
 constexpr int kWfShadeMinBlocks = 4;
 constexpr int kWfSearchMinBlocks = 4;
+// Search kinds: the trace's search kernel is compiled once per kind, holding only the code
+// its stages need (fewer registers, more resident warps).  Bits: kSearchFlat, the stage holds
+// flat elements only; kSearchBrute, the stage has neither ground grid nor BVH (few elements,
+// tested one after the other).
+constexpr int kSearchFlat = 1, kSearchBrute = 2, kSearchKinds = 4;
+__host__ __device__ inline int stage_search_kind(const StageRec &st) {
+    return (st.flat_only ? kSearchFlat : 0) | ((!st.grid_on && st.bvh_off < 0) ? kSearchBrute : 0);
+}
+constexpr int kWfBruteMinBlocks = 6;  // search kernels of stages tested element by element
 
 enum RunFlags : unsigned {
     kFlagHitCap = 1u,         // a ray reached kMaxHitsPerStage in one stage
@@ -43,6 +52,7 @@ struct RunState {
     unsigned long long sun_rays;   // SunRayCount so far (final once reached)
     unsigned int reached;
     unsigned int cursor;           // trace work queue: next hit-list entry to hand out
+    unsigned long long cut_sid;    // sun-ray index of the batch's last numbered hit (set by the sort)
 };
 
 // Per-ray state of the trace between its kernels, one slot per hit-list entry of a batch
@@ -57,14 +67,20 @@ struct WfState {
     uint32_t cap;
 };
 
-// Queues of the trace: two search queues used in turn, one shade queue, and the counts
-// of every round (count 2r: search queue of round r, 2r + 1: its shade queue); the
-// launcher zeroes the counts.
+// Queues of the trace.  Search queues come per search kind present in the scene (the
+// kernel variant that searches the rays' stages) and per round parity; one shade queue.
+// Queue k of parity p holds up to `cap` entries at search[p] + k * cap.  Counts, per
+// round r at r * (n_queues + 1): the n_queues search counts, then the shade count; the
+// finishing kernel takes the search counts of round `rounds`.  The launcher zeroes them.
 struct WfQueues {
     uint32_t *search[2];
     uint32_t *shade;
-    uint32_t *counts;  // 2 * rounds + 1 entries
+    uint32_t *counts;                     // (rounds + 1) * (n_queues + 1) entries
+    uint32_t cap;
     int rounds;
+    int n_queues;
+    int queue_kind[kMaxStages];           // search kind of queue k
+    unsigned char stage_queue[kMaxStages];  // search queue of the rays of stage s
 };
 
 struct TraceOut {
@@ -92,16 +108,30 @@ struct ReplayIn {
 };
 
 
-// First-stage probe of sun rays [s0, s0 + n): hit_elem[i] = element + 1 or 0, and the hit
-// count of every kProbeBlock rays.  `cand` (room for n entries) and `cand_count` are
-// scratch of the grid probe.  Returns the number of kernels launched.
-int launch_probe_fp64(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
-                      uint32_t *cand, uint32_t *cand_count, const RunState *rs, int variant, cudaStream_t st);
-int launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
-                       uint32_t *cand, uint32_t *cand_count, const RunState *rs, int variant, cudaStream_t st);
+// Outputs of the first-stage probe of sun rays [s0, s0 + n):
+//   block_counts  hits of every kProbeBlock rays (always written);
+//   hit_elem      optional: element + 1 or 0 per ray;
+//   cand, cand_count  the probe's ray list (room for n entries) and its length: the grid
+//                 probe's candidates, or (with cand_el) every ray of the other probes;
+//   cand_el       optional: element + 1 or 0 per list entry;
+//   hit_mask      optional: one bit per ray, set for a hit (hit_mask_words(n) words).
+struct ProbeOut {
+    uint32_t *block_counts;
+    uint32_t *hit_elem;
+    uint32_t *cand, *cand_count, *cand_el;
+    uint32_t *hit_mask;
+};
+constexpr size_t hit_mask_words(uint64_t n) { return size_t((n + kCandRays - 1) / kCandRays) * (kCandRays / 32); }
+
+// First-stage probe of sun rays [s0, s0 + n) into `o`.  Returns the number of kernels
+// launched.
+int launch_probe_fp64(const SceneDev &S, uint64_t s0, uint32_t n, const ProbeOut &o, const RunState *rs,
+                      int variant, cudaStream_t st);
+int launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, const ProbeOut &o, const RunState *rs,
+                       int variant, cudaStream_t st);
 // first kernel of the grid probe (shared by both precisions)
-void launch_sun_candidates(const SceneDev &S, uint64_t s0, uint32_t n, uint32_t *hit_elem, uint32_t *block_counts,
-                           uint32_t *cand, uint32_t *cand_count, const RunState *rs, cudaStream_t st);
+void launch_sun_candidates(const SceneDev &S, uint64_t s0, uint32_t n, const ProbeOut &o, const RunState *rs,
+                           cudaStream_t st);
 // Trace of a batch's numbered rays (hit-list entries below the cut-off at the requested
 // hit count): the first kernel, `Q.rounds` rounds of search and shade kernels, and the
 // finishing kernel.  Returns the number of kernels launched.
@@ -113,16 +143,22 @@ int launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, 
 int launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
                        const uint32_t *hit_idx, const uint32_t *total, const RunState *rs, const TraceOut &O,
                        const WfState &W, const WfQueues &Q, const ReplayIn *replay, cudaStream_t st);
-// counting sort of the batch's hits by first-stage element (n_elem0 buckets)
-void launch_sort_by_element(const uint32_t *total, const uint64_t *hit_sid, const uint32_t *hit_el, uint32_t n_elem0,
-                            uint32_t *elem_count, uint32_t *elem_cursor, uint32_t *scratch_total, uint64_t *s_sid,
-                            uint32_t *s_el, uint32_t *s_idx, uint32_t max_n, cudaStream_t st);
+// The batch's hits, from the probe's list (cand, cand_el, hit_mask) and the exclusive
+// scan of its block counts (offsets, total), counting-sorted by first-stage element into
+// s_sid (sun-ray index), s_el (element) and s_idx (rank of the hit in sun-ray order); the
+// hit ranked last below the cut-off at the requested hit count leaves its sun-ray index in
+// rs->cut_sid.  max_n bounds the list length (grid sizing).
+void launch_list_sort(uint64_t s0, const ProbeOut &o, const uint32_t *offsets, const uint32_t *total, RunState *rs,
+                      uint32_t n_elem0, uint32_t *elem_count, uint32_t *elem_cursor, uint32_t *scratch_total,
+                      uint64_t *s_sid, uint32_t *s_el, uint32_t *s_idx, uint32_t max_n, cudaStream_t st);
 // finite-element interpolation failures flagged by the kernels since the last call
 unsigned take_fe_failures_fp64();
 unsigned take_fe_failures_mixed();
 void launch_offsets(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_t *total, cudaStream_t st);
 void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uint32_t *counts,
                     const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st);
+// cut-off and run state after a batch; the last numbered sun ray is read from the
+// sun-ray-ordered hit list `hit_sid`, or from rs->cut_sid when it is null
 void launch_advance(const uint32_t *total, const uint64_t *hit_sid, uint64_t s0, uint32_t n, RunState *rs,
                     cudaStream_t st);
 }  // namespace stb

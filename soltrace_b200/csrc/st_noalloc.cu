@@ -161,7 +161,12 @@ extern "C" int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsig
         report(pcxt, std::string("st_b200_probe_noalloc: ") + cudaGetErrorString(e));
         return -1;
     }
-    launch_probe_fp64(S, s0, n, d_hit_elem, d_counts, d_cand + 1, d_cand, d_rs, 0, st);
+    ProbeOut po{};
+    po.block_counts = d_counts;
+    po.hit_elem = d_hit_elem;
+    po.cand = d_cand + 1;
+    po.cand_count = d_cand;
+    launch_probe_fp64(S, s0, n, po, d_rs, 0, st);
     launch_offsets(d_counts, nb, d_offsets, d_total, st);
     launch_compact(s0, n, d_hit_elem, d_counts, d_offsets, reinterpret_cast<uint64_t *>(hit_sid), hit_elem, st);
     uint32_t total = 0;

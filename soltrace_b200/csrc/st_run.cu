@@ -59,8 +59,10 @@ struct Workspace {
     DevBuf stage_cells, grid_sphere, grid_elem, beam_axis, beam_range, beam_elem;
     DevBuf elems, elem_sphere, optics, surf, tables, bvh, bvh_items, cell_start, cell_disc, cell_par, inv_cdf, expos,
         excos;
-    DevBuf acc, ctr, rs, rec_count, hit_elem, counts, offsets, total, hit_sid, hit_el, recs;
-    DevBuf cand;  // grid probe's candidate list: count, then one sun-ray index per entry
+    DevBuf acc, ctr, rs, rec_count, counts, offsets, total, recs;
+    DevBuf cand;      // probe's ray list: count, then one sun-ray index per entry
+    DevBuf cand_el;   // probe's result per list entry (element + 1, 0 for a miss)
+    DevBuf hit_mask;  // one bit per sun ray of the batch, set for a hit
     // trace state and queues (one slot per hit-list entry of a batch)
     DevBuf wf_sid, wf_raynum, wf_draw, wf_meta, wf_fe0, wf_p, wf_c, wf_q0, wf_q1, wf_qs, wf_counts;
     DevBuf save_rows[2], save_count, replay_rows, replay_fe0;  // stage-data save / replay
@@ -89,20 +91,34 @@ double ms_since(std::chrono::steady_clock::time_point t0) {
 
 }  // namespace
 
+// The probe outputs of a batch of n sun rays, in the workspace's buffers.
+static cudaError_t probe_buffers(Workspace &ws, uint64_t n, ProbeOut &o) {
+    const size_t nb = size_t((n + kProbeBlock - 1) / kProbeBlock);
+    cudaError_t e;
+    if ((e = ws.counts.ensure(nb * 4)) || (e = ws.cand.ensure((n + 1) * 4)) || (e = ws.cand_el.ensure(n * 4)) ||
+        (e = ws.hit_mask.ensure(hit_mask_words(n) * 4)))
+        return e;
+    o = ProbeOut{};
+    o.block_counts = ws.counts.as<uint32_t>();
+    o.cand_count = ws.cand.as<uint32_t>();
+    o.cand = o.cand_count + 1;
+    o.cand_el = ws.cand_el.as<uint32_t>();
+    o.hit_mask = ws.hit_mask.as<uint32_t>();
+    return cudaSuccess;
+}
+
 // Autotuner: time every register-budget variant of the probe on the same 2^21 sun rays
 // (indices 0.., outputs discarded into scratch buffers) and keep the fastest for this
 // workspace and precision.  Variants share their arithmetic, so the choice changes
 // timing only.
 static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, uint64_t max_sun, cudaStream_t st,
-                            DevBuf &hit_elem, DevBuf &counts, int &launches) {
+                            int &launches) {
     Workspace::Tuning &tu = ws.tune[precision ? 1 : 0];
     const uint64_t n = std::min<uint64_t>(uint64_t(1) << 21, max_sun);
     if (n == 0) return cudaSuccess;
-    const uint32_t nb = uint32_t((n + kProbeBlock - 1) / kProbeBlock);
     cudaError_t e;
-    if ((e = hit_elem.ensure(n * 4)) || (e = counts.ensure(size_t(nb) * 4)) ||
-        (e = ws.tune_rs.ensure(sizeof(RunState))) || (e = ws.cand.ensure((n + 1) * 4)))
-        return e;
+    ProbeOut po;
+    if ((e = probe_buffers(ws, n, po)) || (e = ws.tune_rs.ensure(sizeof(RunState)))) return e;
     SceneDev S = S0;
     S.n_flux = 0;
     RunState r0;
@@ -112,14 +128,11 @@ static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, ui
     cudaMemcpyAsync(rs, &r0, sizeof r0, cudaMemcpyHostToDevice, st);
     cudaEvent_t ev[2 * kProbeVariants];
     for (auto &x : ev) cudaEventCreate(&x);
-    uint32_t *cand_count = ws.cand.as<uint32_t>(), *cand = cand_count + 1;
     auto probe = [&](int v) {
         if (precision)
-            launches += launch_probe_mixed(S, 0, uint32_t(n), hit_elem.as<uint32_t>(), counts.as<uint32_t>(), cand,
-                                           cand_count, rs, v, st);
+            launches += launch_probe_mixed(S, 0, uint32_t(n), po, rs, v, st);
         else
-            launches += launch_probe_fp64(S, 0, uint32_t(n), hit_elem.as<uint32_t>(), counts.as<uint32_t>(), cand,
-                                          cand_count, rs, v, st);
+            launches += launch_probe_fp64(S, 0, uint32_t(n), po, rs, v, st);
     };
     probe(0);  // warm the caches
     for (int v = 0; v < kProbeVariants; ++v) {
@@ -145,17 +158,31 @@ static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, ui
     return e;
 }
 
-// trace state and queues for up to `cap` rays
-static cudaError_t wf_buffers(Workspace &ws, uint64_t cap, int nst, WfState &W, WfQueues &Q) {
+// trace state and queues for up to `cap` rays: one search queue per search kind among the
+// stages (and round parity)
+static cudaError_t wf_buffers(Workspace &ws, const SceneDev &S, uint64_t cap, WfState &W, WfQueues &Q) {
     cudaError_t e;
     cap = std::max<uint64_t>(cap, 1);
+    const int nst = S.n_stages;
+    Q = WfQueues{};
+    int queue_of_kind[kSearchKinds] = {-1, -1, -1, -1};
+    for (int s = 0; s < nst; ++s) {
+        const int k = stage_search_kind(S.stages[s]);
+        if (queue_of_kind[k] < 0) {
+            queue_of_kind[k] = Q.n_queues;
+            Q.queue_kind[Q.n_queues++] = k;
+        }
+        Q.stage_queue[s] = (unsigned char)queue_of_kind[k];
+    }
+    const uint64_t nq = uint64_t(std::max(Q.n_queues, 1));
     if ((e = ws.wf_sid.ensure(cap * 8)) || (e = ws.wf_raynum.ensure(cap * 4)) || (e = ws.wf_draw.ensure(cap * 4)) ||
         (e = ws.wf_meta.ensure(cap * 16)) || (e = ws.wf_fe0.ensure(cap * 4)) || (e = ws.wf_p.ensure(cap * 24)) ||
-        (e = ws.wf_c.ensure(cap * 24)) || (e = ws.wf_q0.ensure(cap * 4)) || (e = ws.wf_q1.ensure(cap * 4)) ||
-        (e = ws.wf_qs.ensure(cap * 4)))
+        (e = ws.wf_c.ensure(cap * 24)) || (e = ws.wf_q0.ensure(nq * cap * 4)) ||
+        (e = ws.wf_q1.ensure(nq * cap * 4)) || (e = ws.wf_qs.ensure(cap * 4)))
         return e;
     Q.rounds = 2 * nst;
-    if ((e = ws.wf_counts.ensure(sizeof(uint32_t) * (2 * Q.rounds + 1)))) return e;
+    Q.cap = uint32_t(cap);
+    if ((e = ws.wf_counts.ensure(sizeof(uint32_t) * (Q.rounds + 1) * (nq + 1)))) return e;
     Q.search[0] = ws.wf_q0.as<uint32_t>();
     Q.search[1] = ws.wf_q1.as<uint32_t>();
     Q.shade = ws.wf_qs.as<uint32_t>();
@@ -265,23 +292,19 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
 
     const int nst = S.n_stages;
     const uint64_t kMaxBatch = uint64_t(1) << 25;
-    DevBuf &d_acc = ws.acc, &d_ctr = ws.ctr, &d_rs = ws.rs, &d_rec_count = ws.rec_count, &d_hit_elem = ws.hit_elem,
-           &d_counts = ws.counts, &d_offsets = ws.offsets, &d_total = ws.total, &d_hit_sid = ws.hit_sid,
-           &d_hit_el = ws.hit_el, &d_recs = ws.recs;
-    // rays are regrouped by first-stage element when that stage is large enough to
-    // have a BVH (their blocking tests then walk the same nodes in a warp)
+    DevBuf &d_acc = ws.acc, &d_ctr = ws.ctr, &d_rs = ws.rs, &d_rec_count = ws.rec_count, &d_offsets = ws.offsets,
+           &d_total = ws.total, &d_recs = ws.recs;
+    // the batch's hits are grouped by first-stage element (the rays of a warp then leave
+    // one element and walk the same candidates)
     const uint32_t n_elem0 = uint32_t(S.stages[0].n_elem);
-    const bool sort_hits = S.stages[0].bvh_off >= 0 && n_elem0 > 1;
     DevBuf &d_ecount = ws.ecount, &d_ecursor = ws.ecursor, &d_etotal = ws.etotal, &d_s_sid = ws.s_sid,
            &d_s_el = ws.s_el, &d_s_idx = ws.s_idx;
-    if (sort_hits) {
-        CK(d_ecount.ensure(size_t(n_elem0) * 4));
-        CK(d_ecursor.ensure(size_t(n_elem0) * 4));
-        CK(d_etotal.ensure(8));
-    }
+    CK(d_ecount.ensure(size_t(n_elem0) * 4));
+    CK(d_ecursor.ensure(size_t(n_elem0) * 4));
+    CK(d_etotal.ensure(8));
     unsigned long long rec_cap = 0, save_cap = 0;
     Workspace::Tuning &tu = ws.tune[rq.precision ? 1 : 0];
-    if (!tu.done && !explicit_mode && !rq.replay) CK(autotune(ws, S, rq.precision, rq.max_sun, st, d_hit_elem, d_counts, out.gpu_launches));
+    if (!tu.done && !explicit_mode && !rq.replay) CK(autotune(ws, S, rq.precision, rq.max_sun, st, out.gpu_launches));
     out.probe_variant = tu.probe;
     out.trace_variant = 0;
     (void)dev_sms;
@@ -409,7 +432,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             O.rec_cap = rq.records ? rec_cap : 0;
             WfState W;
             WfQueues Q;
-            CK(wf_buffers(ws, n1, nst, W, Q));
+            CK(wf_buffers(ws, S, n1, W, Q));
             CK(save_setup(n1));
             ReplayIn rin;
             rin.rows = ws.replay_rows.as<double>();
@@ -471,17 +494,13 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             while (queued < want) {
                 const uint64_t n = std::min<uint64_t>(kMaxBatch, want - queued);
                 const uint32_t nb = uint32_t((n + kProbeBlock - 1) / kProbeBlock);
-                CK(d_hit_elem.ensure(n * 4));
-                CK(d_counts.ensure(size_t(nb) * 4));
+                ProbeOut po;
+                CK(probe_buffers(ws, n, po));
                 CK(d_offsets.ensure(size_t(nb) * 4));
                 CK(d_total.ensure(8));
-                CK(d_hit_sid.ensure(n * 8));
-                CK(d_hit_el.ensure(n * 4));
-                if (sort_hits) {
-                    CK(d_s_sid.ensure(n * 8));
-                    CK(d_s_el.ensure(n * 4));
-                    CK(d_s_idx.ensure(n * 4));
-                }
+                CK(d_s_sid.ensure(n * 8));
+                CK(d_s_el.ensure(n * 4));
+                CK(d_s_idx.ensure(n * 4));
                 if (rq.records) {
                     if (rec_cap == 0) rec_cap = std::min<uint64_t>(n, uint64_t(1) << 22) * uint64_t(nst) * 2 + 4096;
                     CK(d_recs.ensure(rec_cap * sizeof(RecordDev)));
@@ -491,33 +510,21 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 O.rec_cap = rq.records ? rec_cap : 0;
                 cudaEvent_t p0 = new_event(), p1 = new_event(), p2 = new_event();
                 CK(cudaEventRecord(p0, st));
-                CK(ws.cand.ensure((n + 1) * 4));
-                uint32_t *cand_count = ws.cand.as<uint32_t>(), *cand = cand_count + 1;
                 if (rq.precision)
-                    out.gpu_launches += launch_probe_mixed(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(),
-                                                           d_counts.as<uint32_t>(), cand, cand_count, drs, tu.probe, st);
+                    out.gpu_launches += launch_probe_mixed(S, sun_next, uint32_t(n), po, drs, tu.probe, st);
                 else
-                    out.gpu_launches += launch_probe_fp64(S, sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(),
-                                                          d_counts.as<uint32_t>(), cand, cand_count, drs, tu.probe, st);
-                launch_offsets(d_counts.as<uint32_t>(), nb, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), st);
-                launch_compact(sun_next, uint32_t(n), d_hit_elem.as<uint32_t>(), d_counts.as<uint32_t>(),
-                               d_offsets.as<uint32_t>(), d_hit_sid.as<uint64_t>(), d_hit_el.as<uint32_t>(), st);
-                const uint64_t *t_sid = d_hit_sid.as<uint64_t>();
-                const uint32_t *t_el = d_hit_el.as<uint32_t>(), *t_idx = nullptr;
-                if (sort_hits) {
-                    launch_sort_by_element(d_total.as<uint32_t>(), d_hit_sid.as<uint64_t>(), d_hit_el.as<uint32_t>(),
-                                           n_elem0, d_ecount.as<uint32_t>(), d_ecursor.as<uint32_t>(),
-                                           d_etotal.as<uint32_t>(), d_s_sid.as<uint64_t>(), d_s_el.as<uint32_t>(),
-                                           d_s_idx.as<uint32_t>(), uint32_t(n), st);
-                    out.gpu_launches += 3;
-                    t_sid = d_s_sid.as<uint64_t>();
-                    t_el = d_s_el.as<uint32_t>();
-                    t_idx = d_s_idx.as<uint32_t>();
-                }
+                    out.gpu_launches += launch_probe_fp64(S, sun_next, uint32_t(n), po, drs, tu.probe, st);
+                launch_offsets(po.block_counts, nb, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), st);
+                launch_list_sort(sun_next, po, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), drs, n_elem0,
+                                 d_ecount.as<uint32_t>(), d_ecursor.as<uint32_t>(), d_etotal.as<uint32_t>(),
+                                 d_s_sid.as<uint64_t>(), d_s_el.as<uint32_t>(), d_s_idx.as<uint32_t>(), uint32_t(n), st);
+                out.gpu_launches += 3;  // element counts, their scan, scatter
+                const uint64_t *t_sid = d_s_sid.as<uint64_t>();
+                const uint32_t *t_el = d_s_el.as<uint32_t>(), *t_idx = d_s_idx.as<uint32_t>();
                 // trace state and queues: one slot per hit-list entry (at most n)
                 WfState W;
                 WfQueues Q;
-                CK(wf_buffers(ws, n, nst, W, Q));
+                CK(wf_buffers(ws, S, n, W, Q));
                 CK(save_setup(n));
                 CK(cudaEventRecord(p1, st));
                 if (rq.precision)
@@ -527,9 +534,9 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                     out.gpu_launches += launch_trace_fp64(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(),
                                                           drs, O, W, Q, nullptr, st);
                 CK(cudaEventRecord(p2, st));
-                launch_advance(d_total.as<uint32_t>(), d_hit_sid.as<uint64_t>(), sun_next, uint32_t(n), drs, st);
+                launch_advance(d_total.as<uint32_t>(), nullptr, sun_next, uint32_t(n), drs, st);
                 CK(cudaGetLastError());
-                out.gpu_launches += 3;  // offsets, compact, advance
+                out.gpu_launches += 2;  // offsets, advance
                 probe_ev.push_back({p0, p1});
                 trace_ev.push_back({p1, p2});
                 queued += n;

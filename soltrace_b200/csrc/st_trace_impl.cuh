@@ -59,7 +59,14 @@ __device__ __forceinline__ void make_ray(const SceneDev &S, uint64_t sid, RayRng
 // ------------------------------------------------------------------------------------
 // nearest accepted hit in a stage (raytrace.cpp:698-770); -1 if none
 // ------------------------------------------------------------------------------------
-template <int MIXED>
+// element_test without the full hit; FLAT: the element is known to be flat
+template <int MIXED, int FLAT>
+__device__ __forceinline__ bool elem_hit(const SceneDev &S, const ElemRec &e, const double ps[3], const double cs[3],
+                                         double &pl) {
+    return FLAT ? element_test_flat<MIXED>(e, ps, cs, pl) : element_test<MIXED>(S, e, ps, cs, pl, nullptr);
+}
+
+template <int MIXED, int FLAT = 0>
 __device__ inline int nearest_brute(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3]) {
     int best = -1;
     double bp = 1e99;
@@ -67,7 +74,7 @@ __device__ inline int nearest_brute(const SceneDev &S, const StageRec &st, const
         const ElemRec &e = S.elems[st.first_elem + j];
         if (!e.enabled) continue;
         double pl;
-        if (element_test<MIXED>(S, e, ps, cs, pl, nullptr) && pl < bp) {
+        if (elem_hit<MIXED, FLAT>(S, e, ps, cs, pl) && pl < bp) {
             bp = pl;
             best = j;
         }
@@ -78,7 +85,7 @@ __device__ inline int nearest_brute(const SceneDev &S, const StageRec &st, const
 // BVH over element bounding spheres; nodes farther than the best hit so far are
 // skipped (the test is on the entry distance minus the 1e-5 nudge, with slack for
 // the float box arithmetic).
-template <int MIXED>
+template <int MIXED, int FLAT = 0>
 __device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3],
                                   int from) {
     const BvhNode *nodes = S.bvh + st.bvh_off;
@@ -121,7 +128,7 @@ __device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const d
                 const ElemRec &e = S.elems[st.first_elem + j];
                 if (!e.enabled) continue;
                 double pl;
-                if (element_test<MIXED>(S, e, ps, cs, pl, nullptr) && (pl < bp || (pl == bp && j < best))) {
+                if (elem_hit<MIXED, FLAT>(S, e, ps, cs, pl) && (pl < bp || (pl == bp && j < best))) {
                     bp = pl;
                     best = j;
                 }
@@ -144,7 +151,7 @@ __device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const d
 // from is listed in a visited cell (the padded discs absorb the float rounding of the
 // walk), and the choice among hits is the serial search's (shortest path, lower index on
 // ties), so the result is the brute-force search's.
-template <int MIXED>
+template <int MIXED, int FLAT = 0>
 __device__ inline int nearest_grid(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3],
                                    int from) {
     const float ox = float(ps[0]), oy = float(ps[1]), oz = float(ps[2]);
@@ -200,7 +207,7 @@ __device__ inline int nearest_grid(const SceneDev &S, const StageRec &st, const 
         for (int c = 0; c < nc; ++c) {
             const int j = cand[256 * c];
             double pl;
-            if (element_test<MIXED>(S, S.elems[st.first_elem + j], ps, cs, pl, nullptr) &&
+            if (elem_hit<MIXED, FLAT>(S, S.elems[st.first_elem + j], ps, cs, pl) &&
                 (pl < bp || (pl == bp && j < best))) {
                 bp = pl;
                 best = j;
@@ -257,6 +264,16 @@ __device__ __forceinline__ int nearest(const SceneDev &S, const StageRec &st, co
     return (st.bvh_off >= 0) ? nearest_bvh<MIXED>(S, st, ps, cs, from) : nearest_brute<MIXED>(S, st, ps, cs);
 }
 
+// nearest element with the code of search kind KIND only (stage_search_kind, st_launch.h)
+template <int MIXED, int KIND>
+__device__ __forceinline__ int nearest_kind(const SceneDev &S, const StageRec &st, const double ps[3],
+                                            const double cs[3], int from) {
+    constexpr int F = (KIND & kSearchFlat) ? 1 : 0;
+    if (KIND & kSearchBrute) return nearest_brute<MIXED, F>(S, st, ps, cs);
+    if (st.grid_on) return nearest_grid<MIXED, F>(S, st, ps, cs, from);
+    return (st.bvh_off >= 0) ? nearest_bvh<MIXED, F>(S, st, ps, cs, from) : nearest_brute<MIXED, F>(S, st, ps, cs);
+}
+
 // first test of a first-stage sun ray through the sun-plane grid (cells list the
 // elements, ascending, whose bounding disc in the sun plane overlaps the cell)
 // The first-stage ray of sun-frame point (xs, ys), as the reference builds it: sun frame ->
@@ -311,8 +328,7 @@ __device__ inline int nearest_sun_grid_lazy(const SceneDev &S, const StageRec &s
             have_ray = true;
         }
         double pl;
-        const bool hit = FLAT ? element_test_flat<MIXED>(e, ps, cs, pl) : element_test<MIXED>(S, e, ps, cs, pl, nullptr);
-        if (hit && pl < bp) {
+        if (elem_hit<MIXED, FLAT>(S, e, ps, cs, pl) && pl < bp) {
             bp = pl;
             best = j;
         }
@@ -516,12 +532,14 @@ __device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed
 // kernels
 // ------------------------------------------------------------------------------------
 template <int MIXED>
-__global__ void __launch_bounds__(kProbeBlock) k_probe(const __grid_constant__ SceneDev S, uint64_t s0, uint32_t n, uint32_t *hit_elem,
-                                                        uint32_t *block_counts, const RunState *rs) {
+__global__ void __launch_bounds__(kProbeBlock) k_probe(const __grid_constant__ SceneDev S, uint64_t s0, uint32_t n,
+                                                        ProbeOut o, const RunState *rs) {
     const uint32_t i = blockIdx.x * kProbeBlock + threadIdx.x;
+    const bool reached = rs->reached != 0;
+    if (o.cand_count && blockIdx.x == 0 && threadIdx.x == 0) *o.cand_count = reached ? 0u : n;
     uint32_t h = 0;
-    if (rs->reached) {  // the requested hits are numbered: this batch is surplus
-        if (threadIdx.x == 0) block_counts[blockIdx.x] = 0;
+    if (reached) {  // the requested hits are numbered: this batch is surplus
+        if (threadIdx.x == 0) o.block_counts[blockIdx.x] = 0;
         return;
     }
     if (i < n) {
@@ -536,57 +554,69 @@ __global__ void __launch_bounds__(kProbeBlock) k_probe(const __grid_constant__ S
         (void)ys;
         const int b = nearest<MIXED>(S, st, ps, cs);
         h = (b >= 0) ? uint32_t(b + 1) : 0u;
-        hit_elem[i] = h;
+        if (o.hit_elem) o.hit_elem[i] = h;
+        if (o.cand_el) {  // the list is every ray of the batch
+            o.cand[i] = i;
+            o.cand_el[i] = h;
+        }
     }
+    const unsigned bal = __ballot_sync(0xffffffffu, h != 0);
+    if (o.hit_mask && (threadIdx.x & 31) == 0) o.hit_mask[i / 32] = bal;
     const int c = __syncthreads_count(h != 0);
-    if (threadIdx.x == 0) block_counts[blockIdx.x] = uint32_t(c);
+    if (threadIdx.x == 0) o.block_counts[blockIdx.x] = uint32_t(c);
 }
 
 // Probe of generated sun rays on a first stage culled by the sun-plane grid, in two
 // kernels so that the double-precision work runs in full warps:
-//   k_sun_candidates (one thread per sun ray, few registers): draws the sun-plane point
-//     and runs the float pre-tests of its grid cell; a ray with no passing entry is a miss
-//     (its hit_elem is written here), the others are appended to a candidate list;
+//   k_sun_candidates (four sun rays per thread, few registers): draws the sun-plane point
+//     and runs the float pre-tests of its grid cell; a ray with no passing entry is a miss,
+//     the others are appended to a candidate list;
 //   k_sun_resolve (one thread per listed ray): redraws the point and runs the serial
-//     nearest-element search of the reference's loop over the first stage, writing
-//     hit_elem and the per-kProbeBlock hit counts.
+//     nearest-element search of the reference's loop over the first stage, writing the
+//     result per list entry (and per ray, when asked), the ray's bit of the hit mask and
+//     the per-kProbeBlock hit counts.
 // On a heliostat field most sun rays miss every footprint and never reach the second
 // kernel, whose warps are then fully occupied by rays that need the element tests.
 template <int MIXED, int MINB, int FLAT>
-__global__ void __launch_bounds__(kResolveBlock, MINB) k_sun_resolve(const __grid_constant__ SceneDev S, uint64_t s0, uint32_t *hit_elem,
-                                                                     uint32_t *block_counts, const uint32_t *cand,
-                                                                     const uint32_t *cand_count, const RunState *rs) {
+__global__ void __launch_bounds__(kResolveBlock, MINB) k_sun_resolve(const __grid_constant__ SceneDev S, uint64_t s0,
+                                                                     ProbeOut o, const RunState *rs) {
     if (rs->reached) return;
-    const uint32_t nc = *cand_count;
+    const uint32_t nc = *o.cand_count;
     const SunDev &sun = S.sun;
     for (uint32_t c = blockIdx.x * kResolveBlock + threadIdx.x; c < nc; c += gridDim.x * kResolveBlock) {
-        const uint32_t i = cand[c];
+        const uint32_t i = o.cand[c];
         RayRng rng;
         rng.init(S.seed, s0 + i, 0);
         const double xs = sun.xmin + (sun.xmax - sun.xmin) * rng.u();
         const double ys = sun.ymin + (sun.ymax - sun.ymin) * rng.u();
         const int b = nearest_sun_grid_lazy<MIXED, FLAT>(S, S.stages[0], xs, ys);
-        hit_elem[i] = (b >= 0) ? uint32_t(b + 1) : 0u;
+        const uint32_t h = (b >= 0) ? uint32_t(b + 1) : 0u;
+        if (o.hit_elem) o.hit_elem[i] = h;
+        if (o.cand_el) o.cand_el[c] = h;
         if (b >= 0) {
-            // one atomic per distinct count slot among the warp's hitting lanes
+            // one atomic per distinct count slot (and mask word) among the warp's hitting lanes
             const unsigned mask = __activemask();
             const uint32_t slot = i / kProbeBlock;
             const unsigned peers = __match_any_sync(mask, slot);
-            if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&block_counts[slot], uint32_t(__popc(peers)));
+            if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&o.block_counts[slot], uint32_t(__popc(peers)));
+            if (o.hit_mask) {
+                const unsigned wp = __match_any_sync(mask, i / 32);
+                const unsigned bits = __reduce_or_sync(wp, 1u << (i & 31));
+                if ((threadIdx.x & 31) == __ffs(wp) - 1) atomicOr(&o.hit_mask[i / 32], bits);
+            }
         }
     }
 }
 
 #ifdef ST_COMMON_KERNELS
-// first kernel of the grid probe (above): misses written, candidates listed
-__global__ void __launch_bounds__(kProbeBlock) k_sun_candidates(const __grid_constant__ SceneDev S, uint64_t s0, uint32_t n,
-                                                                uint32_t *hit_elem, uint32_t *block_counts,
-                                                                uint32_t *cand, uint32_t *cand_count,
-                                                                const RunState *rs) {
+// first kernel of the grid probe (above): candidates listed, hit-mask words cleared
+__global__ void __launch_bounds__(kProbeBlock) k_sun_candidates(const __grid_constant__ SceneDev S, uint64_t s0,
+                                                                uint32_t n, ProbeOut o, const RunState *rs) {
     // a block takes kCandRays sun rays (kCandRays / kProbeBlock per thread, kProbeBlock apart)
     const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;
     if (threadIdx.x < kCandPerThread && blockIdx.x * kCandPerThread + threadIdx.x < nb)
-        block_counts[blockIdx.x * kCandPerThread + threadIdx.x] = 0;
+        o.block_counts[blockIdx.x * kCandPerThread + threadIdx.x] = 0;
+    if (o.hit_mask && threadIdx.x < kCandRays / 32) o.hit_mask[blockIdx.x * (kCandRays / 32) + threadIdx.x] = 0;
     if (rs->reached) return;  // the requested hits are numbered: this batch is surplus
     const SunDev &sun = S.sun;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -607,7 +637,7 @@ __global__ void __launch_bounds__(kProbeBlock) k_sun_candidates(const __grid_con
                     listed = true;
                     break;
                 }
-            if (!listed) hit_elem[i] = 0;
+            if (!listed && o.hit_elem) o.hit_elem[i] = 0;
         }
         bal[m] = __ballot_sync(0xffffffffu, listed);
         mine += __popc(bal[m]);
@@ -623,29 +653,36 @@ __global__ void __launch_bounds__(kProbeBlock) k_sun_candidates(const __grid_con
             wn[k] = t;
             t += x;
         }
-        base = t ? atomicAdd(cand_count, t) : 0u;
+        base = t ? atomicAdd(o.cand_count, t) : 0u;
     }
     __syncthreads();
     uint32_t at = base + wn[w];
     const unsigned lt = (1u << lane) - 1u;
     for (int m = 0; m < kCandPerThread; ++m) {
-        if ((bal[m] >> lane) & 1u) cand[at + __popc(bal[m] & lt)] = blockIdx.x * kCandRays + m * kProbeBlock + threadIdx.x;
+        if ((bal[m] >> lane) & 1u) o.cand[at + __popc(bal[m] & lt)] = blockIdx.x * kCandRays + m * kProbeBlock + threadIdx.x;
         at += __popc(bal[m]);
     }
 }
 
-// exclusive scan of the per-block counts (one block; counts fit in 32 bits per batch)
+// exclusive scan of the per-block counts (one block; counts fit in 32 bits per batch):
+// each thread scans 8 consecutive counts, the block scans the threads' sums
 __global__ void __launch_bounds__(1024) k_offsets(const uint32_t *counts, uint32_t nb, uint32_t *offsets,
                                                    uint32_t *total) {
+    constexpr int kPer = 8;
     __shared__ uint32_t warp_sums[32];
     __shared__ uint32_t carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    for (uint32_t base = 0; base < nb; base += 1024) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t v = (i < nb) ? counts[i] : 0u;
-        uint32_t x = v;
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (uint32_t base = 0; base < nb; base += 1024 * kPer) {
+        const uint32_t i0 = base + threadIdx.x * kPer;
+        uint32_t v[kPer], sum = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            v[k] = (i0 + k < nb) ? counts[i0 + k] : 0u;
+            sum += v[k];
+        }
+        uint32_t x = sum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -664,7 +701,12 @@ __global__ void __launch_bounds__(1024) k_offsets(const uint32_t *counts, uint32
         }
         __syncthreads();
         const uint32_t incl = x + (w > 0 ? warp_sums[w - 1] : 0u) + carry;
-        if (i < nb) offsets[i] = incl - v;
+        uint32_t run = incl - sum;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+            if (i0 + k < nb) offsets[i0 + k] = run;
+            run += v[k];
+        }
         __syncthreads();
         if (threadIdx.x == 1023) carry = incl;
         __syncthreads();
@@ -693,68 +735,117 @@ __global__ void __launch_bounds__(kProbeBlock) k_compact(uint64_t s0, uint32_t n
 }
 
 // Counting sort of a batch's hits by first-stage element, so that each warp of the
-// trace kernel carries rays leaving the same element (coherent traversals).  Order
-// within an element is arbitrary: every result is independent of it (per-ray
-// random streams, integer flux atomics, records ordered by ray number).
-__global__ void __launch_bounds__(256) k_elem_hist(const uint32_t *total, const uint32_t *hit_el, uint32_t *elem_count) {
-    const uint32_t n = *total;
-    for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) atomicAdd(&elem_count[hit_el[i]], 1u);
+// trace kernel carries rays leaving the same element (coherent traversals).  The input is
+// the probe's list (ray, element + 1 or 0 per entry) in any order; the rank of a hit in
+// sun-ray order (its ray number) comes from the scanned per-block counts and the hit mask.
+// Order within an element is arbitrary: every result is independent of it (per-ray random
+// streams, integer flux atomics, records ordered by ray number).
+
+// rank of the hit on ray i among the batch's hits in ray order: the hits of the kProbeBlock
+// rays before its block, then those of the block's mask words before its own
+__device__ __forceinline__ uint32_t hit_rank(const uint32_t *offsets, const uint32_t *mask, uint32_t i) {
+    static_assert(kProbeBlock == 256, "eight mask words per count slot");
+    const uint32_t blk = i / kProbeBlock, w = (i / 32) % 8;
+    const uint4 *m4 = reinterpret_cast<const uint4 *>(mask + size_t(blk) * 8);
+    const uint4 a = m4[0], b = m4[1];
+    const uint32_t words[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+    uint32_t r = offsets[blk];
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k) {
+        if (k < w) r += __popc(words[k]);
+        if (k == w) r += __popc(words[k] & ((1u << (i & 31)) - 1u));
+    }
+    return r;
 }
-__global__ void __launch_bounds__(256) k_elem_scatter(const uint32_t *total, const uint64_t *hit_sid, const uint32_t *hit_el,
-                                                      uint32_t *elem_cursor, uint64_t *s_sid, uint32_t *s_el,
-                                                      uint32_t *s_idx) {
+
+// hits the trace numbers in this batch (the cut-off at the requested hit count)
+__device__ __forceinline__ uint32_t batch_take(const RunState *rs, const uint32_t *total) {
+    if (rs->reached) return 0u;
+    const unsigned long long left = rs->target - rs->hits_done;
     const uint32_t n = *total;
+    return uint32_t(n < left ? n : left);
+}
+
+// one sorted hit: sun-ray index, element, rank; the last numbered one marks the cut-off
+__device__ __forceinline__ void list_put(uint64_t s0, uint32_t ray, uint32_t e, uint32_t pos, const uint32_t *offsets,
+                                         const uint32_t *mask, uint32_t take, RunState *rs, uint64_t *s_sid,
+                                         uint32_t *s_el, uint32_t *s_idx) {
+    const uint32_t rank = hit_rank(offsets, mask, ray);
+    s_sid[pos] = s0 + ray;
+    s_el[pos] = e;
+    s_idx[pos] = rank;
+    if (rank + 1 == take) rs->cut_sid = s0 + ray;
+}
+
+__global__ void __launch_bounds__(256) k_list_hist(const uint32_t *list_count, const uint32_t *cand_el,
+                                                   uint32_t *elem_count) {
+    const uint32_t n = *list_count;
     for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
-        const uint32_t e = hit_el[i];
-        const uint32_t pos = atomicAdd(&elem_cursor[e], 1u);
-        s_sid[pos] = hit_sid[i];
-        s_el[pos] = e;
-        s_idx[pos] = i;
+        const uint32_t h = cand_el[i];
+        if (h) atomicAdd(&elem_count[h - 1], 1u);
+    }
+}
+__global__ void __launch_bounds__(256) k_list_scatter(uint64_t s0, ProbeOut o, const uint32_t *offsets,
+                                                      const uint32_t *total, RunState *rs, uint32_t *elem_cursor,
+                                                      uint64_t *s_sid, uint32_t *s_el, uint32_t *s_idx) {
+    const uint32_t n = *o.cand_count;
+    const uint32_t take = batch_take(rs, total);
+    for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
+        const uint32_t h = o.cand_el[i];
+        if (!h) continue;
+        const uint32_t pos = atomicAdd(&elem_cursor[h - 1], 1u);
+        list_put(s0, o.cand[i], h - 1, pos, offsets, o.hit_mask, take, rs, s_sid, s_el, s_idx);
     }
 }
 
 // The same counting sort for first stages of at most kSortBins elements, with the counts
-// kept per block in shared memory: each block takes a contiguous chunk of the hit list,
+// kept per block in shared memory: each block takes a contiguous chunk of the list,
 // counts its elements there and adds its non-zero counts to the global ones (hist), or
 // reserves one range per element in the output with a single global atomic and hands out
 // the places in it from shared memory (scatter).  Global atomics: one per block and
 // element present, instead of one per hit.
 constexpr int kSortBins = 11264;
 constexpr int kSortBlock = 1024;
-__global__ void __launch_bounds__(kSortBlock) k_elem_hist_sh(const uint32_t *total, const uint32_t *hit_el,
+__global__ void __launch_bounds__(kSortBlock) k_list_hist_sh(const uint32_t *list_count, const uint32_t *cand_el,
                                                              uint32_t n_elem, uint32_t *elem_count) {
     __shared__ uint32_t h[kSortBins];
-    const uint32_t n = *total;
+    const uint32_t n = *list_count;
     const uint32_t chunk = (n + gridDim.x - 1) / gridDim.x;
     const uint32_t a = min(n, blockIdx.x * chunk), b = min(n, a + chunk);
     for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock) h[e] = 0;
     __syncthreads();
-    for (uint32_t i = a + threadIdx.x; i < b; i += kSortBlock) atomicAdd(&h[hit_el[i]], 1u);
+    for (uint32_t i = a + threadIdx.x; i < b; i += kSortBlock) {
+        const uint32_t x = cand_el[i];
+        if (x) atomicAdd(&h[x - 1], 1u);
+    }
     __syncthreads();
     for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock)
         if (h[e]) atomicAdd(&elem_count[e], h[e]);
 }
-__global__ void __launch_bounds__(kSortBlock) k_elem_scatter_sh(const uint32_t *total, const uint64_t *hit_sid,
-                                                                const uint32_t *hit_el, uint32_t n_elem,
+__global__ void __launch_bounds__(kSortBlock) k_list_scatter_sh(uint64_t s0, ProbeOut o, const uint32_t *offsets,
+                                                                const uint32_t *total, RunState *rs, uint32_t n_elem,
                                                                 uint32_t *elem_cursor, uint64_t *s_sid, uint32_t *s_el,
                                                                 uint32_t *s_idx) {
     __shared__ uint32_t h[kSortBins];
-    const uint32_t n = *total;
+    const uint32_t n = *o.cand_count;
+    const uint32_t take = batch_take(rs, total);
     const uint32_t chunk = (n + gridDim.x - 1) / gridDim.x;
     const uint32_t a = min(n, blockIdx.x * chunk), b = min(n, a + chunk);
     for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock) h[e] = 0;
     __syncthreads();
-    for (uint32_t i = a + threadIdx.x; i < b; i += kSortBlock) atomicAdd(&h[hit_el[i]], 1u);
+    for (uint32_t i = a + threadIdx.x; i < b; i += kSortBlock) {
+        const uint32_t x = o.cand_el[i];
+        if (x) atomicAdd(&h[x - 1], 1u);
+    }
     __syncthreads();
     for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock)
         if (h[e]) h[e] = atomicAdd(&elem_cursor[e], h[e]);
     __syncthreads();
     for (uint32_t i = a + threadIdx.x; i < b; i += kSortBlock) {
-        const uint32_t e = hit_el[i];
-        const uint32_t pos = atomicAdd(&h[e], 1u);
-        s_sid[pos] = hit_sid[i];
-        s_el[pos] = e;
-        s_idx[pos] = i;
+        const uint32_t x = o.cand_el[i];
+        if (!x) continue;
+        const uint32_t pos = atomicAdd(&h[x - 1], 1u);
+        list_put(s0, o.cand[i], x - 1, pos, offsets, o.hit_mask, take, rs, s_sid, s_el, s_idx);
     }
 }
 
@@ -767,7 +858,7 @@ __global__ void k_advance(const uint32_t *total, const uint64_t *hit_sid, uint64
     rs->hits_done += take;
     if (rs->hits_done == rs->target && take > 0) {
         rs->reached = 1;
-        rs->sun_rays = hit_sid[take - 1] + 1;
+        rs->sun_rays = (hit_sid ? hit_sid[take - 1] : rs->cut_sid) + 1;
     } else {
         rs->sun_rays = s0 + n;
     }
@@ -873,38 +964,48 @@ __device__ __forceinline__ void wf_store(const WfState &W, uint32_t i, const WfR
         }
 }
 
-// Append `slot` to queue A for every thread with `want_a` and to queue B for every thread
-// with `want_b`, with one global atomic per queue and block (a queue's count is a single
-// address that every block of the grid updates).  Called by all threads of the block.
+// Block-wide queue appends: every thread with `want_a` appends `slot` to queue A, every
+// thread with kb >= 0 to queue kb of the B family (queue k at qb + k * capb, its count at
+// cb[k]), with one global atomic per queue and block (a queue's count is a single address
+// that every block of the grid updates).  Called by all threads of the block; wf_push_init
+// clears the shared counts first.
 struct WfPushSh {
-    uint32_t na[kTraceBlock / 32], nb[kTraceBlock / 32];
-    uint32_t base_a, base_b;
+    uint32_t na[kTraceBlock / 32];
+    uint32_t nb[kSearchKinds];
+    uint32_t base_a, base_b[kSearchKinds];
 };
+__device__ __forceinline__ void wf_push_init(WfPushSh &sh) {
+    if (threadIdx.x < kSearchKinds) sh.nb[threadIdx.x] = 0;  // visible after the next __syncthreads
+}
 __device__ __forceinline__ void wf_block_push(WfPushSh &sh, uint32_t *qa, uint32_t *ca, bool want_a, uint32_t *qb,
-                                              uint32_t *cb, bool want_b, uint32_t slot) {
+                                              uint32_t capb, uint32_t *cb, int kb, uint32_t slot) {
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const unsigned ba = __ballot_sync(0xffffffffu, want_a), bb = __ballot_sync(0xffffffffu, want_b);
-    if (lane == 0) {
-        sh.na[w] = __popc(ba);
-        sh.nb[w] = __popc(bb);
-    }
+    const unsigned lt = (1u << lane) - 1u;
+    const unsigned ba = __ballot_sync(0xffffffffu, want_a);
+    const unsigned peers = __match_any_sync(0xffffffffu, kb);
+    const int leader = __ffs(peers) - 1;
+    uint32_t off = 0;
+    if (lane == 0) sh.na[w] = __popc(ba);
+    if (kb >= 0 && lane == leader) off = atomicAdd(&sh.nb[kb], uint32_t(__popc(peers)));
+    off = __shfl_sync(0xffffffffu, off, leader) + __popc(peers & lt);
     __syncthreads();
     if (threadIdx.x == 0) {
-        uint32_t ta = 0, tb = 0;
+        uint32_t ta = 0;
         for (int k = 0; k < kTraceBlock / 32; ++k) {
-            const uint32_t a = sh.na[k], b = sh.nb[k];
+            const uint32_t a = sh.na[k];
             sh.na[k] = ta;  // exclusive prefix over the warps
-            sh.nb[k] = tb;
             ta += a;
-            tb += b;
         }
         sh.base_a = ta ? atomicAdd(ca, ta) : 0u;
-        sh.base_b = tb ? atomicAdd(cb, tb) : 0u;
+    }
+    if (threadIdx.x < kSearchKinds) {
+        const uint32_t t = sh.nb[threadIdx.x];
+        if (t) sh.base_b[threadIdx.x] = atomicAdd(&cb[threadIdx.x], t);
     }
     __syncthreads();
-    const unsigned lt = (1u << lane) - 1u;
     if (want_a) qa[sh.base_a + sh.na[w] + __popc(ba & lt)] = slot;
-    if (want_b) qb[sh.base_b + sh.nb[w] + __popc(bb & lt)] = slot;
+    if (kb >= 0) qb[size_t(kb) * capb + sh.base_b[kb] + off] = slot;
+    if (threadIdx.x < kSearchKinds) sh.nb[threadIdx.x] = 0;  // read by no thread before the barrier below
     __syncthreads();  // sh is reused by the next call
 }
 
@@ -986,19 +1087,21 @@ __device__ __forceinline__ void wf_stage_ray(const SceneDev &S, const WfRay &r, 
     }
 }
 
-// search step: nearest element of the current stage (raytrace.cpp:698-770)
-template <int MIXED, int RECORDS>
+// search step: nearest element of the current stage (raytrace.cpp:698-770), with the code
+// of search kind KIND (the kind of the ray's stage; 0 holds every case)
+template <int MIXED, int RECORDS, int KIND = 0>
 __device__ __forceinline__ int wf_search(const SceneDev &S, const TraceOut &O, WfBlockCtr &c, WfRay &r) {
     double ps[3], cs[3];
     wf_stage_ray(S, r, ps, cs);
-    const int j = nearest<MIXED>(S, S.stages[r.si], ps, cs, r.last_j);
+    const int j = nearest_kind<MIXED, KIND>(S, S.stages[r.si], ps, cs, r.last_j);
     if (j < 0) return wf_exit_stage<RECORDS>(S, O, c, r, ps, cs);
     r.next_j = j;
     return kWfShade;
 }
 
-// shade step: the hit on element next_j and what the ray does there (raytrace.cpp:830-1000)
-template <int MIXED, int RECORDS>
+// shade step: the hit on element next_j and what the ray does there (raytrace.cpp:830-1000);
+// FLAT: the stage holds flat elements only
+template <int MIXED, int RECORDS, int FLAT = 0>
 __device__ __forceinline__ int wf_shade(const SceneDev &S, const TraceOut &O, WfBlockCtr &c, WfRay &r) {
     const int si = r.si;
     const StageRec &st = S.stages[si];
@@ -1010,7 +1113,8 @@ __device__ __forceinline__ int wf_shade(const SceneDev &S, const TraceOut &O, Wf
     Hit h;
     double pl;
     // re-test the chosen element for the full hit (same arithmetic as the search)
-    if (!element_test<MIXED>(S, e, ps, cs, pl, &h)) return wf_exit_stage<RECORDS>(S, O, c, r, ps, cs);
+    const bool hit = FLAT ? element_test_flat<MIXED>(e, ps, cs, pl, &h) : element_test<MIXED>(S, e, ps, cs, pl, &h);
+    if (!hit) return wf_exit_stage<RECORDS>(S, O, c, r, ps, cs);
     const int hits = ++r.hits;
     if (hits == 1) {
         warp_count(O.first_hits, st.first_elem + j);
@@ -1109,12 +1213,13 @@ __device__ __forceinline__ int wf_shade(const SceneDev &S, const TraceOut &O, Wf
 // First kernel: the batch's numbered rays (hit-list entries below the cut-off at the
 // requested hit count; k_advance applies the same rule after the trace) enter the first
 // stage and are shaded on the element the probe found.
-template <int MIXED, int RECORDS>
+template <int MIXED, int RECORDS, int FLAT>
 __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_first(
     const __grid_constant__ SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx, const uint32_t *total,
-    const RunState *rs, TraceOut O, WfState W, uint32_t *q_search, uint32_t *n_search) {
+    const RunState *rs, TraceOut O, WfState W, const __grid_constant__ WfQueues Q) {
     __shared__ WfBlockCtr c;
     __shared__ WfPushSh psh;
+    wf_push_init(psh);
     wf_ctr_init(c);
     uint32_t n = 0, take = 0, raynum_base = 0;
     if (!rs->reached) {
@@ -1149,14 +1254,17 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_first(
                 r.moved = true;
             }
         }
-        int status = kWfDone;
+        int kb = -1;
         if (live) {
             wf_stage_enter(c, 0, r.raynum);
             // (an entry without a known element is searched in the first round)
-            status = (r.next_j >= 0) ? wf_shade<MIXED, RECORDS>(S, O, c, r) : int(kWfSearch);
-            if (status != kWfDone) wf_store(W, i, r, true);
+            const int status = (r.next_j >= 0) ? wf_shade<MIXED, RECORDS, FLAT>(S, O, c, r) : int(kWfSearch);
+            if (status != kWfDone) {
+                wf_store(W, i, r, true);
+                kb = Q.stage_queue[r.si];
+            }
         }
-        wf_block_push(psh, q_search, n_search, status != kWfDone, q_search, n_search, false, i);
+        wf_block_push(psh, nullptr, nullptr, false, Q.search[0], Q.cap, Q.counts, kb, i);
     }
     wf_ctr_flush(c, S, O);
 }
@@ -1166,9 +1274,10 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_first(
 // (key: bit 62 set, row index), as the replayed rays' first-stage draws are not known.
 template <int MIXED, int RECORDS>
 __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_replay(
-    const __grid_constant__ SceneDev S, TraceOut O, WfState W, ReplayIn in, uint32_t *q_search, uint32_t *n_search) {
+    const __grid_constant__ SceneDev S, TraceOut O, WfState W, ReplayIn in, const __grid_constant__ WfQueues Q) {
     __shared__ WfBlockCtr c;
     __shared__ WfPushSh psh;
+    wf_push_init(psh);
     wf_ctr_init(c);
     const uint32_t n = in.n;
     const uint32_t stride = gridDim.x * kTraceBlock;
@@ -1194,112 +1303,154 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_replay(
             wf_stage_enter(c, 1, r.raynum);
             wf_store(W, i, r, true);
         }
-        wf_block_push(psh, q_search, n_search, live, q_search, n_search, false, i);
+        wf_block_push(psh, nullptr, nullptr, false, Q.search[0], Q.cap, Q.counts, live ? int(Q.stage_queue[1]) : -1,
+                      i);
     }
     wf_ctr_flush(c, S, O);
 }
 
-// Search kernel: rays queued for a search; those that find an element go to the shade
-// queue, those that move on to another stage back to the search queue of the next round.
-template <int MIXED, int RECORDS>
-__global__ void __launch_bounds__(kTraceBlock, kWfSearchMinBlocks) k_wf_search(
-    const __grid_constant__ SceneDev S, TraceOut O, WfState W, const uint32_t *q_in, const uint32_t *n_in, uint32_t *q_shade,
-    uint32_t *n_shade, uint32_t *q_next, uint32_t *n_next) {
+// Search kernel of search kind KIND, over queue k of round r: rays that find an element go
+// to the round's shade queue, those that move on to another stage to the next round's
+// search queue of that stage.
+template <int KIND>
+struct SearchBounds {
+    static constexpr int min_blocks = (KIND & kSearchBrute) ? kWfBruteMinBlocks : kWfSearchMinBlocks;
+};
+template <int MIXED, int RECORDS, int KIND>
+__global__ void __launch_bounds__(kTraceBlock, SearchBounds<KIND>::min_blocks) k_wf_search(
+    const __grid_constant__ SceneDev S, TraceOut O, WfState W, const __grid_constant__ WfQueues Q, int r, int k) {
     __shared__ WfBlockCtr c;
     __shared__ WfPushSh psh;
+    wf_push_init(psh);
     wf_ctr_init(c);
-    const uint32_t n = *n_in;
+    const int nq = Q.n_queues;
+    uint32_t *cnt = Q.counts + r * (nq + 1);
+    const uint32_t *q_in = Q.search[r & 1] + size_t(k) * Q.cap;
+    const uint32_t n = cnt[k];
     const uint32_t stride = gridDim.x * kTraceBlock;
     const uint32_t n_round = (n + kTraceBlock - 1) / kTraceBlock * kTraceBlock;
     for (uint32_t q = blockIdx.x * kTraceBlock + threadIdx.x; q < n_round; q += stride) {
-        int status = kWfDone;
+        int status = kWfDone, kb = -1;
         uint32_t i = 0;
         if (q < n) {
             i = q_in[q];
-            WfRay r = wf_load(W, i);
-            status = wf_search<MIXED, RECORDS>(S, O, c, r);
-            if (status != kWfDone) wf_store(W, i, r, false);
+            WfRay ray = wf_load(W, i);
+            status = wf_search<MIXED, RECORDS, KIND>(S, O, c, ray);
+            if (status != kWfDone) wf_store(W, i, ray, false);
+            if (status == kWfSearch) kb = Q.stage_queue[ray.si];
         }
-        wf_block_push(psh, q_shade, n_shade, status == kWfShade, q_next, n_next, status == kWfSearch, i);
+        wf_block_push(psh, Q.shade, cnt + nq, status == kWfShade, Q.search[(r + 1) & 1], Q.cap, cnt + nq + 1, kb, i);
     }
     wf_ctr_flush(c, S, O);
 }
 
-// Shade kernel: rays with a known element; survivors go to the next round's search queue.
+// Shade kernel over round r's shade queue: survivors go to the next round's search queues.
 template <int MIXED, int RECORDS>
-__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_shade(
-    const __grid_constant__ SceneDev S, TraceOut O, WfState W, const uint32_t *q_in, const uint32_t *n_in, uint32_t *q_next,
-    uint32_t *n_next) {
+__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_shade(const __grid_constant__ SceneDev S, TraceOut O,
+                                                                             WfState W, const __grid_constant__ WfQueues Q,
+                                                                             int r) {
     __shared__ WfBlockCtr c;
     __shared__ WfPushSh psh;
+    wf_push_init(psh);
     wf_ctr_init(c);
-    const uint32_t n = *n_in;
+    const int nq = Q.n_queues;
+    uint32_t *cnt = Q.counts + r * (nq + 1);
+    const uint32_t n = cnt[nq];
     const uint32_t stride = gridDim.x * kTraceBlock;
     const uint32_t n_round = (n + kTraceBlock - 1) / kTraceBlock * kTraceBlock;
     for (uint32_t q = blockIdx.x * kTraceBlock + threadIdx.x; q < n_round; q += stride) {
-        int status = kWfDone;
+        int kb = -1;
         uint32_t i = 0;
         if (q < n) {
-            i = q_in[q];
-            WfRay r = wf_load(W, i);
-            status = wf_shade<MIXED, RECORDS>(S, O, c, r);
-            if (status != kWfDone) wf_store(W, i, r, false);
+            i = Q.shade[q];
+            WfRay ray = wf_load(W, i);
+            const int status = wf_shade<MIXED, RECORDS>(S, O, c, ray);
+            if (status != kWfDone) {
+                wf_store(W, i, ray, false);
+                kb = Q.stage_queue[ray.si];
+            }
         }
-        wf_block_push(psh, q_next, n_next, status != kWfDone, q_next, n_next, false, i);
+        wf_block_push(psh, nullptr, nullptr, false, Q.search[(r + 1) & 1], Q.cap, cnt + nq + 1, kb, i);
     }
     wf_ctr_flush(c, S, O);
 }
 
-// Finishing kernel: every ray still queued runs to its end, one step after the other.
+// Finishing kernel: every ray still queued (the search queues of round `rounds`) runs to
+// its end, one step after the other.
 template <int MIXED, int RECORDS>
-__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_finish(const __grid_constant__ SceneDev S, TraceOut O, WfState W,
-                                                                              const uint32_t *q_in,
-                                                                              const uint32_t *n_in) {
+__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_finish(const __grid_constant__ SceneDev S, TraceOut O,
+                                                                              WfState W, const __grid_constant__ WfQueues Q) {
     __shared__ WfBlockCtr c;
     wf_ctr_init(c);
-    const uint32_t n = *n_in;
-    for (uint32_t q = blockIdx.x * kTraceBlock + threadIdx.x; q < n; q += gridDim.x * kTraceBlock) {
-        WfRay r = wf_load(W, q_in[q]);
-        int status = (r.next_j >= 0) ? int(kWfShade) : int(kWfSearch);
-        while (status != kWfDone)
-            status = (status == kWfShade) ? wf_shade<MIXED, RECORDS>(S, O, c, r) : wf_search<MIXED, RECORDS>(S, O, c, r);
+    const int nq = Q.n_queues, R = Q.rounds;
+    const uint32_t *cnt = Q.counts + R * (nq + 1);
+    for (int k = 0; k < nq; ++k) {
+        const uint32_t n = cnt[k];
+        const uint32_t *q_in = Q.search[R & 1] + size_t(k) * Q.cap;
+        for (uint32_t q = blockIdx.x * kTraceBlock + threadIdx.x; q < n; q += gridDim.x * kTraceBlock) {
+            WfRay r = wf_load(W, q_in[q]);
+            int status = (r.next_j >= 0) ? int(kWfShade) : int(kWfSearch);
+            while (status != kWfDone)
+                status = (status == kWfShade) ? wf_shade<MIXED, RECORDS>(S, O, c, r) : wf_search<MIXED, RECORDS>(S, O, c, r);
+        }
     }
     wf_ctr_flush(c, S, O);
 }
 
 // Host side of the trace launch (instantiated per precision in its translation unit).
+template <int MIXED, int RECORDS, int KIND>
+static void wf_launch_search(const SceneDev &S, const TraceOut &O, const WfState &W, const WfQueues &Q, int r, int k,
+                             int sms, cudaStream_t st) {
+    // persistent grid: every block the kernel can keep resident on every SM
+    static int per_sm = 0;
+    if (per_sm == 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_wf_search<MIXED, RECORDS, KIND>, kTraceBlock, 0);
+        per_sm = per_sm > 0 ? per_sm : 1;
+    }
+    k_wf_search<MIXED, RECORDS, KIND><<<sms * per_sm, kTraceBlock, 0, st>>>(S, O, W, Q, r, k);
+}
+
 template <int MIXED, int RECORDS>
 static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx,
                      const uint32_t *total, const RunState *rs, const TraceOut &O, const WfState &W,
                      const WfQueues &Q, const ReplayIn *replay, cudaStream_t st) {
     // persistent grids: every block the kernels can keep resident on every SM
-    static int per_sm[4] = {0, 0, 0, 0};
+    static int per_sm[3] = {0, 0, 0};
     if (per_sm[0] == 0) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_wf_first<MIXED, RECORDS>, kTraceBlock, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_wf_search<MIXED, RECORDS>, kTraceBlock, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_wf_shade<MIXED, RECORDS>, kTraceBlock, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[3], k_wf_finish<MIXED, RECORDS>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_wf_first<MIXED, RECORDS, 0>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_wf_shade<MIXED, RECORDS>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_wf_finish<MIXED, RECORDS>, kTraceBlock, 0);
         for (int &x : per_sm) x = x > 0 ? x : 1;
     }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int R = Q.rounds;
-    cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * (2 * R + 1), st);
+    const int R = Q.rounds, nq = Q.n_queues;
+    int launches = 2;
+    cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * (R + 1) * (nq + 1), st);
     if (replay)
-        k_wf_replay<MIXED, RECORDS><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, O, W, *replay, Q.search[0], Q.counts);
+        k_wf_replay<MIXED, RECORDS><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, O, W, *replay, Q);
+    else if (S.stages[0].flat_only)  // a first stage of flat elements only (heliostat fields)
+        k_wf_first<MIXED, RECORDS, 1><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs,
+                                                                                 O, W, Q);
     else
-        k_wf_first<MIXED, RECORDS><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs, O,
-                                                                              W, Q.search[0], Q.counts);
+        k_wf_first<MIXED, RECORDS, 0><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs,
+                                                                                 O, W, Q);
     for (int r = 0; r < R; ++r) {
-        uint32_t *c = Q.counts + 2 * r;
-        k_wf_search<MIXED, RECORDS><<<sms * per_sm[1], kTraceBlock, 0, st>>>(
-            S, O, W, Q.search[r & 1], c, Q.shade, c + 1, Q.search[(r + 1) & 1], c + 2);
-        k_wf_shade<MIXED, RECORDS><<<sms * per_sm[2], kTraceBlock, 0, st>>>(S, O, W, Q.shade, c + 1,
-                                                                           Q.search[(r + 1) & 1], c + 2);
+        for (int k = 0; k < nq; ++k) {
+            switch (Q.queue_kind[k]) {
+                case 1: wf_launch_search<MIXED, RECORDS, 1>(S, O, W, Q, r, k, sms, st); break;
+                case 2: wf_launch_search<MIXED, RECORDS, 2>(S, O, W, Q, r, k, sms, st); break;
+                case 3: wf_launch_search<MIXED, RECORDS, 3>(S, O, W, Q, r, k, sms, st); break;
+                default: wf_launch_search<MIXED, RECORDS, 0>(S, O, W, Q, r, k, sms, st);
+            }
+            ++launches;
+        }
+        k_wf_shade<MIXED, RECORDS><<<sms * per_sm[1], kTraceBlock, 0, st>>>(S, O, W, Q, r);
+        ++launches;
     }
-    k_wf_finish<MIXED, RECORDS><<<sms * per_sm[3], kTraceBlock, 0, st>>>(S, O, W, Q.search[R & 1], Q.counts + 2 * R);
-    return 2 + 2 * R;
+    k_wf_finish<MIXED, RECORDS><<<sms * per_sm[2], kTraceBlock, 0, st>>>(S, O, W, Q);
+    return launches;
 }
 
 }  // namespace stb
