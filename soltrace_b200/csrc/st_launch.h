@@ -27,7 +27,9 @@ constexpr int kSearchFlat = 1, kSearchBrute = 2, kSearchKinds = 4;
 __host__ __device__ inline int stage_search_kind(const StageRec &st) {
     return (st.flat_only ? kSearchFlat : 0) | ((!st.grid_on && st.bvh_off < 0) ? kSearchBrute : 0);
 }
-constexpr int kWfBruteMinBlocks = 6;  // search kernels of stages tested element by element
+constexpr int kWfBruteMinBlocks = 8;      // search kernels of stages tested element by element
+constexpr int kWfFlatSearchMinBlocks = 5;  // search kernels of flat-only stages
+constexpr int kWfFirstFlatMinBlocks = 5;   // first kernel on a flat-only first stage
 
 enum RunFlags : unsigned {
     kFlagHitCap = 1u,         // a ray reached kMaxHitsPerStage in one stage

@@ -1214,7 +1214,7 @@ __device__ __forceinline__ int wf_shade(const SceneDev &S, const TraceOut &O, Wf
 // requested hit count; k_advance applies the same rule after the trace) enter the first
 // stage and are shaded on the element the probe found.
 template <int MIXED, int RECORDS, int FLAT>
-__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_first(
+__global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kWfShadeMinBlocks) k_wf_first(
     const __grid_constant__ SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx, const uint32_t *total,
     const RunState *rs, TraceOut O, WfState W, const __grid_constant__ WfQueues Q) {
     __shared__ WfBlockCtr c;
@@ -1314,7 +1314,9 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_replay(
 // search queue of that stage.
 template <int KIND>
 struct SearchBounds {
-    static constexpr int min_blocks = (KIND & kSearchBrute) ? kWfBruteMinBlocks : kWfSearchMinBlocks;
+    static constexpr int min_blocks = (KIND & kSearchBrute) ? kWfBruteMinBlocks
+                                      : (KIND & kSearchFlat) ? kWfFlatSearchMinBlocks
+                                                             : kWfSearchMinBlocks;
 };
 template <int MIXED, int RECORDS, int KIND>
 __global__ void __launch_bounds__(kTraceBlock, SearchBounds<KIND>::min_blocks) k_wf_search(
