@@ -15,6 +15,12 @@ void launch_sun_candidates(const SceneDev &S, uint64_t s0, uint32_t n, const Pro
 void launch_offsets(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_t *total, cudaStream_t st) {
     k_offsets<<<1, 1024, 0, st>>>(counts, nb, offsets, total);
 }
+void launch_scan(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_t *total, uint32_t *parts,
+                 cudaStream_t st) {
+    const uint32_t chunks = std::max(1u, (nb + kScanChunk - 1) / kScanChunk);
+    k_scan_parts<<<chunks, kScanBlock, 0, st>>>(counts, nb, parts);
+    k_scan_chunks<<<chunks, kScanBlock, 0, st>>>(counts, nb, parts, offsets, total);
+}
 void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uint32_t *counts,
                     const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st) {
     const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;

@@ -157,6 +157,12 @@ void launch_list_sort(uint64_t s0, const ProbeOut &o, const uint32_t *offsets, c
 unsigned take_fe_failures_fp64();
 unsigned take_fe_failures_mixed();
 void launch_offsets(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_t *total, cudaStream_t st);
+// the same exclusive scan over the whole grid (two kernels); `parts` holds scan_parts(nb)
+// chunk sums
+void launch_scan(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_t *total, uint32_t *parts,
+                 cudaStream_t st);
+constexpr int kScanChunk = 2048, kScanBlock = 256;
+constexpr size_t scan_parts(uint32_t nb) { return (size_t(nb) + kScanChunk - 1) / kScanChunk + 1; }
 void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uint32_t *counts,
                     const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st);
 // cut-off and run state after a batch; the last numbered sun ray is read from the

@@ -59,7 +59,7 @@ struct Workspace {
     DevBuf stage_cells, grid_sphere, grid_elem, beam_axis, beam_range, beam_elem;
     DevBuf elems, elem_sphere, optics, surf, tables, bvh, bvh_items, cell_start, cell_disc, cell_par, inv_cdf, expos,
         excos;
-    DevBuf acc, ctr, rs, rec_count, counts, offsets, total, recs;
+    DevBuf acc, ctr, rs, rec_count, counts, offsets, total, scan_parts, recs;
     DevBuf cand;      // probe's ray list: count, then one sun-ray index per entry
     DevBuf cand_el;   // probe's result per list entry (element + 1, 0 for a miss)
     DevBuf hit_mask;  // one bit per sun ray of the batch, set for a hit
@@ -497,6 +497,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 ProbeOut po;
                 CK(probe_buffers(ws, n, po));
                 CK(d_offsets.ensure(size_t(nb) * 4));
+                CK(ws.scan_parts.ensure(scan_parts(nb) * 4));
                 CK(d_total.ensure(8));
                 CK(d_s_sid.ensure(n * 8));
                 CK(d_s_el.ensure(n * 4));
@@ -514,7 +515,8 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                     out.gpu_launches += launch_probe_mixed(S, sun_next, uint32_t(n), po, drs, tu.probe, st);
                 else
                     out.gpu_launches += launch_probe_fp64(S, sun_next, uint32_t(n), po, drs, tu.probe, st);
-                launch_offsets(po.block_counts, nb, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), st);
+                launch_scan(po.block_counts, nb, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(),
+                            ws.scan_parts.as<uint32_t>(), st);
                 launch_list_sort(sun_next, po, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), drs, n_elem0,
                                  d_ecount.as<uint32_t>(), d_ecursor.as<uint32_t>(), d_etotal.as<uint32_t>(),
                                  d_s_sid.as<uint64_t>(), d_s_el.as<uint32_t>(), d_s_idx.as<uint32_t>(), uint32_t(n), st);
@@ -536,7 +538,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 CK(cudaEventRecord(p2, st));
                 launch_advance(d_total.as<uint32_t>(), nullptr, sun_next, uint32_t(n), drs, st);
                 CK(cudaGetLastError());
-                out.gpu_launches += 2;  // offsets, advance
+                out.gpu_launches += 3;  // scan (two kernels), advance
                 probe_ev.push_back({p0, p1});
                 trace_ev.push_back({p1, p2});
                 queued += n;

@@ -714,6 +714,70 @@ __global__ void __launch_bounds__(1024) k_offsets(const uint32_t *counts, uint32
     if (threadIdx.x == 0) *total = carry;
 }
 
+// Grid-wide exclusive scan of the per-block counts in two kernels: k_scan_parts sums each
+// chunk of kScanChunk counts, k_scan_chunks scans each chunk with the sum of the chunks
+// before it (at most a few dozen per batch, added up by every block); kScanChunk and
+// kScanBlock in st_launch.h.
+__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t *sh) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    uint32_t t = 0;
+    for (int k = 0; k < kScanBlock / 32; ++k) t += sh[k];
+    __syncthreads();
+    return t;
+}
+__global__ void __launch_bounds__(kScanBlock) k_scan_parts(const uint32_t *counts, uint32_t nb, uint32_t *parts) {
+    __shared__ uint32_t sh[kScanBlock / 32];
+    const uint32_t i0 = blockIdx.x * kScanChunk + threadIdx.x * (kScanChunk / kScanBlock);
+    uint32_t v = 0;
+#pragma unroll
+    for (int k = 0; k < kScanChunk / kScanBlock; ++k) v += (i0 + k < nb) ? counts[i0 + k] : 0u;
+    v = block_sum(v, sh);
+    if (threadIdx.x == 0) parts[blockIdx.x] = v;
+}
+__global__ void __launch_bounds__(kScanBlock) k_scan_chunks(const uint32_t *counts, uint32_t nb, const uint32_t *parts,
+                                                            uint32_t *offsets, uint32_t *total) {
+    constexpr int kPer = kScanChunk / kScanBlock;
+    __shared__ uint32_t sh[kScanBlock / 32];
+    __shared__ uint32_t wsum[kScanBlock / 32];
+    // sum of the chunks before this one (and of all chunks, for the total)
+    uint32_t before = 0, all = 0;
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += kScanBlock) {
+        const uint32_t p = parts[b];
+        all += p;
+        if (b < blockIdx.x) before += p;
+    }
+    before = block_sum(before, sh);
+    all = block_sum(all, sh);
+    const uint32_t i0 = blockIdx.x * kScanChunk + threadIdx.x * kPer;
+    uint32_t v[kPer], sum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        v[k] = (i0 + k < nb) ? counts[i0 + k] : 0u;
+        sum += v[k];
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    uint32_t run = before + x - sum;
+    for (int k = 0; k < w; ++k) run += wsum[k];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        if (i0 + k < nb) offsets[i0 + k] = run;
+        run += v[k];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *total = all;
+}
+
 __global__ void __launch_bounds__(kProbeBlock) k_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem,
                                                           const uint32_t *counts, const uint32_t *offsets,
                                                           uint64_t *hit_sid, uint32_t *hit_el) {
