@@ -1031,7 +1031,9 @@ static __device__ __noinline__ int cold_intersect(const SceneDev &S, const ElemR
     return newton_hit(e, S.surf_data, pe, ce, out, n, t);
 }
 
-template <int MIXED>
+// CLOSED: the element is known to have a closed-form surface (closed_form_surface), so the
+// out-of-line path is left out of the caller
+template <int MIXED, int CLOSED = 0>
 __device__ __forceinline__ bool element_test(const SceneDev &S, const ElemRec &e, const double ps[3],
                                              const double cs[3], double &plen, Hit *full) {
     double pe[3], ce[3];
@@ -1055,7 +1057,7 @@ __device__ __forceinline__ bool element_test(const SceneDev &S, const ElemRec &e
             err = quadric_hit(e, pe, ce, out, n, t);
             break;
         case kSurfTorus:
-            err = cold_intersect(S, e, pe, ce, out, n, t);
+            err = CLOSED ? 1 : cold_intersect(S, e, pe, ce, out, n, t);
             break;
         default: {
             const int s = e.surf | 0x20;
@@ -1064,7 +1066,7 @@ __device__ __forceinline__ bool element_test(const SceneDev &S, const ElemRec &e
             if (closed)
                 err = quadric_hit(e, pe, ce, out, n, t);
             else
-                err = cold_intersect(S, e, pe, ce, out, n, t);
+                err = CLOSED ? 1 : cold_intersect(S, e, pe, ce, out, n, t);
         }
     }
     if (err > 0 || t < 0) return false;

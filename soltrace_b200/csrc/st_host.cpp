@@ -1302,6 +1302,9 @@ bool flatten(Context *cx, HostScene &hs) {
         }
         sr.flat_only = 1;
         for (const Elem &e : st.elems) sr.flat_only &= (e.stype == 3) ? 1 : 0;
+        sr.closed_only = 1;
+        for (int k = sr.first_elem; k < sr.first_elem + sr.n_elem; ++k)
+            sr.closed_only &= closed_form_surface(hs.elems[k].stype, hs.elems[k].surf) ? 1 : 0;
         sr.grid_on = 0;
         if (st.elems.size() >= 64)
             build_ground_grid(st.elems, hs.elem_sphere.data() + sr.first_elem, sr, hs.stage_cells, hs.grid_sphere,

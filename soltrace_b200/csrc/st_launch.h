@@ -22,14 +22,17 @@ constexpr int kWfSearchMinBlocks = 4;
 // Search kinds: the trace's search kernel is compiled once per kind, holding only the code
 // its stages need (fewer registers, more resident warps).  Bits: kSearchFlat, the stage holds
 // flat elements only; kSearchBrute, the stage has neither ground grid nor BVH (few elements,
-// tested one after the other).
-constexpr int kSearchFlat = 1, kSearchBrute = 2, kSearchKinds = 4;
+// tested one after the other); kSearchClosed, the stage's surfaces are all closed-form (set
+// only without kSearchFlat, which implies it).
+constexpr int kSearchFlat = 1, kSearchBrute = 2, kSearchClosed = 4, kSearchKinds = 8;
 __host__ __device__ inline int stage_search_kind(const StageRec &st) {
-    return (st.flat_only ? kSearchFlat : 0) | ((!st.grid_on && st.bvh_off < 0) ? kSearchBrute : 0);
+    return (st.flat_only ? kSearchFlat : (st.closed_only ? kSearchClosed : 0)) |
+           ((!st.grid_on && st.bvh_off < 0) ? kSearchBrute : 0);
 }
 constexpr int kWfBruteMinBlocks = 8;      // search kernels of stages tested element by element
 constexpr int kWfFlatSearchMinBlocks = 5;  // search kernels of flat-only stages
 constexpr int kWfFirstFlatMinBlocks = 5;   // first kernel on a flat-only first stage
+constexpr int kWfClosedShadeMinBlocks = 4; // shade kernel of scenes with closed-form surfaces only
 
 enum RunFlags : unsigned {
     kFlagHitCap = 1u,         // a ray reached kMaxHitsPerStage in one stage

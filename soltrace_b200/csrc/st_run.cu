@@ -165,7 +165,8 @@ static cudaError_t wf_buffers(Workspace &ws, const SceneDev &S, uint64_t cap, Wf
     cap = std::max<uint64_t>(cap, 1);
     const int nst = S.n_stages;
     Q = WfQueues{};
-    int queue_of_kind[kSearchKinds] = {-1, -1, -1, -1};
+    int queue_of_kind[kSearchKinds];
+    for (int &q : queue_of_kind) q = -1;
     for (int s = 0; s < nst; ++s) {
         const int k = stage_search_kind(S.stages[s]);
         if (queue_of_kind[k] < 0) {

@@ -38,6 +38,16 @@ enum SurfType : int {
     kSurfTorus = 10,     // 'd'
 };
 
+// Surfaces the element test intersects in closed form (flat, cylinder and the conics it
+// solves directly); the others (torus, Newton-iterated surfaces) take its out-of-line path.
+ST_HD inline bool closed_form_surface(int stype, int surf) {
+    if (stype == kSurfFlat || stype == kSurfCylinder) return true;
+    if (stype == kSurfTorus) return false;
+    const int s = surf | 0x20;
+    return (s == 'p') || (s == 's' && (stype == kSurfConic || stype == kSurfSingleAxis)) ||
+           (s == 'o' && stype == kSurfConic);
+}
+
 struct ElemRec {
     double R[9];      // stage -> element rotation, row-major (RRefToLoc)
     double o[3];      // element origin in stage coordinates
@@ -79,6 +89,7 @@ struct StageRec {
     int grid_on;
     int gnx, gny, gcell_off;  // cells, first cell in SceneDev::stage_cells
     int flat_only;            // every element of the stage is flat (surface type 3)
+    int closed_only;          // every element's surface is intersected in closed form
     float gx0, gy0, gcell, ginv, gzlo, gzhi;
 };
 

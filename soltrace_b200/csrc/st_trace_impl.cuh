@@ -59,14 +59,17 @@ __device__ __forceinline__ void make_ray(const SceneDev &S, uint64_t sid, RayRng
 // ------------------------------------------------------------------------------------
 // nearest accepted hit in a stage (raytrace.cpp:698-770); -1 if none
 // ------------------------------------------------------------------------------------
-// element_test without the full hit; FLAT: the element is known to be flat
-template <int MIXED, int FLAT>
+// element_test without the full hit.  ET (element-test mode): 0 any element, kEtFlat the
+// element is known to be flat, kEtClosed its surface is known to be closed-form
+constexpr int kEtFlat = 1, kEtClosed = 2;
+template <int MIXED, int ET>
 __device__ __forceinline__ bool elem_hit(const SceneDev &S, const ElemRec &e, const double ps[3], const double cs[3],
                                          double &pl) {
-    return FLAT ? element_test_flat<MIXED>(e, ps, cs, pl) : element_test<MIXED>(S, e, ps, cs, pl, nullptr);
+    if (ET == kEtFlat) return element_test_flat<MIXED>(e, ps, cs, pl);
+    return element_test<MIXED, ET == kEtClosed ? 1 : 0>(S, e, ps, cs, pl, nullptr);
 }
 
-template <int MIXED, int FLAT = 0>
+template <int MIXED, int ET = 0>
 __device__ inline int nearest_brute(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3]) {
     int best = -1;
     double bp = 1e99;
@@ -74,7 +77,7 @@ __device__ inline int nearest_brute(const SceneDev &S, const StageRec &st, const
         const ElemRec &e = S.elems[st.first_elem + j];
         if (!e.enabled) continue;
         double pl;
-        if (elem_hit<MIXED, FLAT>(S, e, ps, cs, pl) && pl < bp) {
+        if (elem_hit<MIXED, ET>(S, e, ps, cs, pl) && pl < bp) {
             bp = pl;
             best = j;
         }
@@ -85,7 +88,7 @@ __device__ inline int nearest_brute(const SceneDev &S, const StageRec &st, const
 // BVH over element bounding spheres; nodes farther than the best hit so far are
 // skipped (the test is on the entry distance minus the 1e-5 nudge, with slack for
 // the float box arithmetic).
-template <int MIXED, int FLAT = 0>
+template <int MIXED, int ET = 0>
 __device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3],
                                   int from) {
     const BvhNode *nodes = S.bvh + st.bvh_off;
@@ -128,7 +131,7 @@ __device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const d
                 const ElemRec &e = S.elems[st.first_elem + j];
                 if (!e.enabled) continue;
                 double pl;
-                if (elem_hit<MIXED, FLAT>(S, e, ps, cs, pl) && (pl < bp || (pl == bp && j < best))) {
+                if (elem_hit<MIXED, ET>(S, e, ps, cs, pl) && (pl < bp || (pl == bp && j < best))) {
                     bp = pl;
                     best = j;
                 }
@@ -151,7 +154,7 @@ __device__ inline int nearest_bvh(const SceneDev &S, const StageRec &st, const d
 // from is listed in a visited cell (the padded discs absorb the float rounding of the
 // walk), and the choice among hits is the serial search's (shortest path, lower index on
 // ties), so the result is the brute-force search's.
-template <int MIXED, int FLAT = 0>
+template <int MIXED, int ET = 0>
 __device__ inline int nearest_grid(const SceneDev &S, const StageRec &st, const double ps[3], const double cs[3],
                                    int from) {
     const float ox = float(ps[0]), oy = float(ps[1]), oz = float(ps[2]);
@@ -207,7 +210,7 @@ __device__ inline int nearest_grid(const SceneDev &S, const StageRec &st, const 
         for (int c = 0; c < nc; ++c) {
             const int j = cand[256 * c];
             double pl;
-            if (elem_hit<MIXED, FLAT>(S, S.elems[st.first_elem + j], ps, cs, pl) &&
+            if (elem_hit<MIXED, ET>(S, S.elems[st.first_elem + j], ps, cs, pl) &&
                 (pl < bp || (pl == bp && j < best))) {
                 bp = pl;
                 best = j;
@@ -268,10 +271,10 @@ __device__ __forceinline__ int nearest(const SceneDev &S, const StageRec &st, co
 template <int MIXED, int KIND>
 __device__ __forceinline__ int nearest_kind(const SceneDev &S, const StageRec &st, const double ps[3],
                                             const double cs[3], int from) {
-    constexpr int F = (KIND & kSearchFlat) ? 1 : 0;
-    if (KIND & kSearchBrute) return nearest_brute<MIXED, F>(S, st, ps, cs);
-    if (st.grid_on) return nearest_grid<MIXED, F>(S, st, ps, cs, from);
-    return (st.bvh_off >= 0) ? nearest_bvh<MIXED, F>(S, st, ps, cs, from) : nearest_brute<MIXED, F>(S, st, ps, cs);
+    constexpr int ET = (KIND & kSearchFlat) ? kEtFlat : (KIND & kSearchClosed) ? kEtClosed : 0;
+    if (KIND & kSearchBrute) return nearest_brute<MIXED, ET>(S, st, ps, cs);
+    if (st.grid_on) return nearest_grid<MIXED, ET>(S, st, ps, cs, from);
+    return (st.bvh_off >= 0) ? nearest_bvh<MIXED, ET>(S, st, ps, cs, from) : nearest_brute<MIXED, ET>(S, st, ps, cs);
 }
 
 // first test of a first-stage sun ray through the sun-plane grid (cells list the
@@ -309,7 +312,7 @@ __device__ __forceinline__ int2 sun_cell(const SunDev &sun, double xs, double ys
 
 // Sun-ray probe through the grid for one ray; the double-precision ray is built only once
 // a cell entry passes the float pre-test.
-template <int MIXED, int FLAT = 0>
+template <int MIXED, int ET = 0>
 __device__ inline int nearest_sun_grid_lazy(const SceneDev &S, const StageRec &st, double xs, double ys) {
     const SunDev &sun = S.sun;
     const int2 range = sun_cell(sun, xs, ys);
@@ -328,7 +331,7 @@ __device__ inline int nearest_sun_grid_lazy(const SceneDev &S, const StageRec &s
             have_ray = true;
         }
         double pl;
-        if (elem_hit<MIXED, FLAT>(S, e, ps, cs, pl) && pl < bp) {
+        if (elem_hit<MIXED, ET>(S, e, ps, cs, pl) && pl < bp) {
             bp = pl;
             best = j;
         }
@@ -589,7 +592,7 @@ __global__ void __launch_bounds__(kResolveBlock, MINB) k_sun_resolve(const __gri
         rng.init(S.seed, s0 + i, 0);
         const double xs = sun.xmin + (sun.xmax - sun.xmin) * rng.u();
         const double ys = sun.ymin + (sun.ymax - sun.ymin) * rng.u();
-        const int b = nearest_sun_grid_lazy<MIXED, FLAT>(S, S.stages[0], xs, ys);
+        const int b = nearest_sun_grid_lazy<MIXED, FLAT ? kEtFlat : 0>(S, S.stages[0], xs, ys);
         const uint32_t h = (b >= 0) ? uint32_t(b + 1) : 0u;
         if (o.hit_elem) o.hit_elem[i] = h;
         if (o.cand_el) o.cand_el[c] = h;
@@ -1164,8 +1167,8 @@ __device__ __forceinline__ int wf_search(const SceneDev &S, const TraceOut &O, W
 }
 
 // shade step: the hit on element next_j and what the ray does there (raytrace.cpp:830-1000);
-// FLAT: the stage holds flat elements only
-template <int MIXED, int RECORDS, int FLAT = 0>
+// FLAT: the stage holds flat elements only; CLOSED: closed-form surfaces only
+template <int MIXED, int RECORDS, int FLAT = 0, int CLOSED = 0>
 __device__ __forceinline__ int wf_shade(const SceneDev &S, const TraceOut &O, WfBlockCtr &c, WfRay &r) {
     const int si = r.si;
     const StageRec &st = S.stages[si];
@@ -1177,7 +1180,7 @@ __device__ __forceinline__ int wf_shade(const SceneDev &S, const TraceOut &O, Wf
     Hit h;
     double pl;
     // re-test the chosen element for the full hit (same arithmetic as the search)
-    const bool hit = FLAT ? element_test_flat<MIXED>(e, ps, cs, pl, &h) : element_test<MIXED>(S, e, ps, cs, pl, &h);
+    const bool hit = FLAT ? element_test_flat<MIXED>(e, ps, cs, pl, &h) : element_test<MIXED, CLOSED>(S, e, ps, cs, pl, &h);
     if (!hit) return wf_exit_stage<RECORDS>(S, O, c, r, ps, cs);
     const int hits = ++r.hits;
     if (hits == 1) {
@@ -1411,8 +1414,9 @@ __global__ void __launch_bounds__(kTraceBlock, SearchBounds<KIND>::min_blocks) k
 }
 
 // Shade kernel over round r's shade queue: survivors go to the next round's search queues.
-template <int MIXED, int RECORDS>
-__global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_shade(const __grid_constant__ SceneDev S, TraceOut O,
+// CLOSED: every stage has closed-form surfaces only.
+template <int MIXED, int RECORDS, int CLOSED>
+__global__ void __launch_bounds__(kTraceBlock, CLOSED ? kWfClosedShadeMinBlocks : kWfShadeMinBlocks) k_wf_shade(const __grid_constant__ SceneDev S, TraceOut O,
                                                                              WfState W, const __grid_constant__ WfQueues Q,
                                                                              int r) {
     __shared__ WfBlockCtr c;
@@ -1430,7 +1434,7 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_shade(con
         if (q < n) {
             i = Q.shade[q];
             WfRay ray = wf_load(W, i);
-            const int status = wf_shade<MIXED, RECORDS>(S, O, c, ray);
+            const int status = wf_shade<MIXED, RECORDS, 0, CLOSED>(S, O, c, ray);
             if (status != kWfDone) {
                 wf_store(W, i, ray, false);
                 kb = Q.stage_queue[ray.si];
@@ -1481,10 +1485,11 @@ static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t 
                      const uint32_t *total, const RunState *rs, const TraceOut &O, const WfState &W,
                      const WfQueues &Q, const ReplayIn *replay, cudaStream_t st) {
     // persistent grids: every block the kernels can keep resident on every SM
-    static int per_sm[3] = {0, 0, 0};
+    static int per_sm[4] = {0, 0, 0, 0};
     if (per_sm[0] == 0) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_wf_first<MIXED, RECORDS, 0>, kTraceBlock, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_wf_shade<MIXED, RECORDS>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_wf_shade<MIXED, RECORDS, 0>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[3], k_wf_shade<MIXED, RECORDS, 1>, kTraceBlock, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_wf_finish<MIXED, RECORDS>, kTraceBlock, 0);
         for (int &x : per_sm) x = x > 0 ? x : 1;
     }
@@ -1492,6 +1497,8 @@ static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int R = Q.rounds, nq = Q.n_queues;
+    bool all_closed = true;  // every stage's surfaces are closed-form: the shade kernel without the rest
+    for (int s = 0; s < S.n_stages; ++s) all_closed = all_closed && S.stages[s].closed_only;
     int launches = 2;
     cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * (R + 1) * (nq + 1), st);
     if (replay)
@@ -1508,11 +1515,16 @@ static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t 
                 case 1: wf_launch_search<MIXED, RECORDS, 1>(S, O, W, Q, r, k, sms, st); break;
                 case 2: wf_launch_search<MIXED, RECORDS, 2>(S, O, W, Q, r, k, sms, st); break;
                 case 3: wf_launch_search<MIXED, RECORDS, 3>(S, O, W, Q, r, k, sms, st); break;
+                case 4: wf_launch_search<MIXED, RECORDS, 4>(S, O, W, Q, r, k, sms, st); break;
+                case 6: wf_launch_search<MIXED, RECORDS, 6>(S, O, W, Q, r, k, sms, st); break;
                 default: wf_launch_search<MIXED, RECORDS, 0>(S, O, W, Q, r, k, sms, st);
             }
             ++launches;
         }
-        k_wf_shade<MIXED, RECORDS><<<sms * per_sm[1], kTraceBlock, 0, st>>>(S, O, W, Q, r);
+        if (all_closed)
+            k_wf_shade<MIXED, RECORDS, 1><<<sms * per_sm[3], kTraceBlock, 0, st>>>(S, O, W, Q, r);
+        else
+            k_wf_shade<MIXED, RECORDS, 0><<<sms * per_sm[1], kTraceBlock, 0, st>>>(S, O, W, Q, r);
         ++launches;
     }
     k_wf_finish<MIXED, RECORDS><<<sms * per_sm[2], kTraceBlock, 0, st>>>(S, O, W, Q);
