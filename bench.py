@@ -323,7 +323,7 @@ def main():
     else:
         ach, pk = trace_tflops, fm.NOMINAL_FP64_TFLOPS
         hbm_ach = fm.trace_bytes(hits) / (trace_ms / 1e3) / 1e9
-    group = {"k_probe": "probe group (k_sun_candidates, k_sun_resolve, k_offsets, k_compact, element sort)",
+    group = {"k_probe": "probe group (k_sun_candidates, k_sun_resolve, block-count scan, element sort)",
              "k_trace": "trace group (k_wf_first, k_wf_search, k_wf_shade, k_wf_finish)"}[dominant]
     roofline = {"bound": "fp64", "kernel": group, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
                 "scope": "per step: the group's launches of every batch, timed by CUDA events around them",

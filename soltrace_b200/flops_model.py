@@ -15,9 +15,10 @@ candidate-element test per ray-stage (culling overhead is not work):
   back-transforms element -> stage -> global                       66
   absorption test                                                   1
 
-Bytes: the probe writes one 4-byte element word per sun ray and the compaction
-re-reads it; every first-stage hit moves 12 bytes (sun index + element) into the
-hit list and the trace kernel reads them back.  Scene tables are L2-resident.
+Bytes: the probe marks every sun ray in a hit mask (one bit, written and read back
+for the ray numbers); every first-stage hit moves 16 bytes (sun index, element, ray
+rank) into the sorted hit list and the trace kernel reads them back.  Scene tables
+are L2-resident.
 """
 
 GEN, XFORM, FLAT, QUAD, BOOK, SUNSHAPE, SLOPE, REFLECT, BACK, ABSORB = 72, 33, 84, 110, 33, 50, 100, 17, 66, 1
@@ -30,8 +31,8 @@ TRACE_FLOPS_PER_HIT = XFORM + FLAT + BOOK + ABSORB + SUNSHAPE + SLOPE + REFLECT 
 # a ray entering the receiver stage: transform, cylinder test, bookkeeping, absorption
 TRACE_FLOPS_PER_RECEIVER_ENTRY = XFORM + QUAD + BOOK + ABSORB
 
-PROBE_BYTES_PER_SUN_RAY = 4 + 4
-HIT_LIST_BYTES_PER_HIT = 12 + 12
+PROBE_BYTES_PER_SUN_RAY = 0.25
+HIT_LIST_BYTES_PER_HIT = 16 + 16
 
 # Nominal vector peaks of a B200 (148 SMs at 1965 MHz; 64 FP64 and 128 FP32 lanes
 # per SM, 2 flops per FMA).  The pool's measured peaks cover HBM copy bandwidth and
@@ -49,8 +50,8 @@ def trace_flops(hits: int, receiver_entries: int) -> float:
 
 
 def probe_bytes(sun_rays: int, hits: int) -> float:
-    return float(sun_rays) * PROBE_BYTES_PER_SUN_RAY + float(hits) * 12
+    return float(sun_rays) * PROBE_BYTES_PER_SUN_RAY + float(hits) * 16
 
 
 def trace_bytes(hits: int) -> float:
-    return float(hits) * 12
+    return float(hits) * 16
