@@ -1280,6 +1280,9 @@ __device__ __forceinline__ int wf_shade(const SceneDev &S, const TraceOut &O, Wf
 // First kernel: the batch's numbered rays (hit-list entries below the cut-off at the
 // requested hit count; k_advance applies the same rule after the trace) enter the first
 // stage and are shaded on the element the probe found.
+// FLAT 1: the first stage holds flat elements only; 2: besides, its search kind is
+// kSearchFlat, and the rays it reflects are searched for blocking in this kernel (their
+// results go to round 0's shade queue and to the search queue of the ray's stage).
 template <int MIXED, int RECORDS, int FLAT>
 __global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kWfShadeMinBlocks) k_wf_first(
     const __grid_constant__ SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx, const uint32_t *total,
@@ -1321,17 +1324,19 @@ __global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kW
                 r.moved = true;
             }
         }
-        int kb = -1;
+        int kb = -1, status = kWfDone;
         if (live) {
             wf_stage_enter(c, 0, r.raynum);
             // (an entry without a known element is searched in the first round)
-            const int status = (r.next_j >= 0) ? wf_shade<MIXED, RECORDS, FLAT>(S, O, c, r) : int(kWfSearch);
+            status = (r.next_j >= 0) ? wf_shade<MIXED, RECORDS, FLAT ? 1 : 0>(S, O, c, r) : int(kWfSearch);
+            // FLAT 2: the ray still in the first stage is searched here (its blocking search)
+            if (FLAT == 2 && status == kWfSearch && r.si == 0) status = wf_search<MIXED, RECORDS, kSearchFlat>(S, O, c, r);
             if (status != kWfDone) {
                 wf_store(W, i, r, true);
-                kb = Q.stage_queue[r.si];
+                if (status == kWfSearch) kb = Q.stage_queue[r.si];
             }
         }
-        wf_block_push(psh, nullptr, nullptr, false, Q.search[0], Q.cap, Q.counts, kb, i);
+        wf_block_push(psh, Q.shade, Q.counts + Q.n_queues, status == kWfShade, Q.search[0], Q.cap, Q.counts, kb, i);
     }
     wf_ctr_flush(c, S, O);
 }
@@ -1485,9 +1490,11 @@ static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t 
                      const uint32_t *total, const RunState *rs, const TraceOut &O, const WfState &W,
                      const WfQueues &Q, const ReplayIn *replay, cudaStream_t st) {
     // persistent grids: every block the kernels can keep resident on every SM
-    static int per_sm[4] = {0, 0, 0, 0};
+    static int per_sm[6] = {0, 0, 0, 0, 0, 0};
     if (per_sm[0] == 0) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_wf_first<MIXED, RECORDS, 0>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[4], k_wf_first<MIXED, RECORDS, 1>, kTraceBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[5], k_wf_first<MIXED, RECORDS, 2>, kTraceBlock, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_wf_shade<MIXED, RECORDS, 0>, kTraceBlock, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[3], k_wf_shade<MIXED, RECORDS, 1>, kTraceBlock, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_wf_finish<MIXED, RECORDS>, kTraceBlock, 0);
@@ -1503,8 +1510,11 @@ static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t 
     cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * (R + 1) * (nq + 1), st);
     if (replay)
         k_wf_replay<MIXED, RECORDS><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, O, W, *replay, Q);
-    else if (S.stages[0].flat_only)  // a first stage of flat elements only (heliostat fields)
-        k_wf_first<MIXED, RECORDS, 1><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs,
+    else if (stage_search_kind(S.stages[0]) == kSearchFlat)  // heliostat fields: blocking search fused
+        k_wf_first<MIXED, RECORDS, 2><<<sms * per_sm[5], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs,
+                                                                                 O, W, Q);
+    else if (S.stages[0].flat_only)  // a first stage of flat elements only
+        k_wf_first<MIXED, RECORDS, 1><<<sms * per_sm[4], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs,
                                                                                  O, W, Q);
     else
         k_wf_first<MIXED, RECORDS, 0><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs,
