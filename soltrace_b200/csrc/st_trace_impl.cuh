@@ -809,14 +809,21 @@ __global__ void __launch_bounds__(kProbeBlock) k_compact(uint64_t s0, uint32_t n
 // streams, integer flux atomics, records ordered by ray number).
 
 // rank of the hit on ray i among the batch's hits in ray order: the hits of the kProbeBlock
-// rays before its block, then those of the block's mask words before its own
-__device__ __forceinline__ uint32_t hit_rank(const uint32_t *offsets, const uint32_t *mask, uint32_t i) {
+// rays before its block (off), then those of the block's mask words (a, b) before its own
+struct RankIn {
+    uint32_t off;
+    uint4 a, b;
+};
+__device__ __forceinline__ RankIn rank_load(const uint32_t *offsets, const uint32_t *mask, uint32_t i) {
     static_assert(kProbeBlock == 256, "eight mask words per count slot");
-    const uint32_t blk = i / kProbeBlock, w = (i / 32) % 8;
+    const uint32_t blk = i / kProbeBlock;
     const uint4 *m4 = reinterpret_cast<const uint4 *>(mask + size_t(blk) * 8);
-    const uint4 a = m4[0], b = m4[1];
-    const uint32_t words[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
-    uint32_t r = offsets[blk];
+    return RankIn{offsets[blk], m4[0], m4[1]};
+}
+__device__ __forceinline__ uint32_t rank_of(const RankIn &q, uint32_t i) {
+    const uint32_t w = (i / 32) % 8;
+    const uint32_t words[8] = {q.a.x, q.a.y, q.a.z, q.a.w, q.b.x, q.b.y, q.b.z, q.b.w};
+    uint32_t r = q.off;
 #pragma unroll
     for (uint32_t k = 0; k < 8; ++k) {
         if (k < w) r += __popc(words[k]);
@@ -834,10 +841,9 @@ __device__ __forceinline__ uint32_t batch_take(const RunState *rs, const uint32_
 }
 
 // one sorted hit: sun-ray index, element, rank; the last numbered one marks the cut-off
-__device__ __forceinline__ void list_put(uint64_t s0, uint32_t ray, uint32_t e, uint32_t pos, const uint32_t *offsets,
-                                         const uint32_t *mask, uint32_t take, RunState *rs, uint64_t *s_sid,
-                                         uint32_t *s_el, uint32_t *s_idx) {
-    const uint32_t rank = hit_rank(offsets, mask, ray);
+__device__ __forceinline__ void list_put(uint64_t s0, uint32_t ray, uint32_t e, uint32_t pos, uint32_t rank,
+                                         uint32_t take, RunState *rs, uint64_t *s_sid, uint32_t *s_el,
+                                         uint32_t *s_idx) {
     s_sid[pos] = s0 + ray;
     s_el[pos] = e;
     s_idx[pos] = rank;
@@ -861,7 +867,9 @@ __global__ void __launch_bounds__(256) k_list_scatter(uint64_t s0, ProbeOut o, c
         const uint32_t h = o.cand_el[i];
         if (!h) continue;
         const uint32_t pos = atomicAdd(&elem_cursor[h - 1], 1u);
-        list_put(s0, o.cand[i], h - 1, pos, offsets, o.hit_mask, take, rs, s_sid, s_el, s_idx);
+        const uint32_t ray = o.cand[i];
+        list_put(s0, ray, h - 1, pos, rank_of(rank_load(offsets, o.hit_mask, ray), ray), take, rs, s_sid, s_el,
+                 s_idx);
     }
 }
 
@@ -873,6 +881,21 @@ __global__ void __launch_bounds__(256) k_list_scatter(uint64_t s0, ProbeOut o, c
 // element present, instead of one per hit.
 constexpr int kSortBins = 11264;
 constexpr int kSortBlock = 1024;
+constexpr int kSortUnroll = 4;
+// count the elements of list entries [a, b) in h (kSortUnroll loads in flight per thread)
+__device__ __forceinline__ void list_count_sh(uint32_t *h, const uint32_t *cand_el, uint32_t a, uint32_t b) {
+    for (uint32_t i0 = a + threadIdx.x; i0 < b; i0 += kSortUnroll * kSortBlock) {
+        uint32_t x[kSortUnroll];
+#pragma unroll
+        for (int u = 0; u < kSortUnroll; ++u) {
+            const uint32_t i = i0 + u * kSortBlock;
+            x[u] = (i < b) ? cand_el[i] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kSortUnroll; ++u)
+            if (x[u]) atomicAdd(&h[x[u] - 1], 1u);
+    }
+}
 __global__ void __launch_bounds__(kSortBlock) k_list_hist_sh(const uint32_t *list_count, const uint32_t *cand_el,
                                                              uint32_t n_elem, uint32_t *elem_count) {
     __shared__ uint32_t h[kSortBins];
@@ -881,10 +904,7 @@ __global__ void __launch_bounds__(kSortBlock) k_list_hist_sh(const uint32_t *lis
     const uint32_t a = min(n, blockIdx.x * chunk), b = min(n, a + chunk);
     for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock) h[e] = 0;
     __syncthreads();
-    for (uint32_t i = a + threadIdx.x; i < b; i += kSortBlock) {
-        const uint32_t x = cand_el[i];
-        if (x) atomicAdd(&h[x - 1], 1u);
-    }
+    list_count_sh(h, cand_el, a, b);
     __syncthreads();
     for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock)
         if (h[e]) atomicAdd(&elem_count[e], h[e]);
@@ -900,19 +920,31 @@ __global__ void __launch_bounds__(kSortBlock) k_list_scatter_sh(uint64_t s0, Pro
     const uint32_t a = min(n, blockIdx.x * chunk), b = min(n, a + chunk);
     for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock) h[e] = 0;
     __syncthreads();
-    for (uint32_t i = a + threadIdx.x; i < b; i += kSortBlock) {
-        const uint32_t x = o.cand_el[i];
-        if (x) atomicAdd(&h[x - 1], 1u);
-    }
+    list_count_sh(h, o.cand_el, a, b);
     __syncthreads();
     for (uint32_t e = threadIdx.x; e < n_elem; e += kSortBlock)
         if (h[e]) h[e] = atomicAdd(&elem_cursor[e], h[e]);
     __syncthreads();
-    for (uint32_t i = a + threadIdx.x; i < b; i += kSortBlock) {
-        const uint32_t x = o.cand_el[i];
-        if (!x) continue;
-        const uint32_t pos = atomicAdd(&h[x - 1], 1u);
-        list_put(s0, o.cand[i], x - 1, pos, offsets, o.hit_mask, take, rs, s_sid, s_el, s_idx);
+    // kSortUnroll entries per thread and step, their loads issued before their uses
+    for (uint32_t i0 = a + threadIdx.x; i0 < b; i0 += kSortUnroll * kSortBlock) {
+        uint32_t x[kSortUnroll], ray[kSortUnroll];
+        RankIn q[kSortUnroll];
+#pragma unroll
+        for (int u = 0; u < kSortUnroll; ++u) {
+            const uint32_t i = i0 + u * kSortBlock;
+            x[u] = (i < b) ? o.cand_el[i] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kSortUnroll; ++u) ray[u] = x[u] ? o.cand[i0 + u * kSortBlock] : 0u;
+#pragma unroll
+        for (int u = 0; u < kSortUnroll; ++u)
+            if (x[u]) q[u] = rank_load(offsets, o.hit_mask, ray[u]);
+#pragma unroll
+        for (int u = 0; u < kSortUnroll; ++u) {
+            if (!x[u]) continue;
+            const uint32_t pos = atomicAdd(&h[x[u] - 1], 1u);
+            list_put(s0, ray[u], x[u] - 1, pos, rank_of(q[u], ray[u]), take, rs, s_sid, s_el, s_idx);
+        }
     }
 }
 
