@@ -292,7 +292,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, rq.device);
 
     const int nst = S.n_stages;
-    const uint64_t kMaxBatch = uint64_t(1) << 25;
+    const uint64_t kMaxBatch = uint64_t(1) << 26;
     DevBuf &d_acc = ws.acc, &d_ctr = ws.ctr, &d_rs = ws.rs, &d_rec_count = ws.rec_count, &d_offsets = ws.offsets,
            &d_total = ws.total, &d_recs = ws.recs;
     // the batch's hits are grouped by first-stage element (the rays of a warp then leave
