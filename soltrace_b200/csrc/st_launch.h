@@ -9,7 +9,7 @@ namespace stb {
 
 constexpr int kProbeBlock = 256;
 constexpr int kResolveBlock = 128;  // threads per block of the grid probe's element-test kernel
-constexpr int kCandPerThread = 4;   // sun rays per thread of the grid probe's pre-test kernel
+constexpr int kCandPerThread = 8;   // sun rays per thread of the grid probe's pre-test kernel
 constexpr int kCandRays = kProbeBlock * kCandPerThread;
 constexpr int kTraceBlock = 128;
 // register-budget variants of the probe and trace kernels (minimum resident blocks per
@@ -31,7 +31,7 @@ __host__ __device__ inline int stage_search_kind(const StageRec &st) {
 }
 constexpr int kWfBruteMinBlocks = 8;      // search kernels of stages tested element by element
 constexpr int kWfFlatSearchMinBlocks = 5;  // search kernels of flat-only stages
-constexpr int kWfFirstFlatMinBlocks = 5;   // first kernel on a flat-only first stage
+constexpr int kWfFirstFlatMinBlocks = 8;   // first kernel on a flat-only first stage
 constexpr int kWfClosedShadeMinBlocks = 4; // shade kernel of scenes with closed-form surfaces only
 
 enum RunFlags : unsigned {
