@@ -1421,9 +1421,18 @@ std::vector<double> saved_second_stage(std::vector<double> in, std::vector<doubl
 // and elements (with their surface data), the sun and the error switches.
 struct SigHash {
     uint64_t h = 1469598103934665603ull;
+    // FNV-1a over 8-byte words (then the tail bytes), each step followed by an xor-shift so
+    // that high bits feed back into the low ones
     void bytes(const void *p, size_t n) {
         const unsigned char *c = static_cast<const unsigned char *>(p);
-        for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
+        size_t i = 0;
+        for (; i + 8 <= n; i += 8) {
+            uint64_t w;
+            memcpy(&w, c + i, 8);
+            h = (h ^ w) * 1099511628211ull;
+            h ^= h >> 29;
+        }
+        for (; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
     }
     template <typename T>
     void pod(const T &v) {
