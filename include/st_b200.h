@@ -146,12 +146,18 @@ int st_b200_sim_run_replay(st_context_t pcxt, unsigned int seed, st_uint_t n0, c
  * hit_elem (room for n entries each); *n_hits receives the count.  The k-th listed
  * hit is the ray st_sim_run numbers k.  Arithmetic is FP64.
  *
+ * The call runs on the context's device (st_b200_set_device, default 0): hit_sid,
+ * hit_elem and `stream` must belong to that device; the caller's current device is
+ * restored before returning.  A context given explicit rays (st_b200_explicit_rays) is
+ * rejected with -1: the probe lists generated sun rays only.
+ *
  * Scene tables and scratch live in a 48 MiB static device array that every GPU
  * loading this library keeps until the process exits; n <= 4194304 and scenes whose
  * tables do not fit are rejected with -1 and a message.  The first call on a device
- * looks up the array's address (make that call before any stream capture).  Calls
- * share the array: calls that overlap on the GPU race.  `stream` is a cudaStream_t
- * (NULL: the legacy default stream); the call returns after the work completes. */
+ * looks up the array's address.  Every call copies its tables from host memory and
+ * waits for its work to finish, so the entry point must not be called while `stream`
+ * is being captured into a CUDA graph.  Calls share the array: calls that overlap on
+ * the GPU race.  `stream` is a cudaStream_t (NULL: the legacy default stream). */
 int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsigned long long s0, unsigned int n,
                           unsigned long long *hit_sid, unsigned int *hit_elem, unsigned int *n_hits, void *stream);
 

@@ -17,7 +17,8 @@
 //   * st_oracle_flux: integer flux bins from the element-local hit positions.
 //
 // Parity is pinned against the reference compiled from its own sources
-// (oracle/Makefile target "ref"): see tests/test_oracle_vs_reference.py.
+// (oracle/Makefile target "ref"): see tests/test_oracle.py and the digests in
+// tests/golden/reference_runs.json.
 #include <cmath>
 #include <cstdarg>
 #include <cstdint>

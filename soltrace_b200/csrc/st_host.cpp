@@ -107,10 +107,10 @@ struct Context {
     std::vector<double> stage_s0, stage_s1;  // saved: 8 doubles per stage-1 record, 7 per ray
     bool replaying = false;
     std::vector<double> replay_s0, replay_s1;
-    // the flattened scene of the last run and a signature of the inputs it was built from:
+    // the flattened scene of the last run and the exact key of the inputs it was built from:
     // a run whose inputs are unchanged reuses it (geometry set-up, grids and lists skipped)
     HostScene scene_cache;
-    uint64_t scene_sig = 0;
+    std::string scene_key;
     bool scene_valid = false;
     Workspace *ws = nullptr;     // device buffers reused by every run of this context
     ~Context() {
@@ -1417,23 +1417,14 @@ std::vector<double> saved_second_stage(std::vector<double> in, std::vector<doubl
     return s1;
 }
 
-// 64-bit FNV-1a signature of every input the flattened scene is built from: optics, stages
-// and elements (with their surface data), the sun and the error switches.
-struct SigHash {
-    uint64_t h = 1469598103934665603ull;
-    // FNV-1a over 8-byte words (then the tail bytes), each step followed by an xor-shift so
-    // that high bits feed back into the low ones
-    void bytes(const void *p, size_t n) {
-        const unsigned char *c = static_cast<const unsigned char *>(p);
-        size_t i = 0;
-        for (; i + 8 <= n; i += 8) {
-            uint64_t w;
-            memcpy(&w, c + i, 8);
-            h = (h ^ w) * 1099511628211ull;
-            h ^= h >> 29;
-        }
-        for (; i < n; ++i) h = (h ^ c[i]) * 1099511628211ull;
-    }
+// Exact key of every input the flattened scene is built from: optics, stages and elements
+// (with their surface data), the sun and the error switches, serialised byte for byte.  A
+// run reuses the cached scene only when the key equals the stored one, so no input change
+// can go unseen (a front end that re-sends an unchanged scene before every run, as
+// pysoltrace does, still reuses it).
+struct SceneKey {
+    std::string k;
+    void bytes(const void *p, size_t n) { k.append(static_cast<const char *>(p), n); }
     template <typename T>
     void pod(const T &v) {
         bytes(&v, sizeof v);
@@ -1448,8 +1439,9 @@ struct SigHash {
     }
 };
 
-uint64_t scene_signature(const Context *cx) {
-    SigHash g;
+std::string scene_key(const Context *cx) {
+    SceneKey g;
+    g.k.reserve(cx->scene_key.size() + 64);
     g.pod(cx->err_sun);
     g.pod(cx->err_opt);
     const SunM &s = cx->sun;
@@ -1518,7 +1510,7 @@ uint64_t scene_signature(const Context *cx) {
             g.str(e.optic);
         }
     }
-    return g.h;
+    return std::move(g.k);
 }
 
 int run(Context *cx, unsigned seed) {
@@ -1539,13 +1531,14 @@ int run(Context *cx, unsigned seed) {
         return -1;
     }
     const auto t0 = std::chrono::steady_clock::now();
-    if (!cx->scene_valid || cx->scene_sig != scene_signature(cx)) {
+    std::string key = scene_key(cx);
+    if (!cx->scene_valid || cx->scene_key != key) {
         cx->scene_valid = false;
         if (!init_geometries(cx)) return -1;
         cx->scene_cache = HostScene();
         if (!flatten(cx, cx->scene_cache)) return -1;
         // the set-up fills derived fields; the next run starts from this state
-        cx->scene_sig = scene_signature(cx);
+        cx->scene_key = scene_key(cx);
         cx->scene_valid = true;
     }
     const HostScene &hs = cx->scene_cache;
@@ -1685,6 +1678,14 @@ Context *C(st_context_t p) { return reinterpret_cast<Context *>(p); }
 }  // namespace
 
 namespace stb {
+bool context_device(void *ctx, int &device, bool &sun_rays) {
+    Context *cx = C(ctx);
+    if (!cx) return false;
+    device = cx->device;
+    sun_rays = cx->ex_pos.empty() && !cx->replaying;
+    return true;
+}
+
 // Geometry set-up and flattening of a context's scene for callers outside this file;
 // on failure the reason is appended to the context's messages and false is returned.
 bool prepare_scene(void *ctx, HostScene &hs) {

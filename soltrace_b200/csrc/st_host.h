@@ -84,5 +84,8 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
 // st_host.cpp: set up and flatten the scene of a context; append a message to it
 bool prepare_scene(void *ctx, HostScene &hs);
 void report(void *ctx, const std::string &msg);
+// the device a context runs on (st_b200_set_device), and whether its rays come from the sun
+// (false when it was given explicit rays or is replaying saved stage data)
+bool context_device(void *ctx, int &device, bool &sun_rays);
 
 }  // namespace stb

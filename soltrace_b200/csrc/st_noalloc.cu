@@ -63,6 +63,23 @@ struct Carve {
     }
 };
 
+// makes the context's device current for the call and restores the caller's on return
+struct DeviceScope {
+    int saved = -1;
+    cudaError_t enter(int device) {
+        cudaError_t e = cudaGetDevice(&saved);
+        if (e != cudaSuccess) {
+            saved = -1;
+            return e;
+        }
+        return saved == device ? cudaSuccess : cudaSetDevice(device);
+    }
+    ~DeviceScope() {
+        int now = -1;
+        if (saved >= 0 && cudaGetDevice(&now) == cudaSuccess && now != saved) cudaSetDevice(saved);
+    }
+};
+
 template <typename T>
 cudaError_t put(T *dst, const std::vector<T> &v, cudaStream_t st) {
     if (v.empty()) return cudaSuccess;
@@ -89,11 +106,25 @@ extern "C" int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsig
                          std::to_string(kNoAllocMaxRays) + " per call");
         return -1;
     }
+    int device = 0;
+    bool sun_rays = true;
+    if (!context_device(pcxt, device, sun_rays)) return -1;
+    if (!sun_rays) {
+        report(pcxt, "st_b200_probe_noalloc: the context traces explicit rays (st_b200_explicit_rays); "
+                     "the probe lists generated sun rays only");
+        return -1;
+    }
     HostScene hs;
     if (!prepare_scene(pcxt, hs)) return -1;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    DeviceScope scope;
+    cudaError_t e = scope.enter(device);
+    if (e != cudaSuccess) {
+        report(pcxt, std::string("st_b200_probe_noalloc: cannot use the context's device: ") + cudaGetErrorString(e));
+        return -1;
+    }
     unsigned char *scratch = nullptr;
-    cudaError_t e = scratch_on_current_device(&scratch);
+    e = scratch_on_current_device(&scratch);
     if (e != cudaSuccess) {
         report(pcxt, std::string("st_b200_probe_noalloc: no device scratch: ") + cudaGetErrorString(e));
         return -1;

@@ -89,3 +89,20 @@ def test_probe_noalloc_rejects_oversized_requests(product):
         assert "at most" in product.messages(ctx)[-1]
     finally:
         product.st_free_context(ctx)
+
+
+def test_probe_noalloc_rejects_explicit_ray_contexts(product):
+    """A context given explicit rays traces those rays, not sun rays: the probe refuses it
+    (before any device work) instead of listing sun rays st_sim_run would not trace."""
+    ctx = product.st_create_context()
+    try:
+        scenes.push(product, ctx, scenes.dish_scene(100))
+        pos = np.array([[0.0, 0.0, 4.0]])
+        cos = np.array([[0.0, 0.0, -1.0]])
+        product.explicit_rays(ctx, pos, cos)
+        nh = C.c_uint(7)
+        rc = _bind(product)(ctx, 1, 0, 1000, 16, 16, C.byref(nh), None)
+        assert rc == -1 and nh.value == 0
+        assert "explicit rays" in product.messages(ctx)[-1]
+    finally:
+        product.st_free_context(ctx)
