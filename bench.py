@@ -17,8 +17,10 @@ kernels, flux and counter readback into host arrays).
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Under torchrun (N > 1) every rank traces its own 1e8 hits with its own seed
-(weak scaling) and the receiver flux maps are summed with one NCCL all-reduce.
+Under torchrun (N > 1) the ranks make one st_sim_run of N x 1e8 hits together
+(st_b200_set_ranks: each traces a contiguous slice of every sun-ray batch; one NCCL
+all-gather of the ranks' hit counts per batch, one all-reduce of the counters and flux maps
+at the end), so the per-GPU work is fixed (weak scaling) and the results equal one GPU's.
 `--impl reference` times the reference coretrace (built from its sources into
 oracle/_ref/) on the host cores instead.
 """
@@ -60,16 +62,17 @@ def parse():
     p.add_argument("--seed", type=int, default=3)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extra", action="store_true", help="skip the other configurations' lines")
     return p.parse_args()
 
 
 def workload(args):
     return {"workload": f"heliostat field: {args.helios} flat 10x10 m heliostats, Buie CSR 0.1, "
                         f"8 m x 10 m cylindrical receiver, {args.hits:.0e} first-stage hits per step",
-            "heliostats": args.helios, "hits_per_step": args.hits, "receiver_flux_map": "100x100",
+            "heliostats": args.helios, "hits_per_step_per_gpu": args.hits, "receiver_flux_map": "100x100",
             "l2": "per-step working set > L2 (hit lists of up to 0.5 GB per sun-ray batch); "
                   "scene tables (~1 MB) stay L2-resident by design",
-            "parallelism": f"dp{args.gpus} (independent rays per GPU)"}
+            "parallelism": f"dp{args.gpus} (one run's sun-ray range split contiguously over the GPUs)"}
 
 
 # ---------------------------------------------------------------------------------------
@@ -173,6 +176,146 @@ def reference_sample(sc, seconds: float, seed: int):
                       f"{wall:.1f} s wall, st_sim_run only, polar receiver hash on)"}
 
 
+def reference_positions(scene_list, seconds: float, seed: int, label: str):
+    """The reference on all host cores, one context per thread, thread i tracing scene
+    i % len(scene_list) with seed seed + i*123; hits per thread sized from a calibration run
+    so that each thread works about `seconds`.  Times st_sim_run only; returns ray-stage/s."""
+    from soltrace_b200.capi import StApi
+    if not os.path.exists(REF_SO):
+        raise FileNotFoundError(REF_SO)
+    ref = StApi(REF_SO)
+    ncores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+
+    def one(sc, hits, s, out, idx, barrier=None):
+        ctx = ref.st_create_context()
+        scenes.push(ref, ctx, dataclasses.replace(sc, raycount=hits, raymax=2_000_000_000 - 1))
+        if barrier:
+            barrier.wait()
+        t0 = time.perf_counter()
+        n = ref.run(ctx, s)
+        dt = time.perf_counter() - t0
+        if n < 0:
+            raise RuntimeError("reference st_sim_run failed: " + "; ".join(ref.messages(ctx)))
+        ss = ref.sun_stats(ctx)
+        rec = ref.records(ctx)
+        ref.st_free_context(ctx)
+        later = sum(len(np.unique(rec["raynum"][rec["stage"] == k])) for k in range(2, 17)) if n > 0 else 0
+        out[idx] = (dt, ss["nsunrays"] + later, n)
+
+    probe = [None]
+    one(scene_list[0], 500, seed, probe, 0)
+    rate = probe[0][1] / max(probe[0][0], 1e-6)
+    hits_per_thread = max(500, int(rate * seconds / max(probe[0][1] / 500.0, 1e-9)))
+    res = [None] * ncores
+    bar = threading.Barrier(ncores)
+    th = [threading.Thread(target=one, args=(scene_list[i % len(scene_list)], hits_per_thread, seed + i * 123, res, i,
+                                             bar)) for i in range(ncores)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    wall = max(r[0] for r in res)
+    units = sum(r[1] for r in res)
+    return {"value": units / wall, "unit": UNIT, "cores": ncores, "kind": "reference",
+            "sample": f"{label}: {ncores} threads x {hits_per_thread} hits ({units} ray-stage units, {wall:.1f} s wall, "
+                      "st_sim_run only)"}
+
+
+def config_lines(api, args) -> dict:
+    """The other BASELINE configurations, each timed beside the reference on the host cores:
+    C1 dish (FP64, 1e6 hits, 50 x 50 absorber map), C2 trough (FP64 and mixed, 1e7 hits,
+    72 x 120 absorber-tube map), C4 batched annual beam-down trace (512 sun positions, tracking
+    field of 10,000 heliostats, 64 x 64 ground map, one st_b200_sim_run_batch call), and the
+    headline field with records on (1e7 hits, st_locations & co. read back: what pysoltrace
+    pays)."""
+    out = {}
+
+    def timed_runs(sc, maps, prec, seed, steps, records=False):
+        ctx = api.st_create_context()
+        scenes.push(api, ctx, sc)
+        api.st_b200_set_precision(ctx, prec)
+        api.st_b200_set_records(ctx, 1 if records else 0)
+        for m in maps:
+            api.st_b200_add_flux_map(ctx, *m)
+        api.run(ctx, seed)  # warm-up (scene set-up, autotuning)
+        units = dev = wall = 0.0
+        flux = None
+        for k in range(steps):
+            t0 = time.perf_counter()
+            rc = api.run(ctx, seed + 1 + k)
+            if records and rc > 0:
+                api.records(ctx)
+            wall += time.perf_counter() - t0
+            if rc < 0:
+                raise RuntimeError("; ".join(api.messages(ctx)))
+            st = api.stats(ctx)
+            units += st["ray_stage_units"]
+            dev += st["kernel_ms"] / 1e3
+            flux = [api.flux(ctx, i, m[3], m[4]) for i, m in enumerate(maps)]
+        api.st_free_context(ctx)
+        return {"value": units / dev, "e2e": units / wall, "ms_per_step": dev / steps * 1e3,
+                "units_per_step": units / steps}, flux
+
+    seconds = min(args.cpu_seconds, 8.0)
+    # C1: dish
+    dish = scenes.dish_scene(1_000_000)
+    c1, _ = timed_runs(dish, [(2, 1, 0, 50, 50, -0.25, 0.25, -0.25, 0.25, 1)], 0, 1, 3)
+    c1.update(workload="C1 parabolic dish + flat absorber, pillbox sun, 1e6 hits, 50x50 map", dtype="f64")
+    # C2: trough, FP64 and mixed
+    trough = scenes.trough_scene(10_000_000)
+    tmap = [(3, 2, 1, 72, 120, 0.0, 0.035, -6.0, 6.0, 1)]
+    c2, f64 = timed_runs(trough, tmap, 0, 2, 2)
+    c2m, fmx = timed_runs(trough, tmap, 1, 2, 2)
+    a, b = f64[0].astype(float), fmx[0].astype(float)
+    c2.update(workload="C2 parabolic trough + glass envelope + absorber tube, gaussian sun, 1e7 hits, 72x120 map",
+              dtype="f64", mixed={"value": c2m["value"], "ms_per_step": c2m["ms_per_step"],
+                                  "flux_l2_mixed_vs_fp64": float(np.linalg.norm(a - b) / max(np.linalg.norm(a), 1e-30))})
+    # headline field with records (pysoltrace's path)
+    fld = scenes.field_scene(args.helios, 10_000_000)
+    rec, _ = timed_runs(fld, [FLUX_MAP], 1, 5, 2, records=True)
+    rec.update(workload="C3 field, 1e7 hits, records on and read back (st_locations, st_cosines, st_elementmap, "
+                        "st_stagemap, st_raynumbers)", dtype="fp32+fp64 (mixed)")
+    out["records_on_field_1e7"] = rec
+    # C4: batched annual beam-down trace
+    suns, hits, dni = scenes.annual_suns(512)
+    bd = scenes.beam_down_scene(10_000, raycount=1000)
+    ctx = api.st_create_context()
+    scenes.push(api, ctx, bd)
+    api.st_b200_set_precision(ctx, 1)
+    api.st_b200_add_flux_map(ctx, *scenes.GROUND_MAP)
+    tgt = scenes.beam_down_target()
+    api.run_batch(ctx, 100, suns[:8], hits[:8] // 10, tgt)  # warm-up
+    t0 = time.perf_counter()
+    rc = api.run_batch(ctx, 100, suns, hits, tgt)
+    wall = time.perf_counter() - t0
+    if rc < 0:
+        raise RuntimeError("; ".join(api.messages(ctx)))
+    tot = api.batch_stats(ctx, -1)
+    intercept = []
+    for k in range(len(hits)):
+        g = api.batch_flux(ctx, 0, k, scenes.GROUND_MAP[3], scenes.GROUND_MAP[4])
+        intercept.append(float(g.sum()) / max(hits[k], 1))
+    api.st_free_context(ctx)
+    c4 = {"value": tot["ray_stage_units"] / (tot["kernel_ms"] / 1e3), "e2e": tot["ray_stage_units"] / wall,
+          "unit": UNIT, "positions": len(hits), "hits": int(hits.sum()), "sun_rays": tot["sun_rays"],
+          "device_ms": tot["kernel_ms"], "wall_ms": wall * 1e3, "host_setup_ms": tot["setup_ms"],
+          "gpu_launches": tot["gpu_launches"], "h2d_bytes": tot["h2d_bytes"],
+          "mean_ground_intercept_per_hit": float(np.mean(intercept)), "dtype": "fp32+fp64 (mixed)",
+          "workload": "C4 beam-down: 10,000 tracking heliostats, hyperboloid secondary (e 1.3) with torus lip, "
+                      "64x64 ground receiver; 512 sun positions at 40 N, 1e6 x DNI/1000 hits each"}
+    if not args.no_cpu_baseline:
+        for name, line, sc_list in (("C1", c1, [dish]), ("C2", c2, [trough]),
+                                    ("C4", c4, [scenes.beam_down_scene(10_000, raycount=1000, sun_xyz=suns[k])
+                                                for k in range(16)])):
+            try:
+                line["reference"] = reference_positions(sc_list, seconds, 7, name)
+                line["vs_reference"] = line["value"] / line["reference"]["value"]
+            except Exception as ex:  # noqa: BLE001
+                line["reference"] = {"unavailable": str(ex)}
+    out["C1_dish"], out["C2_trough"], out["C4_batch"] = c1, c2, c4
+    return out
+
+
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -234,12 +377,22 @@ def main():
 
     from soltrace_b200.lib import load
     api = load()
-    sc = scenes.field_scene(args.helios, args.hits)
+    # weak scaling: the run numbers args.hits first-stage hits per GPU; over N GPUs it is one
+    # st_sim_run of N x args.hits hits split over the ranks (st_b200_set_ranks), with the
+    # results of that run on one GPU
+    sc = scenes.field_scene(args.helios, args.hits * world)
     ctx = api.st_create_context()
     scenes.push(api, ctx, sc)
     api.st_b200_set_device(ctx, local if world > 1 else 0)
     api.st_b200_set_records(ctx, 0)
     api.st_b200_add_flux_map(ctx, *FLUX_MAP)
+    if api.has("st_b200_set_max_sun_rays"):
+        api.st_b200_set_max_sun_rays(ctx, 40 * args.hits * world)  # beyond st_sim_params' int cap
+    exchange = None
+    if world > 1:
+        exchange = parallel.RankExchange(device="cuda")
+        if exchange.attach(api, ctx) != 1:
+            raise RuntimeError("st_b200_set_ranks failed: " + "; ".join(api.messages(ctx)))
 
     def step(prec, seed):
         api.st_b200_set_precision(ctx, prec)
@@ -253,7 +406,7 @@ def main():
         st["flux"] = api.flux(ctx, 0, FLUX_MAP[3], FLUX_MAP[4])
         return st
 
-    seed0 = parallel.rank_seed(args.seed, rank)
+    seed0 = args.seed  # every rank runs the same seed: the ranks share one run
     for k in range(args.warmup):
         step(1, seed0 + k)
 
@@ -283,10 +436,10 @@ def main():
     l2 = [float(np.linalg.norm(runs[k]["flux"].astype(float) - runs64[k]["flux"].astype(float)) /
                 max(np.linalg.norm(runs64[k]["flux"].astype(float)), 1e-30)) for k in range(n64)]
 
-    # whole-job totals: units summed, device and wall times max over ranks, the receiver
-    # flux maps of all ranks summed (one NCCL all-reduce each; no-ops on one rank)
-    units, dev_ms, wall_ms, flux_sum = parallel.combine(units, dev_ms, wall_ms, runs[-1]["flux"],
-                                                        device="cuda" if dist else "cpu")
+    # whole-job totals: the units are the run's (already over all ranks), device and wall
+    # times the max over ranks
+    units, dev_ms, wall_ms = parallel.combine(units, dev_ms, wall_ms, device="cuda" if dist else "cpu")
+    flux_sum = runs[-1]["flux"]
     if rank != 0:
         api.st_free_context(ctx)
         if dist:
@@ -343,6 +496,13 @@ def main():
         except Exception as ex:  # noqa: BLE001
             cpu = {"value": None, "unavailable": str(ex)}
 
+    extra = None
+    if world == 1 and not args.no_extra:
+        try:
+            extra = config_lines(api, args)
+        except Exception as ex:  # noqa: BLE001
+            extra = {"error": str(ex)}
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": dev_ms / len(runs), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -356,8 +516,9 @@ def main():
         "autotuned_variants": {"probe": runs[-1]["probe_variant"], "trace": runs[-1]["trace_variant"],
                                "fp64_trace": runs64[-1]["trace_variant"]},
         "units_per_step": units / len(runs), "sun_rays_per_step": sun_rays / len(runs),
-        "receiver_flux_counts_all_ranks": int(flux_sum.sum()),
+        "receiver_flux_counts": int(flux_sum.sum()),
         "roofline": roofline, "clocks": clk.summary(), "cpu_baseline": cpu,
+        "other_configs": extra,
     }
     print(json.dumps(line), flush=True)
     api.st_free_context(ctx)

@@ -135,6 +135,61 @@ int st_b200_sim_run_replay(st_context_t pcxt, unsigned int seed, st_uint_t n0, c
                                            st_uint_t curstage, st_uint_t nstages, void *data),
                            void *cbdata);
 
+/* Cap on the sun rays a run may generate beyond the int of st_sim_params' maxcount
+ * (stapi.h:154), for runs of more than about 2^31 sun rays (large hit counts, runs over
+ * several GPUs); 0 (default) uses maxcount.  SunRayCount is then read from
+ * st_b200_run_stats, whose count is 64-bit (st_sun_stats reports an int). */
+int st_b200_set_max_sun_rays(st_context_t pcxt, unsigned long long n);
+
+/* One run over several GPUs, one process (or thread) per GPU, each with its own context
+ * holding the same scene, flux maps and settings.  No counterpart in the reference, whose
+ * front ends run independent contexts with seeds seed + i*123 and concatenate them
+ * (app/src/trace.cpp:709-735); here the ranks together make the one run st_sim_run makes
+ * on one GPU.  With nranks > 1, st_sim_run(seed) on rank r traces a contiguous slice of every
+ * sun-ray batch (every ray keeping its own random stream), numbers its hits after those of
+ * the ranks before it, and stops at the same hit as a single-GPU run; the counters, flux maps,
+ * per-element counts and SunRayCount it then reports are the whole run's, equal to a single-GPU
+ * run's, and its records (st_locations & co.) are the rays this rank traced, numbered as in
+ * the whole run.  Every rank must call st_sim_run with the same seed at the same time.
+ *   allgather(send[count] -> recv[count * nranks], rank-major) and allreduce(buf[count], op:
+ *   0 sum, 1 max) are the caller's collectives over the ranks (torch.distributed, MPI, NCCL);
+ *   they return 1 on success, 0 on failure, which fails the run.
+ * Explicit rays, replay and stage-data saving are single-GPU only.  nranks = 1 turns it off. */
+typedef int (*st_b200_allgather_t)(const unsigned long long *send, unsigned long long *recv, int count, void *user);
+typedef int (*st_b200_allreduce_t)(unsigned long long *buf, unsigned long long count, int op, void *user);
+int st_b200_set_ranks(st_context_t pcxt, int rank, int nranks, st_b200_allgather_t allgather,
+                      st_b200_allreduce_t allreduce, void *user);
+
+/* Batched multi-sun run: K sun positions traced over the context's scene in one launch
+ * sequence.  It stands in for K calls of st_sun_xyz + st_sim_run (coretrace/stapi.cpp:
+ * 680-734, one Trace per call) that a front end makes for an annual or daily simulation,
+ * whose sun vectors come from st_sun_position (stapi.cpp:500-527).
+ *   sun_xyz       3 K doubles: the sun position of each run, as st_sun_xyz takes it;
+ *   hits          K first-stage hit counts (each as st_sim_params' raycount; maxcount and
+ *                 include_dynamic_group come from st_sim_params and apply to every position);
+ *   track_target  NULL, or 3 doubles: every first-stage element then tracks the sun,
+ *                 re-aimed per position so that its normal bisects the sun direction and
+ *                 the direction from its origin to the target (aim point origin + 100 n,
+ *                 zrot kept), as a heliostat field aimed at a receiver.
+ * Position k draws from the random streams of seed + k: its counters, flux maps and
+ * SunRayCount are those of st_sim_run(seed + k) on the context with sun k (and the first
+ * stage aimed for sun k).  Precision and flux maps (st_b200_add_flux_map, kept per position)
+ * come from the context; records are not built.  The host reads the positions' progress
+ * once per wave (a few times per call), not once per position.  Returns 1, or -1 with the
+ * reason in st_message(). */
+int st_b200_sim_run_batch(st_context_t pcxt, unsigned int seed, int n_positions, const double *sun_xyz,
+                          const st_uint_t *hits, const double *track_target);
+/* Results of the last batched run.  position >= 0: that position's SunRayCount, hits, stage
+ * entries, ray-stage units and intersections; position -1: their sums with the call's device
+ * time, set-up time, launches and copies. */
+int st_b200_batch_stats(st_context_t pcxt, int position, st_b200_stats *out);
+/* nx*ny counts of flux map `map` for one position, row-major [iy][ix]. */
+int st_b200_batch_flux_counts(st_context_t pcxt, int map, int position, unsigned long long *counts);
+/* absorbed intersections per element of stage `stage` (1-based) for one position. */
+int st_b200_batch_absorbed(st_context_t pcxt, int position, int stage, unsigned long long *absorbed);
+/* the position's sun box in the sun frame (the power per ray is dni x box area / SunRayCount). */
+int st_b200_batch_sun_box(st_context_t pcxt, int position, double *xmin, double *xmax, double *ymin, double *ymax);
+
 /* First-stage probe without device allocation.  No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc: code running inside a framework that owns

@@ -8,6 +8,7 @@
 // and coretrace/suntoprimarystage.cpp, and then flattens everything into the
 // device tables of st_scene.h.
 #include <algorithm>
+#include <array>
 #include <cctype>
 #include <chrono>
 #include <cmath>
@@ -20,6 +21,7 @@
 #include <numeric>
 #include <string>
 #include <strings.h>
+#include <thread>
 #include <vector>
 
 #include "../../include/st_b200.h"
@@ -113,10 +115,24 @@ struct Context {
     std::string scene_key;
     bool scene_valid = false;
     Workspace *ws = nullptr;     // device buffers reused by every run of this context
+    // results of the last batched run (st_b200_sim_run_batch), per sun position
+    std::vector<PositionResult> batch;
+    std::vector<std::array<double, 4>> batch_box;  // sun box (xmin, xmax, ymin, ymax)
+    st_b200_stats batch_stats;
+    double sun_grid_cells = 4.0e6;  // cell budget of the sun-plane grid
+    uint64_t max_sun64 = 0;  // st_b200_set_max_sun_rays: sun-ray cap beyond st_sim_params' int (0: unused)
+    // this context's place in a run over several GPUs (st_b200_set_ranks)
+    int rank = 0, nranks = 1;
+    int (*allgather)(const unsigned long long *, unsigned long long *, int, void *) = nullptr;
+    int (*allreduce)(unsigned long long *, unsigned long long, int, void *) = nullptr;
+    void *comm_user = nullptr;
     ~Context() {
         if (ws) workspace_destroy(ws);
     }
-    Context() { memset(&stats, 0, sizeof stats); }
+    Context() {
+        memset(&stats, 0, sizeof stats);
+        memset(&batch_stats, 0, sizeof batch_stats);
+    }
     void log(const char *fmt, ...) {
         char buf[513];
         va_list a;
@@ -774,6 +790,35 @@ void fe_table(const std::vector<double> &nodes, std::vector<double> &out) {
 constexpr double kBeamHalfAngle = 0.1;  // rad
 constexpr size_t kBeamMaxList = 256;
 
+// The first stage's folded sun maps (SceneDev::sun_fold): sun-plane point (xs, ys, -10000)
+// -> stage (generateray.cpp:151-159, whose stage -> global -> stage round trip is the
+// identity) -> element frame (mathproc.cpp:115-173), composed once per element.
+void build_sun_fold(Context *cx, HostScene &hs) {
+    hs.sun_fold.clear();
+    if (cx->sun.point_source || hs.dev.n_stages < 1) return;
+    const StageRec &sr = hs.dev.stages[0];
+    const SunDev &sd = hs.dev.sun;
+    hs.sun_fold.assign(size_t(sr.n_elem) * kFoldStride, 0.0);
+    const double ex[3] = {1.0, 0.0, 0.0}, ey[3] = {0.0, 1.0, 0.0}, ez[3] = {0.0, 0.0, 1.0},
+                 p0[3] = {0.0, 0.0, -10000.0};
+    for (int k = 0; k < sr.n_elem; ++k) {
+        const ElemRec &e = hs.elems[size_t(sr.first_elem + k)];
+        double *f = &hs.sun_fold[size_t(k) * kFoldStride];
+        double t[3];
+        mulvt(sd.Rsun, ex, t);
+        mulv(e.R, t, f + 0);
+        mulvt(sd.Rsun, ey, t);
+        mulv(e.R, t, f + 3);
+        mulvt(sd.Rsun, ez, t);
+        mulv(e.R, t, f + 9);
+        mulvt(sd.Rsun, p0, t);
+        for (int q = 0; q < 3; ++q) t[q] += sd.pos_sun_stage[q] - e.o[q];
+        mulv(e.R, t, f + 6);
+        for (int q = 0; q < 3; ++q) f[6 + q] += 1.0e-5 * f[9 + q];
+        f[12] = 1.0 / (f[11] + 0.00000000001);
+    }
+}
+
 void build_beam_lists(Context *cx, HostScene &hs) {
     const size_t ne = hs.elems.size();
     hs.beam_axis.assign(ne, float4{0.f, 0.f, 0.f, 2.f});
@@ -1099,8 +1144,8 @@ bool sun_setup(Context *cx, HostScene &hs) {
         if (bounded && rmax > 0) {
             const double W = sun.xmax - sun.xmin, H = sun.ymax - sun.ymin;
             double cell = std::max(rmax * 0.5, 1e-6);
-            // keep the grid within ~4M cells
-            while ((W / cell + 1) * (H / cell + 1) > 4.0e6) cell *= 1.5;
+            // keep the grid within the context's cell budget (~4M cells for a single run)
+            while ((W / cell + 1) * (H / cell + 1) > cx->sun_grid_cells) cell *= 1.5;
             const int nx = std::max(1, int(ceil(W / cell))), ny = std::max(1, int(ceil(H / cell)));
             std::vector<std::vector<int>> cells(size_t(nx) * ny);
             for (size_t j = 0; j < st.elems.size(); ++j) {
@@ -1318,6 +1363,7 @@ bool flatten(Context *cx, HostScene &hs) {
     }
     if (!sun_setup(cx, hs)) return false;
     build_beam_lists(cx, hs);
+    build_sun_fold(cx, hs);
     hs.dev.sunshape_on = cx->err_sun;
     hs.dev.errors_on = cx->err_opt;
     return true;
@@ -1513,6 +1559,21 @@ std::string scene_key(const Context *cx) {
     return std::move(g.k);
 }
 
+// the flattened scene of the context's current inputs (rebuilt only when they changed)
+bool ensure_scene(Context *cx) {
+    std::string key = scene_key(cx);
+    if (!cx->scene_valid || cx->scene_key != key) {
+        cx->scene_valid = false;
+        if (!init_geometries(cx)) return false;
+        cx->scene_cache = HostScene();
+        if (!flatten(cx, cx->scene_cache)) return false;
+        // the set-up fills derived fields; the next run starts from this state
+        cx->scene_key = scene_key(cx);
+        cx->scene_valid = true;
+    }
+    return true;
+}
+
 int run(Context *cx, unsigned seed) {
     cx->records.clear();
     memset(&cx->stats, 0, sizeof cx->stats);
@@ -1531,20 +1592,11 @@ int run(Context *cx, unsigned seed) {
         return -1;
     }
     const auto t0 = std::chrono::steady_clock::now();
-    std::string key = scene_key(cx);
-    if (!cx->scene_valid || cx->scene_key != key) {
-        cx->scene_valid = false;
-        if (!init_geometries(cx)) return -1;
-        cx->scene_cache = HostScene();
-        if (!flatten(cx, cx->scene_cache)) return -1;
-        // the set-up fills derived fields; the next run starts from this state
-        cx->scene_key = scene_key(cx);
-        cx->scene_valid = true;
-    }
+    if (!ensure_scene(cx)) return -1;
     const HostScene &hs = cx->scene_cache;
     RunRequest rq;
     rq.n_hits = uint64_t(cx->raycount);
-    rq.max_sun = uint64_t(std::max(cx->raymax, 0));
+    rq.max_sun = cx->max_sun64 ? cx->max_sun64 : uint64_t(std::max(cx->raymax, 0));
     rq.seed = seed;
     rq.precision = cx->precision;
     rq.records = cx->want_records;
@@ -1556,6 +1608,12 @@ int run(Context *cx, unsigned seed) {
     rq.cbdata = cx->cbdata;
     rq.hit_rate_hint = cx->last_hit_rate;
     rq.save_stage_data = cx->save_stage_data;
+    rq.rank = cx->rank;
+    rq.nranks = cx->nranks;
+    rq.allgather = cx->allgather;
+    rq.allreduce = cx->allreduce;
+    rq.comm_user = cx->comm_user;
+    if (cx->nranks > 1) rq.hit_rate_hint = 0.0;  // every rank must plan from the same numbers
     if (cx->replaying) {
         // rays enter stage 2 from the saved rows; each row's first first-stage element from
         // the saved stage-1 records of its ray number (the first one), for the per-element
@@ -1671,6 +1729,194 @@ int run(Context *cx, unsigned seed) {
     S.records = cx->records.size();
     S.intersections = cx->want_records ? uint64_t(cx->records.size()) : rr.intersections;
     return int(cx->records.size());
+}
+
+// Batched runs keep every position's sun-plane grid on the device at once (per chunk of
+// kBatchChunk positions), so their grids get a smaller cell budget than a single run's.
+constexpr double kBatchSunGridCells = 2.5e5;
+constexpr size_t kBatchChunk = 64;
+
+// The sun-dependent tables of one position of a batched run: the context's sun moved to
+// `sun_xyz` and, with `target`, every first-stage element re-aimed so that its normal bisects
+// the sun direction and the direction to the target (a heliostat tracking the sun; the aim
+// point is origin + 100 n, zrot kept, rotation by input.cpp:160-176).
+bool build_position(const Context *cx, const HostScene &hs, const double sun_xyz[3], const double *target,
+                    SunPosition &out, std::string &err) {
+    Context c;
+    c.sun = cx->sun;
+    c.sun_grid_cells = kBatchSunGridCells;
+    for (int q = 0; q < 3; ++q) c.sun.origin[q] = sun_xyz[q];
+    c.err_sun = cx->err_sun;
+    c.err_opt = cx->err_opt;
+    c.stages.push_back(cx->stages[0]);
+    StageM &st0 = c.stages[0];
+    if (target) {
+        const double sn = sqrt(sq(sun_xyz[0]) + sq(sun_xyz[1]) + sq(sun_xyz[2]));
+        if (!(sn > 0)) {
+            err = "sun position at the origin";
+            return false;
+        }
+        const double s[3] = {sun_xyz[0] / sn, sun_xyz[1] / sn, sun_xyz[2] / sn};
+        for (Elem &e : st0.elems) {
+            double t[3] = {target[0] - e.origin[0], target[1] - e.origin[1], target[2] - e.origin[2]};
+            const double tn = sqrt(sq(t[0]) + sq(t[1]) + sq(t[2]));
+            double n[3];
+            for (int q = 0; q < 3; ++q) n[q] = s[q] + (tn > 0 ? t[q] / tn : 0.0);
+            const double nn = sqrt(sq(n[0]) + sq(n[1]) + sq(n[2]));
+            if (!(nn > 0)) {
+                err = "a tracking element cannot bisect the sun and target directions";
+                return false;
+            }
+            for (int q = 0; q < 3; ++q) e.aim[q] = e.origin[q] + 100.0 * (n[q] / nn);
+            double eu[3];
+            if (!euler_of(e.origin, e.aim, e.zrot, eu)) {
+                err = "a tracking element's geometry is not possible";
+                return false;
+            }
+            rot_from_euler(eu, e.R);
+        }
+    }
+    HostScene h;
+    h.dev = hs.dev;
+    if (!sun_setup(&c, h)) {
+        err = c.messages.empty() ? std::string("sun set-up failed") : c.messages.back();
+        return false;
+    }
+    out.sun = h.dev.sun;
+    out.cell_start.swap(h.cell_start);
+    out.cell_disc.swap(h.cell_disc);
+    out.cell_par.swap(h.cell_par);
+    if (target) {
+        out.elems = hs.elems;
+        const StageRec &sr = hs.dev.stages[0];
+        for (int k = 0; k < sr.n_elem; ++k)
+            for (int q = 0; q < 9; ++q) out.elems[size_t(sr.first_elem + k)].R[q] = st0.elems[size_t(k)].R[q];
+    }
+    h.elems = target ? out.elems : hs.elems;
+    build_sun_fold(&c, h);
+    out.sun_fold.swap(h.sun_fold);
+    return true;
+}
+
+int run_batch(Context *cx, unsigned seed, int n_pos, const double *sun_xyz, const st_uint_t *hits,
+              const double *target) {
+    cx->batch.clear();
+    cx->batch_box.clear();
+    memset(&cx->batch_stats, 0, sizeof cx->batch_stats);
+    if (n_pos < 1 || !sun_xyz || !hits) {
+        cx->log("st_b200_sim_run_batch: at least one sun position with its hit count is needed");
+        return -1;
+    }
+    if (!cx->ex_pos.empty()) {
+        cx->log("st_b200_sim_run_batch: the context traces explicit rays; batched runs trace sun rays");
+        return -1;
+    }
+    if (cx->stages.empty()) {
+        cx->log("no stages defined.");
+        return -1;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    if (!ensure_scene(cx)) return -1;
+    const HostScene &hs = cx->scene_cache;
+    const size_t np = static_cast<size_t>(n_pos);
+    RunRequest rq;
+    rq.max_sun = uint64_t(std::max(cx->raymax, 0));
+    rq.precision = cx->precision;
+    rq.device = cx->device;
+    for (auto &f : cx->flux) rq.flux.push_back(f.req);
+    // positions go to the device in chunks; the host builds the next chunk's tables while
+    // the device runs the current one
+    auto build_chunk = [cx, &hs, sun_xyz, hits, target, seed](size_t a, size_t b, std::vector<SunPosition> &pos,
+                                                               std::string &err) -> bool {
+        const size_t n = b - a;
+        pos.assign(n, SunPosition());
+        std::vector<std::string> errs(n);
+        std::vector<char> ok(n, 0);
+        const size_t nth = std::max<size_t>(1, std::min<size_t>(n, std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (size_t t = 0; t < nth; ++t)
+            th.emplace_back([&, t]() {
+                for (size_t i = t; i < n; i += nth) {
+                    const size_t p = a + i;
+                    ok[i] = build_position(cx, hs, sun_xyz + 3 * p, target, pos[i], errs[i]);
+                    pos[i].n_hits = uint64_t(hits[p]);
+                    pos[i].seed = seed + unsigned(p);
+                }
+            });
+        for (auto &x : th) x.join();
+        for (size_t i = 0; i < n; ++i)
+            if (!ok[i]) {
+                err = "sun position " + std::to_string(a + i) + ": " + errs[i];
+                return false;
+            }
+        return true;
+    };
+    if (!cx->ws) cx->ws = workspace_create();
+    double host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    BatchResult tot;
+    std::vector<SunPosition> cur, nxt;
+    std::string err, err_next;
+    const auto tb = std::chrono::steady_clock::now();
+    if (!build_chunk(0, std::min(np, kBatchChunk), cur, err)) {
+        cx->log("st_b200_sim_run_batch: %s", err.c_str());
+        return -1;
+    }
+    host_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
+    for (size_t a = 0; a < np; a += kBatchChunk) {
+        const size_t b = std::min(np, a + kBatchChunk);
+        bool next_ok = true;
+        std::thread builder;
+        if (b < np)
+            builder = std::thread([&]() { next_ok = build_chunk(b, std::min(np, b + kBatchChunk), nxt, err_next); });
+        BatchResult br;
+        const bool ran = gpu_run_batch(hs, cur, rq, br, *cx->ws);
+        if (builder.joinable()) builder.join();
+        if (!ran) {
+            cx->log("%s", br.error.c_str());
+            return -1;
+        }
+        if (!next_ok) {
+            cx->log("st_b200_sim_run_batch: %s", err_next.c_str());
+            return -1;
+        }
+        for (const SunPosition &sp : cur) cx->batch_box.push_back({sp.sun.xmin, sp.sun.xmax, sp.sun.ymin, sp.sun.ymax});
+        for (auto &r : br.pos) tot.pos.push_back(std::move(r));
+        tot.device_ms += br.device_ms;
+        tot.probe_ms += br.probe_ms;
+        tot.trace_ms += br.trace_ms;
+        tot.setup_ms += br.setup_ms;
+        tot.batches += br.batches;
+        tot.waves += br.waves;
+        tot.gpu_launches += br.gpu_launches;
+        tot.h2d_bytes += br.h2d_bytes;
+        tot.d2h_bytes += br.d2h_bytes;
+        tot.probe_variant = br.probe_variant;
+        cur.swap(nxt);
+        nxt.clear();
+    }
+    BatchResult &br = tot;
+    cx->batch.swap(br.pos);
+    st_b200_stats &S = cx->batch_stats;
+    for (const PositionResult &r : cx->batch) {
+        S.sun_rays += r.sun_rays;
+        S.ray_hits += r.ray_hits;
+        S.ray_stage_units += r.sun_rays;
+        for (size_t k = 0; k < r.stage_entries.size() && k < 16; ++k) {
+            S.stage_entries[k] += r.stage_entries[k];
+            if (k >= 1) S.ray_stage_units += r.stage_entries[k];
+        }
+        S.intersections += r.intersections;
+    }
+    S.kernel_ms = br.device_ms;
+    S.probe_ms = br.probe_ms;
+    S.trace_ms = br.trace_ms;
+    S.setup_ms = br.setup_ms + host_ms;
+    S.batches = br.batches;
+    S.gpu_launches = br.gpu_launches;
+    S.h2d_bytes = br.h2d_bytes;
+    S.d2h_bytes = br.d2h_bytes;
+    S.probe_variant = br.probe_variant;
+    return 1;
 }
 
 Context *C(st_context_t p) { return reinterpret_cast<Context *>(p); }
@@ -2345,6 +2591,79 @@ int st_b200_element_counts(st_context_t p, int stage, unsigned long long *first_
         if (absorbed) absorbed[i] = cx->elem_absorbed[s][i];
         if (delivered) delivered[i] = cx->elem_delivered[s][i];
     }
+    return 1;
+}
+
+int st_b200_set_max_sun_rays(st_context_t p, unsigned long long n) {
+    CTX(p, -1);
+    cx->max_sun64 = n;
+    return 1;
+}
+int st_b200_set_ranks(st_context_t p, int rank, int nranks, st_b200_allgather_t allgather,
+                      st_b200_allreduce_t allreduce, void *user) {
+    CTX(p, -1);
+    if (nranks < 1 || rank < 0 || rank >= nranks || (nranks > 1 && (!allgather || !allreduce))) {
+        cx->log("st_b200_set_ranks: rank must be in [0, nranks) and both exchange callbacks given for nranks > 1");
+        return -1;
+    }
+    cx->rank = rank;
+    cx->nranks = nranks;
+    cx->allgather = allgather;
+    cx->allreduce = allreduce;
+    cx->comm_user = user;
+    return 1;
+}
+int st_b200_sim_run_batch(st_context_t p, unsigned int seed, int n_positions, const double *sun_xyz,
+                          const st_uint_t *hits, const double *track_target) {
+    CTX(p, -1);
+    return run_batch(cx, seed, n_positions, sun_xyz, hits, track_target);
+}
+int st_b200_batch_stats(st_context_t p, int position, st_b200_stats *out) {
+    CTX(p, -1);
+    if (!out) return -1;
+    if (position < 0) {
+        *out = cx->batch_stats;
+        return 1;
+    }
+    if (size_t(position) >= cx->batch.size()) return -1;
+    const PositionResult &r = cx->batch[size_t(position)];
+    memset(out, 0, sizeof *out);
+    out->sun_rays = r.sun_rays;
+    out->ray_hits = r.ray_hits;
+    out->ray_stage_units = r.sun_rays;
+    for (size_t k = 0; k < r.stage_entries.size() && k < 16; ++k) {
+        out->stage_entries[k] = r.stage_entries[k];
+        if (k >= 1) out->ray_stage_units += r.stage_entries[k];
+    }
+    out->intersections = r.intersections;
+    return 1;
+}
+int st_b200_batch_flux_counts(st_context_t p, int map, int position, unsigned long long *counts) {
+    CTX(p, -1);
+    if (!counts || position < 0 || size_t(position) >= cx->batch.size()) return -1;
+    const PositionResult &r = cx->batch[size_t(position)];
+    if (map < 0 || size_t(map) >= r.flux.size()) return -1;
+    std::copy(r.flux[size_t(map)].begin(), r.flux[size_t(map)].end(), counts);
+    return 1;
+}
+int st_b200_batch_absorbed(st_context_t p, int position, int stage, unsigned long long *absorbed) {
+    CTX(p, -1);
+    if (!absorbed || position < 0 || size_t(position) >= cx->batch.size() || stage < 1 ||
+        size_t(stage) > cx->stages.size() || !cx->scene_valid)
+        return -1;
+    const StageRec &sr = cx->scene_cache.dev.stages[stage - 1];
+    const PositionResult &r = cx->batch[size_t(position)];
+    std::copy(r.absorbed.begin() + sr.first_elem, r.absorbed.begin() + sr.first_elem + sr.n_elem, absorbed);
+    return 1;
+}
+int st_b200_batch_sun_box(st_context_t p, int position, double *xmin, double *xmax, double *ymin, double *ymax) {
+    CTX(p, -1);
+    if (position < 0 || size_t(position) >= cx->batch_box.size()) return -1;
+    const auto &b = cx->batch_box[size_t(position)];
+    if (xmin) *xmin = b[0];
+    if (xmax) *xmax = b[1];
+    if (ymin) *ymin = b[2];
+    if (ymax) *ymax = b[3];
     return 1;
 }
 

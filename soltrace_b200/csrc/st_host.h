@@ -29,6 +29,7 @@ struct HostScene {
     std::vector<float4> cell_disc;  // sun-plane grid entries: disc centre x, y, radius, element
     std::vector<float4> cell_par;   // sun-plane grid entries: footprint parallelogram (dual basis rows)
     std::vector<double> inv_cdf;  // table-sunshape inverse CDF (kSunInvCells + 1 entries)
+    std::vector<double> sun_fold; // per first-stage element: sun plane -> element map (SceneDev::sun_fold)
     SceneDev dev;  // stages, sun scalars and flags; device pointers are filled by gpu_run
 };
 
@@ -54,6 +55,12 @@ struct RunRequest {
     std::vector<double> replay_rows;    // 7 doubles per ray: global position, direction, ray number
     std::vector<int> replay_fe0;        // per ray: global index of its first first-stage element, -1
     uint64_t replay_sun_rays = 0;       // SunRayCount of a replay (the last saved stage-1 ray number)
+    // one rank of a run split over several GPUs (st_b200_set_ranks): this rank traces its
+    // contiguous slice of every batch's sun-ray range and exchanges through the callbacks
+    int rank = 0, nranks = 1;
+    int (*allgather)(const unsigned long long *send, unsigned long long *recv, int count, void *user) = nullptr;
+    int (*allreduce)(unsigned long long *buf, unsigned long long count, int op, void *user) = nullptr;
+    void *comm_user = nullptr;
 };
 
 struct RunResult {
@@ -76,10 +83,46 @@ struct RunResult {
     int probe_variant = 0, trace_variant = 0;
 };
 
+// One sun position of a batched run (st_b200_sim_run_batch): the tables that depend on the
+// sun (sun frame and box, sun-plane grid, folded maps) and, when the first stage tracks the
+// sun, the scene's elements with the first stage re-aimed.
+struct SunPosition {
+    SunDev sun;                       // device pointers are filled by gpu_run_batch
+    std::vector<int> cell_start;
+    std::vector<float4> cell_disc, cell_par;
+    std::vector<ElemRec> elems;       // empty: the scene's elements
+    std::vector<double> sun_fold;
+    uint64_t n_hits = 0;
+    uint32_t seed = 0;
+};
+
+struct PositionResult {
+    uint64_t sun_rays = 0, ray_hits = 0, intersections = 0;
+    std::vector<uint64_t> stage_entries;
+    std::vector<uint32_t> max_enter;
+    std::vector<std::vector<unsigned long long>> flux;  // per flux map of the request
+    std::vector<unsigned long long> absorbed;           // per element of the scene
+};
+
+struct BatchResult {
+    bool ok = false;
+    std::string error;
+    std::vector<PositionResult> pos;
+    double device_ms = 0, probe_ms = 0, trace_ms = 0, setup_ms = 0;
+    int gpu_launches = 0, batches = 0, waves = 0;
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;
+    int probe_variant = 0;
+};
+
 struct Workspace;
 Workspace *workspace_create();
 void workspace_destroy(Workspace *w);
 bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspace &ws);
+// K sun positions over one scene in one launch sequence: every position's sun-ray batches
+// are queued without a host round trip, the host reading the positions' progress once per
+// wave.  rq supplies precision, device, flux maps and the sun-ray cap per position.
+bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, const RunRequest &rq, BatchResult &out,
+                   Workspace &ws);
 
 // st_host.cpp: set up and flatten the scene of a context; append a message to it
 bool prepare_scene(void *ctx, HostScene &hs);

@@ -16,6 +16,11 @@
 #include "st_host.h"
 #include "st_launch.h"
 
+// mixed precision on flat first stages takes the folded sun -> element maps
+#ifndef ST_SUN_FOLD
+#define ST_SUN_FOLD 1
+#endif
+
 namespace stb {
 
 namespace {
@@ -67,6 +72,9 @@ struct Workspace {
     DevBuf wf_sid, wf_raynum, wf_draw, wf_meta, wf_fe0, wf_p, wf_c, wf_q0, wf_q1, wf_qs, wf_counts;
     DevBuf save_rows[2], save_count, replay_rows, replay_fe0;  // stage-data save / replay
     DevBuf ecount, ecursor, etotal, s_sid, s_el, s_idx;
+    DevBuf sun_fold;
+    // batched runs: per-position sun tables, element copies, run states, counters, accumulators
+    DevBuf pos_cells, pos_disc, pos_par, pos_elems, pos_fold, pos_rs, pos_ctr, pos_acc;
     std::vector<cudaEvent_t> events;
     // autotuned kernel variants per precision (FP64, mixed), chosen on the first run
     struct Tuning {
@@ -249,6 +257,11 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     CK(upload(d_inv_cdf, hs.inv_cdf, st, out.h2d_bytes));
     CK(upload(d_expos, rq.ex_pos, st, out.h2d_bytes));
     CK(upload(d_excos, rq.ex_cos, st, out.h2d_bytes));
+    // mixed precision on a flat first stage culled by the sun-plane grid: the grid probe and
+    // the first trace kernel take the folded sun -> element maps
+    const bool fold = ST_SUN_FOLD && rq.precision && rq.ex_pos.empty() && !rq.replay && hs.dev.sun.grid_on &&
+                      !hs.dev.sun.point_source && hs.dev.stages[0].flat_only && !hs.sun_fold.empty();
+    if (fold) CK(upload(ws.sun_fold, hs.sun_fold, st, out.h2d_bytes));
 
     SceneDev S = hs.dev;
     S.elems = d_elems.as<ElemRec>();
@@ -275,6 +288,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     S.explicit_rays = explicit_mode ? 1 : 0;
     S.ex_pos = d_expos.as<double>();
     S.ex_cos = d_excos.as<double>();
+    S.sun_fold = fold ? ws.sun_fold.as<double>() : nullptr;
 
     // run-level accumulators: [first_hits | absorbed | delivered | flux bins of every map]
     const size_t ne = hs.elems.size();
@@ -293,6 +307,23 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
 
     const int nst = S.n_stages;
     const uint64_t kMaxBatch = uint64_t(1) << 26;
+    // one rank of a run over several GPUs: every batch's sun-ray range is split contiguously
+    // over the ranks; after the probe the ranks exchange their hit counts, so that each numbers
+    // its hits after the hits of the ranks before it and the run stops at the same hit as on
+    // one GPU (app/src/trace.cpp:709-735 is the reference's independent-context convention
+    // this replaces)
+    const bool multi = rq.nranks > 1;
+    const int R = multi ? rq.nranks : 1;
+    if (multi && (explicit_mode || rq.replay || rq.save_stage_data || !rq.allgather || !rq.allreduce ||
+                  rq.rank < 0 || rq.rank >= rq.nranks)) {
+        out.error = "runs over several ranks trace sun rays with both exchange callbacks set (no explicit rays, "
+                    "replay or stage-data saving)";
+        return false;
+    }
+    auto exchange = [&](const std::vector<unsigned long long> &send, std::vector<unsigned long long> &recv) -> bool {
+        recv.assign(send.size() * size_t(R), 0ull);
+        return rq.allgather(send.data(), recv.data(), int(send.size()), rq.comm_user) != 0;
+    };
     DevBuf &d_acc = ws.acc, &d_ctr = ws.ctr, &d_rs = ws.rs, &d_rec_count = ws.rec_count, &d_offsets = ws.offsets,
            &d_total = ws.total, &d_recs = ws.recs;
     // the batch's hits are grouped by first-stage element (the rays of a warp then leave
@@ -404,6 +435,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             return cudaSuccess;
         };
         uint64_t sun_next = 0;
+        uint64_t global_done = 0;  // over several ranks: hits numbered by all ranks so far
         double p_est = rq.hit_rate_hint > 0 ? rq.hit_rate_hint : 0.0;
         RunState rs = rs0;
         size_t ev_used = 0;
@@ -476,7 +508,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             if (explicit_mode) {
                 want = n_explicit - sun_next;
             } else {
-                const uint64_t need = rq.n_hits - rs.hits_done;
+                const uint64_t need = rq.n_hits - (multi ? global_done : rs.hits_done);
                 if (p_est <= 0.0)
                     want = std::min<uint64_t>(uint64_t(1) << 20, rq.max_sun - sun_next);  // pilot batch
                 else
@@ -493,10 +525,19 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             }
             uint64_t queued = 0;
             while (queued < want) {
-                const uint64_t n = std::min<uint64_t>(kMaxBatch, want - queued);
-                const uint32_t nb = uint32_t((n + kProbeBlock - 1) / kProbeBlock);
+                // this batch's global sun-ray range [sun_next, sun_next + n_all) and, over several
+                // ranks, this rank's contiguous slice [s0, s0 + n) of it
+                const uint64_t n_all = std::min<uint64_t>(kMaxBatch * uint64_t(R), want - queued);
+                uint64_t n = n_all, s0 = sun_next;
+                if (multi) {
+                    const uint64_t base = n_all / uint64_t(R), rem = n_all % uint64_t(R);
+                    const uint64_t rk = uint64_t(rq.rank);
+                    n = base + (rk < rem ? 1 : 0);
+                    s0 = sun_next + rk * base + std::min<uint64_t>(rk, rem);
+                }
+                const uint32_t nb = uint32_t((std::max<uint64_t>(n, 1) + kProbeBlock - 1) / kProbeBlock);
                 ProbeOut po;
-                CK(probe_buffers(ws, n, po));
+                CK(probe_buffers(ws, std::max<uint64_t>(n, 1), po));
                 CK(d_offsets.ensure(size_t(nb) * 4));
                 CK(ws.scan_parts.ensure(scan_parts(nb) * 4));
                 CK(d_total.ensure(8));
@@ -512,16 +553,52 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 O.rec_cap = rq.records ? rec_cap : 0;
                 cudaEvent_t p0 = new_event(), p1 = new_event(), p2 = new_event();
                 CK(cudaEventRecord(p0, st));
-                if (rq.precision)
-                    out.gpu_launches += launch_probe_mixed(S, sun_next, uint32_t(n), po, drs, tu.probe, st);
-                else
-                    out.gpu_launches += launch_probe_fp64(S, sun_next, uint32_t(n), po, drs, tu.probe, st);
-                launch_scan(po.block_counts, nb, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(),
-                            ws.scan_parts.as<uint32_t>(), st);
-                launch_list_sort(sun_next, po, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), drs, n_elem0,
-                                 d_ecount.as<uint32_t>(), d_ecursor.as<uint32_t>(), d_etotal.as<uint32_t>(),
-                                 d_s_sid.as<uint64_t>(), d_s_el.as<uint32_t>(), d_s_idx.as<uint32_t>(), uint32_t(n), st);
-                out.gpu_launches += 3;  // element counts, their scan, scatter
+                if (n > 0) {
+                    if (rq.precision)
+                        out.gpu_launches += launch_probe_mixed(S, s0, uint32_t(n), po, drs, tu.probe, st);
+                    else
+                        out.gpu_launches += launch_probe_fp64(S, s0, uint32_t(n), po, drs, tu.probe, st);
+                    launch_scan(po.block_counts, nb, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(),
+                                ws.scan_parts.as<uint32_t>(), st);
+                    out.gpu_launches += 2;
+                } else {
+                    CK(cudaMemsetAsync(d_total.p, 0, 8, st));
+                }
+                if (multi) {
+                    // every rank's hit count in this batch: this rank's hits are numbered after those of
+                    // the ranks before it, and the ranks after the run's last hit trace nothing
+                    uint32_t tot = 0;
+                    CK(cudaMemcpyAsync(&tot, d_total.p, 4, cudaMemcpyDeviceToHost, st));
+                    CK(cudaMemcpyAsync(&rs, drs, sizeof rs, cudaMemcpyDeviceToHost, st));
+                    CK(cudaStreamSynchronize(st));
+                    out.d2h_bytes += 4 + sizeof rs;
+                    std::vector<unsigned long long> got;
+                    if (!exchange({(unsigned long long)tot}, got)) {
+                        out.error = "the exchange of hit counts between ranks failed";
+                        return false;
+                    }
+                    uint64_t before = 0, all = 0;
+                    for (int k = 0; k < R; ++k) {
+                        if (k < rq.rank) before += got[size_t(k)];
+                        all += got[size_t(k)];
+                    }
+                    const uint64_t base = global_done + before;
+                    rs.target = rq.n_hits;
+                    rs.hits_done = std::min<uint64_t>(base, rq.n_hits);
+                    rs.reached = base >= rq.n_hits ? 1u : 0u;
+                    rs.cursor = 0;
+                    rs.cut_sid = 0;
+                    CK(cudaMemcpyAsync(drs, &rs, sizeof rs, cudaMemcpyHostToDevice, st));
+                    out.h2d_bytes += sizeof rs;
+                    global_done += std::min<uint64_t>(all, rq.n_hits - global_done);
+                }
+                if (n > 0) {
+                    launch_list_sort(s0, po, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), drs, n_elem0,
+                                     d_ecount.as<uint32_t>(), d_ecursor.as<uint32_t>(), d_etotal.as<uint32_t>(),
+                                     d_s_sid.as<uint64_t>(), d_s_el.as<uint32_t>(), d_s_idx.as<uint32_t>(),
+                                     uint32_t(n), st);
+                    out.gpu_launches += 3;  // element counts, their scan, scatter
+                }
                 const uint64_t *t_sid = d_s_sid.as<uint64_t>();
                 const uint32_t *t_el = d_s_el.as<uint32_t>(), *t_idx = d_s_idx.as<uint32_t>();
                 // trace state and queues: one slot per hit-list entry (at most n)
@@ -530,20 +607,24 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 CK(wf_buffers(ws, S, n, W, Q));
                 CK(save_setup(n));
                 CK(cudaEventRecord(p1, st));
-                if (rq.precision)
-                    out.gpu_launches += launch_trace_mixed(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(),
-                                                           drs, O, W, Q, nullptr, st);
-                else
-                    out.gpu_launches += launch_trace_fp64(rq.records, S, t_sid, t_el, t_idx, d_total.as<uint32_t>(),
-                                                          drs, O, W, Q, nullptr, st);
+                if (n > 0) {
+                    if (rq.precision)
+                        out.gpu_launches += launch_trace_mixed(rq.records, S, t_sid, t_el, t_idx,
+                                                               d_total.as<uint32_t>(), drs, O, W, Q, nullptr, st);
+                    else
+                        out.gpu_launches += launch_trace_fp64(rq.records, S, t_sid, t_el, t_idx,
+                                                              d_total.as<uint32_t>(), drs, O, W, Q, nullptr, st);
+                }
                 CK(cudaEventRecord(p2, st));
-                launch_advance(d_total.as<uint32_t>(), nullptr, sun_next, uint32_t(n), drs, st);
+                if (n > 0) {
+                    launch_advance(d_total.as<uint32_t>(), nullptr, s0, uint32_t(n), drs, st);
+                    out.gpu_launches += 1;
+                }
                 CK(cudaGetLastError());
-                out.gpu_launches += 3;  // scan (two kernels), advance
                 probe_ev.push_back({p0, p1});
                 trace_ev.push_back({p1, p2});
-                queued += n;
-                sun_next += n;
+                queued += n_all;
+                sun_next += n_all;
                 out.batches++;
                 if (sync_each) {
                     CK(cudaMemcpyAsync(&rs, drs, sizeof rs, cudaMemcpyDeviceToHost, st));
@@ -551,7 +632,20 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                     unsigned long long nrec = 0;
                     if (rq.records) CK(cudaMemcpyAsync(&nrec, d_rec_count.p, 8, cudaMemcpyDeviceToHost, st));
                     CK(cudaStreamSynchronize(st));
-                    if (rq.records && nrec > rec_cap) {
+                    bool overflow = rq.records && nrec > rec_cap;
+                    if (multi) {  // a rank out of record room makes every rank re-run, in step
+                        std::vector<unsigned long long> got;
+                        if (!exchange({overflow ? 1ull : 0ull, rec_cap, nrec}, got)) {
+                            out.error = "the exchange of record counts between ranks failed";
+                            return false;
+                        }
+                        for (int k = 0; k < R; ++k) {
+                            overflow = overflow || got[3 * size_t(k)] != 0;
+                            rec_cap = std::max<unsigned long long>(rec_cap, got[3 * size_t(k) + 1]);
+                            nrec = std::max<unsigned long long>(nrec, got[3 * size_t(k) + 2]);
+                        }
+                    }
+                    if (overflow) {
                         rec_cap = nrec + nrec / 4 + 4096;  // re-run the whole job with room for it
                         restart = true;
                         break;
@@ -580,15 +674,19 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                         done = true;
                         break;
                     }
-                    if (rs.reached) break;
+                    if (multi ? global_done == rq.n_hits : rs.reached != 0) break;
                 }
+                if (multi && global_done == rq.n_hits) break;
             }
             if (restart) break;
             CK(cudaMemcpyAsync(&rs, drs, sizeof rs, cudaMemcpyDeviceToHost, st));
             out.d2h_bytes += sizeof rs;
             CK(cudaStreamSynchronize(st));
-            if (rs.reached || out.cancelled || (explicit_mode && sun_next >= n_explicit)) done = true;
-            if (!explicit_mode && sun_next > 0) p_est = std::max(double(rs.hits_done) / double(sun_next), 1e-9);
+            const uint64_t done_hits = multi ? global_done : rs.hits_done;
+            if ((multi ? global_done == rq.n_hits : rs.reached != 0) || out.cancelled ||
+                (explicit_mode && sun_next >= n_explicit))
+                done = true;
+            if (!explicit_mode && sun_next > 0) p_est = std::max(double(done_hits) / double(sun_next), 1e-9);
         }
         if (restart) continue;
         CK(cudaEventRecord(t_last, st));
@@ -606,9 +704,9 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             cudaEventElapsedTime(&x, pe.first, pe.second);
             out.trace_ms += x;
         }
-        out.ray_hits = rs.hits_done;
+        out.ray_hits = multi ? global_done : rs.hits_done;
         out.sun_rays = explicit_mode ? n_explicit : rs.sun_rays;
-        if (!explicit_mode && !rs.reached && !out.cancelled) {
+        if (!explicit_mode && !(multi ? global_done == rq.n_hits : rs.reached != 0) && !out.cancelled) {
             out.error = "run ended before the requested hits were numbered";
             return false;
         }
@@ -619,6 +717,39 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
         if (acc_n) CK(cudaMemcpyAsync(accv.data(), d_acc.p, acc_n * 8, cudaMemcpyDeviceToHost, st));
         out.d2h_bytes += acc_n * 8 + sizeof c;
         CK(cudaStreamSynchronize(st));
+        unsigned fe_fail = rq.precision ? take_fe_failures_mixed() : take_fe_failures_fp64();
+        if (multi) {
+            // the run's totals over all ranks: counts summed, SunRayCount (the cutting rank's;
+            // the others' are below it), largest ray numbers and flags by max; integer, so exact
+            std::vector<unsigned long long> sum(kMaxStages + 1 + acc_n), mx(2 * kMaxStages + 2 + 32);
+            for (int k = 0; k < kMaxStages; ++k) sum[size_t(k)] = c.stage_entries[k];
+            sum[kMaxStages] = c.records;
+            std::copy(accv.begin(), accv.end(), sum.begin() + kMaxStages + 1);
+            for (int k = 0; k < kMaxStages; ++k) {
+                mx[size_t(k)] = c.max_enter[k];
+                mx[size_t(kMaxStages + k)] = c.max_ttmiss[k];
+            }
+            mx[2 * kMaxStages] = rs.sun_rays;
+            mx[2 * kMaxStages + 1] = fe_fail ? 1 : 0;
+            for (int b = 0; b < 32; ++b) mx[size_t(2 * kMaxStages + 2 + b)] = (c.flags >> b) & 1u;
+            if (!rq.allreduce(sum.data(), sum.size(), 0, rq.comm_user) ||
+                !rq.allreduce(mx.data(), mx.size(), 1, rq.comm_user)) {
+                out.error = "the reduction of the run's counters over ranks failed";
+                return false;
+            }
+            for (int k = 0; k < kMaxStages; ++k) c.stage_entries[k] = sum[size_t(k)];
+            c.records = sum[kMaxStages];
+            std::copy(sum.begin() + kMaxStages + 1, sum.end(), accv.begin());
+            for (int k = 0; k < kMaxStages; ++k) {
+                c.max_enter[k] = unsigned(mx[size_t(k)]);
+                c.max_ttmiss[k] = unsigned(mx[size_t(kMaxStages + k)]);
+            }
+            out.sun_rays = mx[2 * kMaxStages];
+            fe_fail = mx[2 * kMaxStages + 1] ? 1u : 0u;
+            c.flags = 0;
+            for (int b = 0; b < 32; ++b)
+                if (mx[size_t(2 * kMaxStages + 2 + b)]) c.flags |= 1u << b;
+        }
         for (int s = 0; s < nst; ++s) {
             out.stage_entries[s] = c.stage_entries[s];
             out.max_enter[s] = c.max_enter[s];
@@ -634,7 +765,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             out.flux.emplace_back(accv.begin() + flux_off[m],
                                   accv.begin() + flux_off[m] + size_t(rq.flux[m].nx) * rq.flux[m].ny);
         out.readback_ms += ms_since(tr);
-        if (rq.precision ? take_fe_failures_mixed() : take_fe_failures_fp64()) {
+        if (fe_fail) {
             // the reference throws at such a query (vshot.cpp:177-178) and returns no result
             out.error = "Interpolation failed to find nearby nodes to ray hit in FEA surface.";
             return false;
@@ -648,6 +779,345 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     }
     out.error = "record buffer could not be sized for this run";
     return false;
+}
+
+#undef CK
+#define CK(x)                                                                                 \
+    do {                                                                                      \
+        cudaError_t e_ = (x);                                                                 \
+        if (e_ != cudaSuccess) {                                                              \
+            out.error = std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #x;     \
+            return false;                                                                     \
+        }                                                                                     \
+    } while (0)
+
+// Batched run of K sun positions (st_b200_sim_run_batch).  Every position p has its own
+// scene view S_p (its sun frame, sun-plane grid, folded maps and, when tracking, elements),
+// run state, counters and accumulators; its rays draw from the streams of its own seed, so
+// position p's results are those of a single run with that sun and seed.  Positions advance
+// in waves: a wave queues, for every position still short of its hits, the sun rays its hit
+// rate (measured by the previous wave; the first wave probes 2^20 rays) says it needs, with
+// no host round trip inside the wave; the host then reads all positions' run states at once.
+bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, const RunRequest &rq, BatchResult &out,
+                   Workspace &ws) {
+    const auto t_setup = std::chrono::steady_clock::now();
+    const size_t K = pos.size();
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        out.error = "no CUDA device is available to the B200 trace";
+        return false;
+    }
+    if (rq.device < 0 || rq.device >= ndev) {
+        out.error = "CUDA device ordinal out of range";
+        return false;
+    }
+    if (K == 0) {
+        out.ok = true;
+        return true;
+    }
+    CK(cudaSetDevice(rq.device));
+    if (ws.device != rq.device) {
+        ws.~Workspace();
+        new (&ws) Workspace();
+        ws.device = rq.device;
+    }
+    if (!ws.stream) CK(cudaStreamCreateWithFlags(&ws.stream, cudaStreamNonBlocking));
+    cudaStream_t st = ws.stream;
+    uint64_t &h2d = out.h2d_bytes;
+    // the scene's shared tables
+    CK(upload(ws.elems, hs.elems, st, h2d));
+    CK(upload(ws.elem_sphere, hs.elem_sphere, st, h2d));
+    CK(upload(ws.stage_cells, hs.stage_cells, st, h2d));
+    CK(upload(ws.grid_sphere, hs.grid_sphere, st, h2d));
+    CK(upload(ws.grid_elem, hs.grid_elem, st, h2d));
+    CK(upload(ws.optics, hs.optics, st, h2d));
+    CK(upload(ws.surf, hs.surf_data, st, h2d));
+    CK(upload(ws.tables, hs.tables, st, h2d));
+    CK(upload(ws.bvh, hs.bvh, st, h2d));
+    CK(upload(ws.bvh_items, hs.bvh_items, st, h2d));
+    CK(upload(ws.inv_cdf, hs.inv_cdf, st, h2d));
+    // every position's tables, concatenated
+    std::vector<int> cells;
+    std::vector<float4> disc, par;
+    std::vector<ElemRec> pelems;
+    std::vector<double> pfold;
+    std::vector<size_t> off_cells(K), off_disc(K), off_elems(K), off_fold(K);
+    for (size_t p = 0; p < K; ++p) {
+        const SunPosition &sp = pos[p];
+        off_cells[p] = cells.size();
+        cells.insert(cells.end(), sp.cell_start.begin(), sp.cell_start.end());
+        off_disc[p] = disc.size();
+        disc.insert(disc.end(), sp.cell_disc.begin(), sp.cell_disc.end());
+        par.insert(par.end(), sp.cell_par.begin(), sp.cell_par.end());
+        off_elems[p] = sp.elems.empty() ? size_t(-1) : pelems.size();
+        pelems.insert(pelems.end(), sp.elems.begin(), sp.elems.end());
+        off_fold[p] = sp.sun_fold.empty() ? size_t(-1) : pfold.size();
+        pfold.insert(pfold.end(), sp.sun_fold.begin(), sp.sun_fold.end());
+    }
+    CK(upload(ws.pos_cells, cells, st, h2d));
+    CK(upload(ws.pos_disc, disc, st, h2d));
+    CK(upload(ws.pos_par, par, st, h2d));
+    CK(upload(ws.pos_elems, pelems, st, h2d));
+    CK(upload(ws.pos_fold, pfold, st, h2d));
+
+    SceneDev S0 = hs.dev;
+    S0.elems = ws.elems.as<ElemRec>();
+    S0.elem_sphere = ws.elem_sphere.as<float4>();
+    S0.stage_cells = ws.stage_cells.as<int2>();
+    S0.grid_sphere = ws.grid_sphere.as<float4>();
+    S0.grid_elem = ws.grid_elem.as<int>();
+    S0.beam_axis = nullptr;  // outgoing-beam lists depend on the sun: blocking searches walk the ground grid
+    S0.beam_range = nullptr;
+    S0.beam_elem = nullptr;
+    S0.optics = ws.optics.as<OpticRec>();
+    S0.surf_data = ws.surf.as<double>();
+    S0.tables = ws.tables.as<double>();
+    S0.bvh = ws.bvh.as<BvhNode>();
+    S0.bvh_items = ws.bvh_items.as<int>();
+    S0.precision = rq.precision;
+    S0.explicit_rays = 0;
+    S0.ex_pos = S0.ex_cos = nullptr;
+    S0.sun_fold = nullptr;
+
+    const int nst = S0.n_stages;
+    const size_t ne = hs.elems.size();
+    std::vector<size_t> flux_off;
+    size_t acc_n = 3 * ne;
+    for (const auto &f : rq.flux) {
+        flux_off.push_back(acc_n);
+        acc_n += size_t(f.nx) * f.ny;
+    }
+    if (rq.flux.size() > size_t(kMaxFluxMaps)) {
+        out.error = "too many flux maps";
+        return false;
+    }
+    CK(ws.pos_rs.ensure(K * sizeof(RunState)));
+    CK(ws.pos_ctr.ensure(K * sizeof(RunCounters)));
+    CK(ws.pos_acc.ensure(K * acc_n * 8 + 8));
+    CK(cudaMemsetAsync(ws.pos_ctr.p, 0, K * sizeof(RunCounters), st));
+    CK(cudaMemsetAsync(ws.pos_acc.p, 0, K * acc_n * 8 + 8, st));
+    std::vector<RunState> rs_h(K);
+    for (size_t p = 0; p < K; ++p) {
+        memset(&rs_h[p], 0, sizeof(RunState));
+        rs_h[p].target = pos[p].n_hits;
+    }
+    CK(cudaMemcpyAsync(ws.pos_rs.p, rs_h.data(), K * sizeof(RunState), cudaMemcpyHostToDevice, st));
+    h2d += K * sizeof(RunState);
+
+    std::vector<SceneDev> Sp(K, S0);
+    std::vector<TraceOut> Op(K);
+    unsigned long long *acc = ws.pos_acc.as<unsigned long long>();
+    for (size_t p = 0; p < K; ++p) {
+        SceneDev &S = Sp[p];
+        S.sun = pos[p].sun;
+        S.sun.cell_start = ws.pos_cells.as<int>() + off_cells[p];
+        S.sun.cell_disc = ws.pos_disc.as<float4>() + off_disc[p];
+        S.sun.cell_par = ws.pos_par.as<float4>() + off_disc[p];
+        S.sun.inv_cdf = hs.inv_cdf.empty() ? nullptr : ws.inv_cdf.as<double>();
+        if (off_elems[p] != size_t(-1)) S.elems = ws.pos_elems.as<ElemRec>() + off_elems[p];
+        // the folded maps serve mixed-precision runs on flat first stages culled by the grid
+        if (ST_SUN_FOLD && rq.precision && off_fold[p] != size_t(-1) && S.sun.grid_on && !S.sun.point_source &&
+            S.stages[0].flat_only)
+            S.sun_fold = ws.pos_fold.as<double>() + off_fold[p];
+        S.seed = pos[p].seed;
+        unsigned long long *a = acc + p * acc_n;
+        S.n_flux = int(rq.flux.size());
+        for (size_t m = 0; m < rq.flux.size(); ++m) {
+            const FluxMapReq &f = rq.flux[m];
+            FluxMapDev &fd = S.flux[m];
+            fd.stage = f.stage;
+            fd.elem = f.elem;
+            fd.kind = f.kind;
+            fd.nx = f.nx;
+            fd.ny = f.ny;
+            fd.absorbed_only = f.absorbed_only;
+            fd.x0 = f.x0;
+            fd.x1 = f.x1;
+            fd.y0 = f.y0;
+            fd.y1 = f.y1;
+            fd.bins = a + flux_off[m];
+        }
+        TraceOut &O = Op[p];
+        memset(&O, 0, sizeof O);
+        O.ctr = ws.pos_ctr.as<RunCounters>() + p;
+        O.first_hits = a;
+        O.absorbed = a + ne;
+        O.delivered = a + 2 * ne;
+        O.recs = nullptr;
+        O.rec_cap = 0;
+        O.rec_count = ws.rec_count.as<unsigned long long>();
+    }
+    CK(ws.rec_count.ensure(8));
+    for (auto &O : Op) O.rec_count = ws.rec_count.as<unsigned long long>();
+
+    // buffers for the largest batch, sized before anything is queued (growing a buffer frees
+    // the old one, which must not happen under queued work)
+    const uint64_t kMaxBatch = uint64_t(1) << 26;
+    const uint32_t n_elem0 = uint32_t(S0.stages[0].n_elem);
+    {
+        const uint64_t n = kMaxBatch;
+        const uint32_t nb = uint32_t((n + kProbeBlock - 1) / kProbeBlock);
+        ProbeOut po;
+        WfState W;
+        WfQueues Q;
+        CK(probe_buffers(ws, n, po));
+        CK(ws.offsets.ensure(size_t(nb) * 4));
+        CK(ws.scan_parts.ensure(scan_parts(nb) * 4));
+        CK(ws.total.ensure(8));
+        CK(ws.s_sid.ensure(n * 8));
+        CK(ws.s_el.ensure(n * 4));
+        CK(ws.s_idx.ensure(n * 4));
+        CK(ws.ecount.ensure(size_t(std::max<uint32_t>(n_elem0, 1)) * 4));
+        CK(ws.ecursor.ensure(size_t(std::max<uint32_t>(n_elem0, 1)) * 4));
+        CK(ws.etotal.ensure(8));
+        CK(wf_buffers(ws, S0, n, W, Q));
+    }
+    Workspace::Tuning &tu = ws.tune[rq.precision ? 1 : 0];
+    if (!tu.done) CK(autotune(ws, Sp[0], rq.precision, rq.max_sun, st, out.gpu_launches));
+    out.probe_variant = tu.probe;
+    CK(cudaStreamSynchronize(st));
+    out.setup_ms = ms_since(t_setup);
+
+    size_t ev_used = 0;
+    auto new_event = [&]() {
+        if (ev_used == ws.events.size()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            ws.events.push_back(e);
+        }
+        return ws.events[ev_used++];
+    };
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> probe_ev, trace_ev;
+    cudaEvent_t t_first = new_event(), t_last = new_event();
+    CK(cudaEventRecord(t_first, st));
+    RunState *drs = ws.pos_rs.as<RunState>();
+    std::vector<uint64_t> sun_next(K, 0);
+    std::vector<double> p_est(K, 0.0);
+    std::vector<bool> reached(K, false);
+    size_t left = K;
+    for (size_t p = 0; p < K; ++p)
+        if (pos[p].n_hits == 0) {  // nothing to trace: SunRayCount 0
+            reached[p] = true;
+            --left;
+        }
+    while (left > 0) {
+        out.waves++;
+        for (size_t p = 0; p < K; ++p) {
+            if (reached[p]) continue;
+            uint64_t want;
+            const uint64_t need = pos[p].n_hits - rs_h[p].hits_done;
+            if (p_est[p] <= 0.0)
+                want = std::min<uint64_t>(uint64_t(1) << 20, rq.max_sun - sun_next[p]);
+            else
+                want = std::min<uint64_t>(uint64_t(1.03 * double(need) / p_est[p]) + 65536, rq.max_sun - sun_next[p]);
+            if (want == 0) {
+                char buf[200];
+                snprintf(buf, sizeof buf, "sun position %zu: generated sun rays reached maximum count: %llu", p,
+                         (unsigned long long)rq.max_sun);
+                out.error = buf;
+                return false;
+            }
+            const SceneDev &S = Sp[p];
+            for (uint64_t queued = 0; queued < want;) {
+                const uint64_t n = std::min<uint64_t>(kMaxBatch, want - queued);
+                const uint32_t nb = uint32_t((n + kProbeBlock - 1) / kProbeBlock);
+                ProbeOut po;
+                WfState W;
+                WfQueues Q;
+                CK(probe_buffers(ws, n, po));
+                CK(wf_buffers(ws, S, n, W, Q));
+                cudaEvent_t p0 = new_event(), p1 = new_event(), p2 = new_event();
+                CK(cudaEventRecord(p0, st));
+                const uint64_t s0 = sun_next[p];
+                if (rq.precision)
+                    out.gpu_launches += launch_probe_mixed(S, s0, uint32_t(n), po, drs + p, tu.probe, st);
+                else
+                    out.gpu_launches += launch_probe_fp64(S, s0, uint32_t(n), po, drs + p, tu.probe, st);
+                launch_scan(po.block_counts, nb, ws.offsets.as<uint32_t>(), ws.total.as<uint32_t>(),
+                            ws.scan_parts.as<uint32_t>(), st);
+                launch_list_sort(s0, po, ws.offsets.as<uint32_t>(), ws.total.as<uint32_t>(), drs + p, n_elem0,
+                                 ws.ecount.as<uint32_t>(), ws.ecursor.as<uint32_t>(), ws.etotal.as<uint32_t>(),
+                                 ws.s_sid.as<uint64_t>(), ws.s_el.as<uint32_t>(), ws.s_idx.as<uint32_t>(),
+                                 uint32_t(n), st);
+                CK(cudaEventRecord(p1, st));
+                if (rq.precision)
+                    out.gpu_launches += launch_trace_mixed(false, S, ws.s_sid.as<uint64_t>(), ws.s_el.as<uint32_t>(),
+                                                           ws.s_idx.as<uint32_t>(), ws.total.as<uint32_t>(), drs + p,
+                                                           Op[p], W, Q, nullptr, st);
+                else
+                    out.gpu_launches += launch_trace_fp64(false, S, ws.s_sid.as<uint64_t>(), ws.s_el.as<uint32_t>(),
+                                                          ws.s_idx.as<uint32_t>(), ws.total.as<uint32_t>(), drs + p,
+                                                          Op[p], W, Q, nullptr, st);
+                CK(cudaEventRecord(p2, st));
+                launch_advance(ws.total.as<uint32_t>(), nullptr, s0, uint32_t(n), drs + p, st);
+                CK(cudaGetLastError());
+                out.gpu_launches += 6;  // scan (two kernels), sort (three), advance
+                probe_ev.push_back({p0, p1});
+                trace_ev.push_back({p1, p2});
+                queued += n;
+                sun_next[p] += n;
+                out.batches++;
+            }
+        }
+        CK(cudaMemcpyAsync(rs_h.data(), drs, K * sizeof(RunState), cudaMemcpyDeviceToHost, st));
+        out.d2h_bytes += K * sizeof(RunState);
+        CK(cudaStreamSynchronize(st));
+        for (size_t p = 0; p < K; ++p) {
+            if (reached[p]) continue;
+            if (rs_h[p].reached) {
+                reached[p] = true;
+                --left;
+            } else if (sun_next[p] > 0) {
+                p_est[p] = std::max(double(rs_h[p].hits_done) / double(sun_next[p]), 1e-9);
+            }
+        }
+    }
+    CK(cudaEventRecord(t_last, st));
+    CK(cudaStreamSynchronize(st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, t_first, t_last);
+    out.device_ms = ms;
+    for (auto &pe : probe_ev) {
+        float x = 0;
+        cudaEventElapsedTime(&x, pe.first, pe.second);
+        out.probe_ms += x;
+    }
+    for (auto &pe : trace_ev) {
+        float x = 0;
+        cudaEventElapsedTime(&x, pe.first, pe.second);
+        out.trace_ms += x;
+    }
+    std::vector<RunCounters> ctr(K);
+    std::vector<unsigned long long> accv(K * acc_n);
+    CK(cudaMemcpyAsync(ctr.data(), ws.pos_ctr.p, K * sizeof(RunCounters), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(accv.data(), ws.pos_acc.p, K * acc_n * 8, cudaMemcpyDeviceToHost, st));
+    out.d2h_bytes += K * (sizeof(RunCounters) + acc_n * 8);
+    CK(cudaStreamSynchronize(st));
+    out.pos.assign(K, PositionResult());
+    for (size_t p = 0; p < K; ++p) {
+        PositionResult &r = out.pos[p];
+        r.sun_rays = pos[p].n_hits ? rs_h[p].sun_rays : 0;
+        r.ray_hits = rs_h[p].hits_done;
+        r.intersections = ctr[p].records;
+        r.stage_entries.assign(ctr[p].stage_entries, ctr[p].stage_entries + nst);
+        r.max_enter.assign(ctr[p].max_enter, ctr[p].max_enter + nst);
+        const unsigned long long *a = accv.data() + p * acc_n;
+        r.absorbed.assign(a + ne, a + 2 * ne);
+        for (size_t m = 0; m < rq.flux.size(); ++m)
+            r.flux.emplace_back(a + flux_off[m], a + flux_off[m] + size_t(rq.flux[m].nx) * rq.flux[m].ny);
+    }
+    if (rq.precision ? take_fe_failures_mixed() : take_fe_failures_fp64()) {
+        out.error = "Interpolation failed to find nearby nodes to ray hit in FEA surface.";
+        return false;
+    }
+    unsigned flags = 0;
+    for (auto &c : ctr) flags |= c.flags;
+    if (flags & kFlagBadInteraction) {
+        out.error = "Bad optical interaction type (only 1 = refraction and 2 = reflection are traced)";
+        return false;
+    }
+    out.ok = true;
+    return true;
 }
 
 }  // namespace stb

@@ -23,6 +23,8 @@ constexpr int kMaxStages = 16;
 constexpr int kMaxFluxMaps = 8;
 constexpr int kSunCdfCells = 4096;
 constexpr int kSunInvCells = 8192;
+// doubles per first-stage element in SceneDev::sun_fold
+constexpr int kFoldStride = 16;
 
 // surface model codes after coretrace/input.cpp:288-366 translation
 enum SurfType : int {
@@ -155,6 +157,12 @@ struct SceneDev {
     const double *ex_pos, *ex_cos;
     int n_flux;
     FluxMapDev flux[kMaxFluxMaps];
+    // Mixed precision, sun rays on a flat first stage culled by the sun-plane grid: per
+    // first-stage element, the affine map from the sun-plane point (xs, ys) to the element
+    // frame that the chain sun frame -> stage -> global -> stage -> element composes to
+    // (kFoldStride doubles: the columns of xs and ys, the offset with the 1e-5 nudge, the
+    // direction, 1 / (direction z + 1e-11)); null when unused
+    const double *sun_fold;
 };
 
 // One intersection record as the reference stores it (coretrace/types.h:239-246),

@@ -68,6 +68,13 @@ EXTENSIONS = {
     "st_b200_sim_run_replay": (C.c_int, [C.c_void_p, C.c_uint, st_uint_t, c_double_p, st_uint_t, c_double_p,
                                          C.c_void_p, C.c_void_p]),
     "st_b200_load_stinput": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "st_b200_set_max_sun_rays": (C.c_int, [C.c_void_p, C.c_ulonglong]),
+    "st_b200_set_ranks": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "st_b200_sim_run_batch": (C.c_int, [C.c_void_p, C.c_uint, C.c_int, c_double_p, C.POINTER(st_uint_t), c_double_p]),
+    "st_b200_batch_stats": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(Stats)]),
+    "st_b200_batch_flux_counts": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _u64p]),
+    "st_b200_batch_absorbed": (C.c_int, [C.c_void_p, C.c_int, C.c_int, _u64p]),
+    "st_b200_batch_sun_box": (C.c_int, [C.c_void_p, C.c_int, c_double_p, c_double_p, c_double_p, c_double_p]),
     "st_b200_write_rays": (C.c_int, [C.c_void_p, C.c_char_p]),
 }
 
@@ -116,6 +123,44 @@ class B200Api(StApi):
         c = np.zeros(n, dtype=np.uint64)
         self.st_b200_element_counts(ctx, stage, a.ctypes.data_as(_u64p), b.ctypes.data_as(_u64p), c.ctypes.data_as(_u64p))
         return a, b, c
+
+    def run_batch(self, ctx, seed: int, sun_xyz, hits, track_target=None) -> int:
+        """st_b200_sim_run_batch: K sun positions (K x 3) with their hit counts; position k
+        draws from the streams of seed + k."""
+        sun = np.ascontiguousarray(sun_xyz, dtype=np.float64).reshape(-1, 3)
+        h = np.ascontiguousarray(hits, dtype=np.uint64).reshape(-1)
+        if len(h) != len(sun):
+            raise ValueError("one hit count per sun position")
+        tgt = None if track_target is None else np.ascontiguousarray(track_target, dtype=np.float64)
+        return self.st_b200_sim_run_batch(ctx, seed, len(sun), sun.ctypes.data_as(c_double_p),
+                                          h.ctypes.data_as(C.POINTER(st_uint_t)),
+                                          None if tgt is None else tgt.ctypes.data_as(c_double_p))
+
+    def batch_stats(self, ctx, position: int) -> dict:
+        s = Stats()
+        if self.st_b200_batch_stats(ctx, position, C.byref(s)) < 0:
+            raise RuntimeError("st_b200_batch_stats failed")
+        d = {k: getattr(s, k) for k, _ in Stats._fields_ if k != "stage_entries"}
+        d["stage_entries"] = list(s.stage_entries)
+        return d
+
+    def batch_flux(self, ctx, idx: int, position: int, nx: int, ny: int) -> np.ndarray:
+        out = np.zeros(nx * ny, dtype=np.uint64)
+        if self.st_b200_batch_flux_counts(ctx, idx, position, out.ctypes.data_as(_u64p)) < 0:
+            raise RuntimeError("st_b200_batch_flux_counts failed")
+        return out.reshape(ny, nx)
+
+    def batch_absorbed(self, ctx, position: int, stage: int, n: int) -> np.ndarray:
+        out = np.zeros(n, dtype=np.uint64)
+        if self.st_b200_batch_absorbed(ctx, position, stage, out.ctypes.data_as(_u64p)) < 0:
+            raise RuntimeError("st_b200_batch_absorbed failed")
+        return out
+
+    def batch_sun_box(self, ctx, position: int):
+        v = [C.c_double() for _ in range(4)]
+        if self.st_b200_batch_sun_box(ctx, position, *[C.byref(x) for x in v]) < 0:
+            raise RuntimeError("st_b200_batch_sun_box failed")
+        return tuple(x.value for x in v)
 
     def explicit_rays(self, ctx, pos: np.ndarray, cos: np.ndarray) -> int:
         pos = np.ascontiguousarray(pos, dtype=np.float64)

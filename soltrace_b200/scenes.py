@@ -312,3 +312,112 @@ def field_scene(n_helio: int = 2000, raycount: int = 100_000_000, elevation_deg:
     return Scene(sun, optics, [Stage(helios), Stage([rec])], raycount=raycount,
                  raymax=max(2_000_000_000 - 1, 0) if raycount > 10_000_000 else 200 * raycount + 10_000,
                  dynamic_group=dynamic_group, name="field")
+
+
+# ------------------------------------------------------------------------------------
+# Batched annual trace: beam-down tower
+# ------------------------------------------------------------------------------------
+BEAM_DOWN_HEIGHT = 120.0     # secondary vertex height (m)
+BEAM_DOWN_ECC = 1.3          # hyperboloid eccentricity
+BEAM_DOWN_DIAM = 20.0        # secondary aperture diameter (m)
+LIP_RA, LIP_RS = 10.0, 0.5   # torus lip: annular and cross-section radius (m)
+GROUND_MAP = (3, 1, 0, 64, 64, -8.0, 8.0, -8.0, 8.0, 1)  # ground receiver, 64 x 64 over 16 m x 16 m, absorbed
+
+
+def beam_down_geometry(height: float = BEAM_DOWN_HEIGHT, ecc: float = BEAM_DOWN_ECC):
+    """(vertex curvature c, kappa, upper focus height) of a convex hyperboloid whose vertex is
+    at `height` and whose lower focus is on the ground.  SolTrace's 'o' surface is
+    x^2 + y^2 + kappa z^2 - 2 z / c = 0 (kappa = 1 - e^2); the foci lie R/(1+e) above and
+    R/(e-1) below the vertex, R = 1/c, so R = height (e - 1)."""
+    R = height * (ecc - 1.0)
+    return 1.0 / R, 1.0 - ecc * ecc, height + R / (1.0 + ecc)
+
+
+def beam_down_scene(n_helio: int = 10000, raycount: int = 1_000_000, sun_xyz=None, r_min: float = 100.0,
+                    r_max: float | None = None, slope: float = 1.5, csr: float = 0.1) -> Scene:
+    """Beam-down tower: the heliostat field layout of field_scene scaled to n_helio heliostats
+    (same density), a convex hyperboloid secondary (eccentricity 1.3, kappa = -0.69, 20 m
+    aperture, vertex at 120 m, surface 'o' of quadricsurfaceclosedform.cpp:129-148) with an
+    absorbing torus lip (surface 'd', annular radius 10 m, cross-section 0.5 m, aperture 'a'
+    as input.cpp:349-355 requires) around its rim, and a flat ground receiver at the lower
+    focus.  The heliostats are aimed at the upper focus for `sun_xyz` (default: 45 deg
+    elevation, south); st_b200_sim_run_batch re-aims them per sun position with that focus
+    as its tracking target (beam_down_target)."""
+    c, kappa, f1 = beam_down_geometry()
+    if r_max is None:  # the density of the 2,000-heliostat field over 100-1000 m
+        r_max = math.sqrt(n_helio / 2000.0 * (1000.0 ** 2 - r_min ** 2) + r_min ** 2)
+    xy = field_layout(n_helio, r_min=r_min, r_max=r_max)
+    s = _unit(sun_xyz) if sun_xyz is not None else sun_vector(45.0, 180.0)
+    target = np.array([0.0, 0.0, f1])
+    helios = []
+    for (x, y) in xy:
+        pos = np.array([x, y, 5.0])
+        t = target - pos
+        n = s + t / math.sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2])
+        nn = math.sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2])
+        helios.append(Element(origin=tuple(pos), aim=tuple(pos + 100.0 * (n / nn)), aperture="r",
+                              aperture_params=(10.0, 10.0), surface="f", interaction=2, optic="helio"))
+    h = BEAM_DOWN_HEIGHT
+    rim = beam_down_rim_height()
+    secondary = Element(origin=(0.0, 0.0, h), aim=(0.0, 0.0, h + 100.0), aperture="c", aperture_params=(BEAM_DOWN_DIAM,),
+                        surface="o", surface_params=(c, kappa), interaction=2, optic="secondary")
+    lip = Element(origin=(0.0, 0.0, rim - LIP_RS), aim=(0.0, 0.0, rim + 100.0), aperture="a",
+                  aperture_params=(0.0, 0.0, 360.0), surface="d", surface_params=(LIP_RA, LIP_RS), interaction=2,
+                  optic="lip")
+    ground = Element(origin=(0.0, 0.0, 0.0), aim=(0.0, 0.0, 100.0), aperture="r", aperture_params=(16.0, 16.0),
+                     surface="f", interaction=2, optic="receiver")
+    optics = [OpticSet("helio", OpticFace("g", refl=0.9, slope=slope), OpticFace("g", refl=0.9, slope=slope)),
+              OpticSet("secondary", OpticFace("g", refl=0.95, slope=0.5), OpticFace("g", refl=0.95, slope=0.5)),
+              OpticSet("lip", OpticFace("g", refl=0.0), OpticFace("g", refl=0.0)),
+              OpticSet("receiver", OpticFace("g", refl=0.0), OpticFace("g", refl=0.0))]
+    t_, inten = buie_csr_table(csr)
+    sun = Sun("d", 0.0, tuple(1.0e4 * s), table=(t_, inten))
+    return Scene(sun, optics, [Stage(helios), Stage([secondary, lip]), Stage([ground])], raycount=raycount,
+                 raymax=2_000_000_000 - 1, dynamic_group=True, name="beam_down")
+
+
+def beam_down_rim_height() -> float:
+    """Height of the secondary's rim (r = 10 m) on x^2 + y^2 + kappa z^2 - 2 z / c = 0."""
+    c, kappa, _ = beam_down_geometry()
+    r2 = (BEAM_DOWN_DIAM / 2.0) ** 2
+    # kappa z^2 - (2/c) z + r2 = 0, the root nearest the vertex
+    b = 2.0 / c
+    return BEAM_DOWN_HEIGHT + (b - math.sqrt(b * b - 4.0 * kappa * r2)) / (2.0 * kappa)
+
+
+def beam_down_target() -> np.ndarray:
+    """The heliostats' aim point: the hyperboloid's upper focus."""
+    return np.array([0.0, 0.0, beam_down_geometry()[2]])
+
+
+def sun_position(lat: float, day: float, hour: float):
+    """(elevation, azimuth from north) in degrees by the formula of coretrace/stapi.cpp:500-527."""
+    d2r = math.pi / 180.0
+    decl = math.degrees(math.asin(0.39795 * math.cos(0.98563 * d2r * (day - 173))))
+    ha = 15.0 * (hour - 12.0)
+    el = math.degrees(math.asin(math.sin(decl * d2r) * math.sin(lat * d2r) +
+                                math.cos(decl * d2r) * math.cos(ha * d2r) * math.cos(lat * d2r)))
+    az = math.degrees(math.acos((math.sin(d2r * decl) * math.cos(d2r * lat) -
+                                 math.cos(d2r * decl) * math.sin(d2r * lat) * math.cos(d2r * ha)) /
+                                math.cos(d2r * el) + 1e-10))
+    if math.sin(ha * d2r) > 0.0:
+        az = 360.0 - az
+    return el, az
+
+
+def annual_suns(n: int = 512, lat: float = 40.0, seed: int = 7, min_elevation: float = 5.0, rays_per_kw: float = 1e6):
+    """n sun positions drawn uniformly over the daylight hours of a year at latitude `lat`
+    (day and hour uniform, kept when the sun is above min_elevation), each with a DNI drawn
+    uniform in 300-1000 W/m2 and a hit budget of rays_per_kw x DNI / 1000.
+    Returns (sun_xyz (n, 3) at 1e4 m, hits (n,), dni (n,))."""
+    rng = np.random.default_rng(seed)
+    suns, dni = [], []
+    while len(suns) < n:
+        day, hour = rng.uniform(1.0, 366.0), rng.uniform(0.0, 24.0)
+        el, az = sun_position(lat, day, hour)
+        if el < min_elevation:
+            continue
+        suns.append(1.0e4 * sun_vector(el, az))
+        dni.append(rng.uniform(300.0, 1000.0))
+    dni = np.asarray(dni)
+    return np.asarray(suns), np.maximum(1, (rays_per_kw * dni / 1000.0).astype(np.int64)), dni

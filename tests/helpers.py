@@ -51,3 +51,51 @@ def assert_same_records(a: dict, b: dict, pos_tol: float, rel_tol: float = 0.0, 
     for k in ("cx", "cy", "cz"):
         d = np.abs(a[k] - b[k])
         assert np.all(d <= dtol + rel_tol), (k, float(d.max()))
+
+
+def c_declarations(text: str) -> dict:
+    """name -> (return type, [parameter types]) of every st_* function declared in a C header,
+    with comments, export macros and parameter names removed and array parameters written
+    as the pointers they decay to (double x[8] -> double*, double m[3][3] -> double(*)[3])."""
+    import re
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", " ", text)
+    text = text.replace("STCORE_API", " ")
+    out = {}
+    for m in re.finditer(r"([A-Za-z_][\w\s\*]*?)\b(st_\w+)\s*\(((?:[^()]|\([^()]*\))*)\)\s*;", text):
+        ret = " ".join(m.group(1).split()).replace(" *", "*")
+        params = []
+        body = m.group(3).strip()
+        if body and body != "void":
+            depth, cur, parts = 0, "", []
+            for ch in body:
+                if ch == "(":
+                    depth += 1
+                elif ch == ")":
+                    depth -= 1
+                if ch == "," and depth == 0:
+                    parts.append(cur)
+                    cur = ""
+                else:
+                    cur += ch
+            parts.append(cur)
+            for p in parts:
+                p = " ".join(p.split())
+                if "(*" in p:
+                    params.append("fnptr")
+                    continue
+                dims = re.findall(r"\[\s*\d*\s*\]", p)
+                p = re.sub(r"\[\s*\d*\s*\]", "", p).strip()
+                # drop the parameter name (the last identifier, unless the type is bare)
+                toks = re.findall(r"[A-Za-z_]\w*|\*", p)
+                if len(toks) > 1 and re.match(r"[A-Za-z_]", toks[-1]) and toks[-1] not in ("int", "double", "char",
+                                                                                          "st_uint_t", "st_context_t"):
+                    toks = toks[:-1]
+                t = " ".join(toks).replace(" *", "*")
+                if len(dims) == 1:
+                    t += "*"
+                elif len(dims) == 2:
+                    t += "(*)" + dims[1].replace(" ", "")
+                params.append(t)
+        out[m.group(2)] = (ret, params)
+    return out

@@ -24,10 +24,83 @@ FIELD_HITS = 10_000_000
 FIELD_SEED = 3
 
 
-def field_stat_scene():
-    """The headline field (2,000 flat heliostats, Buie CSR 0.1, 8 m x 10 m receiver) with
-    exact culling on the reference's side (include_dynamic_group = 0)."""
-    return scenes.field_scene(FIELD_HELIOSTATS, FIELD_HITS, dynamic_group=False), FIELD_HITS, FIELD_SEED
+def field_stat_scene(sun: str = "buie"):
+    """The headline field (2,000 flat heliostats, 8 m x 10 m receiver) with exact culling on
+    the reference's side (include_dynamic_group = 0); sun "buie": the headline Buie CSR 0.1
+    table sunshape; "gauss": a Gaussian sunshape of sigma 2.73 mrad instead (whose sampler the
+    reference draws without the table sampler's bias, see sun_theta_scene)."""
+    import dataclasses
+    sc = scenes.field_scene(FIELD_HELIOSTATS, FIELD_HITS, dynamic_group=False)
+    if sun == "gauss":
+        sc = dataclasses.replace(sc, sun=dataclasses.replace(sc.sun, shape="g", sigma=2.73, table=None))
+    return sc, FIELD_HITS, FIELD_SEED
+
+
+# The reference's generator has a single cycle of 2^31 - 2 states, which all its threads share.
+# Its table-sunshape sampler (2-D rejection, about 2 % accepted) takes about 290 generator calls
+# per sun angle, so the Buie-table field costs about 330 calls per first-stage hit and one cycle
+# holds only about 6.5e6 hits: a longer reference run repeats its random numbers and its
+# Monte-Carlo error stops shrinking.  The reference's fixtures therefore stay within the cycle:
+# REFERENCE_HITS per configuration, each thread on its own stretch (spaced_seeds).
+REFERENCE_CYCLE = 2 ** 31 - 2
+REFERENCE_HITS = {"buie": 4_000_000, "gauss": 10_000_000}
+
+
+def spaced_seeds(n: int, offset: int = 999):
+    """Seeds for n reference threads whose random streams never overlap: the reference's
+    generator is libstdc++'s minstd_rand0 (x <- 16807 x mod 2^31-1, seeded with x0 = seed),
+    so seeding thread i with 16807^(i (2^31-2)/n + offset) starts it i/n of the way around
+    the generator's cycle, and each thread owns (2^31-2)/n consecutive states."""
+    M = 2 ** 31 - 1
+    return [pow(16807, i * ((M - 1) // n) + offset, M) for i in range(n)]
+
+
+# sun-angle sampler: a 0.2 mm flat mirror under the Buie CSR 0.1 table sunshape reflecting onto
+# a target 500 m above it: a ray sampled at sun angle theta lands at radius 500 tan(theta)
+THETA_HEIGHT, THETA_BINS, THETA_MAX = 500.0, 120, 30.0
+
+
+def sun_theta_scene(hits: int):
+    t, inten = scenes.buie_csr_table(0.1)
+    sun = Sun("d", 0.0, (0.0, 0.0, 100.0), table=(t, inten))
+    mirror = Element(origin=(0, 0, 0), aim=(0, 0, 1), aperture="c", aperture_params=(0.0002,), surface="f",
+                     interaction=2, optic="mirror")
+    target = Element(origin=(0, 0, THETA_HEIGHT), aim=(0, 0, 0), aperture="c", aperture_params=(40.0,), surface="f",
+                     interaction=2, optic="target")
+    optics = [OpticSet("mirror", OpticFace("g", refl=1.0), OpticFace("g", refl=1.0)),
+              OpticSet("target", OpticFace("g", refl=0.0), OpticFace("g", refl=0.0))]
+    return Scene(sun, optics, [Stage([mirror]), Stage([target])], raycount=hits, raymax=100 * hits + 1000)
+
+
+def theta_histogram(rec: dict) -> np.ndarray:
+    """Histogram of the sampled sun angles (mrad, THETA_BINS bins over [0, THETA_MAX]) from the
+    target hits of sun_theta_scene."""
+    sel = rec["stage"] == 2
+    r = np.hypot(rec["x"][sel], rec["y"][sel])
+    return np.histogram(np.arctan(r / THETA_HEIGHT) * 1000.0, bins=THETA_BINS, range=(0.0, THETA_MAX))[0].astype(np.int64)
+
+
+def theta_exact() -> np.ndarray:
+    """Bin probabilities of the sun angle the table sunshape defines: p(theta) ~ theta I(theta)
+    on [0, 30] mrad with I linearly interpolated on the table (errors.cpp:160-185: a point drawn
+    uniformly in the square of half-side MaxAngle, kept with probability I(theta)/I_max inside
+    the circle of radius MaxAngle), integrated numerically."""
+    t, inten = scenes.buie_csr_table(0.1)
+    th = np.linspace(0.0, THETA_MAX, 3_000_001)
+    pdf = th * np.interp(th, t, inten)
+    cdf = np.concatenate([[0.0], np.cumsum((pdf[1:] + pdf[:-1]) / 2.0 * np.diff(th))])
+    cdf /= cdf[-1]
+    return np.diff(np.interp(np.linspace(0.0, THETA_MAX, THETA_BINS + 1), th, cdf))
+
+
+def one_sample_chi2(h: np.ndarray, p: np.ndarray, min_expected: float = 5.0):
+    """Goodness of fit of histogram h to bin probabilities p: (chi2, dof, p-value)."""
+    n = h.sum()
+    e = n * p
+    k = e > min_expected
+    chi2 = float(((h[k] - e[k]) ** 2 / e[k]).sum())
+    dof = int(k.sum()) - 1
+    return chi2, dof, float(sps.chi2.sf(chi2, dof))
 
 
 def _mirror_target(sun: Sun, optic: OpticFace, height: float, target_d: float, hits: int) -> Scene:

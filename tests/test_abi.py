@@ -38,9 +38,39 @@ def test_every_declared_function_is_exported():
         assert not missing, (h, missing)
 
 
-def test_stapi_header_covers_reference_api():
-    # every entry point of the reference's stapi.h (the ctypes table mirrors it)
-    assert set(STAPI_FUNCTIONS) <= _declared("stapi.h")
+def test_stapi_header_matches_reference_declarations():
+    """Every function the reference's coretrace/stapi.h declares (tests/golden/
+    reference_stapi.json, parsed from it by tests/golden/make_api_fixture.py) is declared in
+    include/stapi.h with the same return and parameter types, and exported."""
+    import json
+
+    from helpers import c_declarations
+    ref = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_stapi.json")))["functions"]
+    assert len(ref) >= 50
+    mine = c_declarations(open(os.path.join(ROOT, "include", "stapi.h")).read())
+    exported = _exports()
+    for name, d in ref.items():
+        assert name in mine, name
+        assert mine[name] == (d["returns"], d["params"]), (name, mine[name], d)
+        assert name in exported, name
+    # the ctypes table used by the tests binds the same set
+    assert set(STAPI_FUNCTIONS) == set(ref)
+
+
+def test_batch_arguments_checked_before_device_work(product):
+    """st_b200_sim_run_batch rejects bad arguments and explicit-ray contexts with -1 and a
+    message, before touching a device."""
+    ctx = product.st_create_context()
+    try:
+        scenes.push(product, ctx, scenes.dish_scene(100))
+        assert product.run_batch(ctx, 1, np.zeros((0, 3)), []) == -1
+        assert "at least one sun position" in product.messages(ctx)[-1]
+        product.explicit_rays(ctx, np.array([[0.0, 0.0, 4.0]]), np.array([[0.0, 0.0, -1.0]]))
+        assert product.run_batch(ctx, 1, np.array([[0.0, 0.0, 100.0]]), [10]) == -1
+        assert "explicit rays" in product.messages(ctx)[-1]
+        assert product.st_b200_batch_stats(ctx, 0, None) == -1
+    finally:
+        product.st_free_context(ctx)
 
 
 def test_library_loads_and_setters(product):

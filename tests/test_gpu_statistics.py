@@ -3,19 +3,21 @@
 The reference's random stream (one libstdc++ minstd_rand0 per context) and the device's
 (per-ray Philox) differ, so results agree only within Monte-Carlo error.  The fixture
 tests/golden/reference_stats.npz holds the reference's results, made by
-tests/golden/make_stat_fixtures.py from the reference built from its own sources.
+tests/golden/make_stat_fixtures.py from the reference built from its own sources, every
+reference thread on its own stretch of the generator's cycle.
 
-* Headline field (2,000 flat heliostats, Buie CSR 0.1 table sunshape, cylindrical
-  receiver, 1e7 first-stage hits; the reference with exact culling): the 100 x 100
-  receiver flux map (chi-square over the bins, and the share of bins beyond 3 sigma), the
-  total intercept and the sun rays per hit (3 sigma), the per-heliostat first hits and
-  deliveries (chi-square), in FP64 and in mixed precision.
-* Samplers: the table sunshape 'd' (the device inverts the CDF of theta I(theta); the
-  reference rejects in 2-D, errors.cpp:160-185) and the diffuse distribution 'f'
-  (errors.cpp:187-190), through the radial histogram of a far target (chi-square).
+* The headline field (2,000 flat heliostats, cylindrical receiver; the reference with exact
+  culling), traced by the device to 1e7 first-stage hits, under the headline Buie CSR 0.1
+  table sunshape and under a 2.73 mrad Gaussian sun: the 100 x 100 receiver flux map by
+  chi-square and by the share of bins beyond 3 sigma, the total intercept and the sun rays
+  per hit within 3 sigma, the per-heliostat first hits and deliveries by chi-square; FP64
+  and mixed precision.  The reference's side holds 4e6 hits for the Buie sun (the most its
+  generator's cycle holds without repeating random numbers: stat_scenes.REFERENCE_HITS) and
+  1e7 for the Gaussian sun.
+* Samplers: the table sunshape against the distribution the table defines and against the
+  reference, and the diffuse distribution 'f' (errors.cpp:187-190) against the reference.
 
-A chi-square p-value below 1e-3 fails (a correct trace fails one such test in a
-thousand runs).
+A chi-square p-value below 1e-3 fails (a correct trace fails one such test in a thousand).
 """
 import os
 
@@ -23,8 +25,8 @@ import numpy as np
 import pytest
 
 from soltrace_b200 import scenes
-from stat_scenes import (FIELD_FLUX, field_stat_scene, rate_z, sampler_scenes, target_radial_from_records,
-                         two_sample_chi2)
+from stat_scenes import (FIELD_FLUX, field_stat_scene, one_sample_chi2, rate_z, sampler_scenes, sun_theta_scene,
+                         target_radial_from_records, theta_exact, theta_histogram, two_sample_chi2)
 
 pytestmark = pytest.mark.gpu
 
@@ -37,9 +39,8 @@ def ref_stats():
     return dict(np.load(FIX))
 
 
-@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "mixed"])
-def test_field_flux_and_intercept_match_reference(product, ref_stats, prec):
-    sc, hits, _ = field_stat_scene()
+def _field_run(product, sun, prec):
+    sc, hits, _ = field_stat_scene(sun)
     n_el = len(sc.stages[0].elements)
     ctx = product.st_create_context()
     try:
@@ -53,24 +54,58 @@ def test_field_flux_and_intercept_match_reference(product, ref_stats, prec):
         st = product.stats(ctx)
     finally:
         product.st_free_context(ctx)
-    r_hits, r_sun, r_abs = (int(x) for x in ref_stats["field_totals"])
     assert st["ray_hits"] == hits
-    # sun rays per numbered hit and the receiver intercept, within 3 sigma
+    return hits, st, flux, np.asarray(first, dtype=np.int64), np.asarray(delivered, dtype=np.int64)
+
+
+def _beyond_3_sigma(a, na, b, nb):
+    pa, pb = a / na, b / nb
+    sig = np.sqrt(a / na ** 2 + b / nb ** 2)
+    m = (a + b) >= 10
+    return float(np.mean(np.abs(pa - pb)[m] > 3 * sig[m]))
+
+
+def _compare_totals(key, ref_stats, hits, st, flux, first):
+    r_hits, r_sun, r_abs = (int(x) for x in ref_stats[f"{key}_totals"])
     z_sun = rate_z(hits, st["sun_rays"], r_hits, r_sun)
     z_int = rate_z(int(flux.sum()), hits, r_abs, r_hits)
     assert abs(z_sun) < 3, (st["sun_rays"], r_sun, z_sun)
     assert abs(z_int) < 3, (int(flux.sum()), r_abs, z_int)
-    # the receiver map, bin by bin
-    chi2, dof, p = two_sample_chi2(flux, hits, ref_stats["field_flux"], r_hits)
+    # first heliostat hit by each numbered ray: the sun-box sampling and the first stage only
+    chi2, dof, p = two_sample_chi2(first, hits, ref_stats[f"{key}_first"], r_hits)
+    assert p > P_MIN, ("first hits", chi2, dof, p)
+    return r_hits
+
+
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "mixed"])
+@pytest.mark.parametrize("sun", ["buie", "gauss"])
+def test_field_matches_reference(product, ref_stats, sun, prec):
+    key = "field" if sun == "buie" else "field_gauss"
+    hits, st, flux, first, delivered = _field_run(product, sun, prec)
+    r_hits = _compare_totals(key, ref_stats, hits, st, flux, first)
+    chi2, dof, p = two_sample_chi2(flux, hits, ref_stats[f"{key}_flux"], r_hits)
+    assert p > P_MIN, ("flux map", chi2, dof, p)
+    assert _beyond_3_sigma(flux, hits, ref_stats[f"{key}_flux"], r_hits) <= 0.01  # 0.27 % expected
+    chi2, dof, p = two_sample_chi2(delivered, hits, ref_stats[f"{key}_delivered"], r_hits)
+    assert p > P_MIN, ("deliveries", chi2, dof, p)
+
+
+@pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "mixed"])
+def test_table_sampler_draws_exact_distribution(product, prec):
+    """The device's table-sunshape sampler against the angle distribution the table defines,
+    p(theta) ~ theta I(theta) (errors.cpp:160-185), over 4e6 draws."""
+    hits = 4_000_000
+    ctx = product.st_create_context()
+    try:
+        scenes.push(product, ctx, sun_theta_scene(hits))
+        product.st_b200_set_precision(ctx, prec)
+        assert product.run(ctx, 19) > 0, product.messages(ctx)
+        h = theta_histogram(product.records(ctx))
+    finally:
+        product.st_free_context(ctx)
+    assert h.sum() == hits
+    chi2, dof, p = one_sample_chi2(h, theta_exact())
     assert p > P_MIN, (chi2, dof, p)
-    a, b = flux.astype(float) / hits, ref_stats["field_flux"].astype(float) / r_hits
-    sig = np.sqrt(flux / hits ** 2 + ref_stats["field_flux"] / r_hits ** 2)
-    beyond = np.mean(np.abs(a - b) > 3 * np.maximum(sig, 1e-300))
-    assert beyond <= 0.01, beyond  # 0.27 % expected
-    # per-heliostat intercept: first hits and deliveries
-    for mine, theirs in ((first, ref_stats["field_first"]), (delivered, ref_stats["field_delivered"])):
-        chi2, dof, p = two_sample_chi2(np.asarray(mine, dtype=np.int64), hits, theirs, r_hits)
-        assert p > P_MIN, (chi2, dof, p)
 
 
 @pytest.mark.parametrize("prec", [0, 1], ids=["fp64", "mixed"])

@@ -3,10 +3,17 @@ CUDA trace uses) against the reference's rejection samplers, on the CPU.
 
 The oracle's Philox mode restates the device's sampling, so the GPU tests that compare
 the device with it ray by ray cannot show that those samplers draw the reference's
-distributions.  This test does, without a GPU: the table sunshape 'd' (errors.cpp:160-185)
-and the diffuse distribution 'f' (errors.cpp:187-190) through the radial histogram of a
-far target, against the reference's results in tests/golden/reference_stats.npz
-(tests/golden/make_stat_fixtures.py).  A chi-square p-value below 1e-3 fails.
+distributions.  These tests do, without a GPU, against the reference's results in
+tests/golden/reference_stats.npz (tests/golden/make_stat_fixtures.py):
+
+* the table sunshape 'd' (errors.cpp:160-185) and the diffuse distribution 'f'
+  (errors.cpp:187-190) through the radial histogram of a far target, against the reference;
+* the table sunshape's sampled angles against the distribution the table defines,
+  p(theta) ~ theta I(theta), for the oracle's inverse-CDF sampler and for the reference's
+  own 2-D rejection sampler (4e6 recorded draws, every reference thread on its own stretch
+  of the generator's cycle).
+
+A chi-square p-value below 1e-3 fails.
 """
 import dataclasses
 import os
@@ -15,7 +22,8 @@ import numpy as np
 import pytest
 
 from helpers import run_scene
-from stat_scenes import rate_z, sampler_scenes, target_radial_from_records, two_sample_chi2
+from stat_scenes import (one_sample_chi2, rate_z, sampler_scenes, sun_theta_scene, target_radial_from_records,
+                         theta_exact, theta_histogram, two_sample_chi2)
 
 FIX = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_stats.npz")
 HITS = 400_000
@@ -33,3 +41,39 @@ def test_oracle_samplers_match_reference(oracle, name):
     assert abs(rate_z(on_target, HITS, r_on, r_hits)) < 3
     chi2, dof, p = two_sample_chi2(h, HITS, ref[f"{name}_radial"], r_hits)
     assert p > 1e-3, (name, chi2, dof, p)
+
+
+def test_oracle_table_sampler_draws_exact_distribution(oracle):
+    hits = 1_000_000
+    n, rec, _, msg, _ = run_scene(oracle, sun_theta_scene(hits), 29, lambda a, c: a.st_oracle_set_rng(c, 1))
+    assert n > 0, msg
+    h = theta_histogram(rec)
+    assert h.sum() == hits
+    chi2, dof, p = one_sample_chi2(h, theta_exact())
+    assert p > 1e-3, (chi2, dof, p)
+
+
+def test_reference_table_sampler_draws_exact_distribution():
+    """The reference's recorded table-sunshape draws fit the same distribution: the two
+    samplers (rejection in the reference, inverse CDF in the product) are equivalent."""
+    h = dict(np.load(FIX))["theta"]
+    assert h.sum() >= 3_900_000
+    chi2, dof, p = one_sample_chi2(h, theta_exact())
+    assert p > 1e-3, (chi2, dof, p)
+
+
+def test_reference_generator_cycle_budget():
+    """The reference fixtures stay within the reference generator's cycle: its table-sunshape
+    rejection keeps about 2 % of its candidate angles (3 uniforms, 6 generator calls each), so
+    the Buie field needs several hundred calls per hit and the 2^31 - 2 states of
+    minstd_rand0 hold a few million hits; the fixture's Buie field uses fewer."""
+    from soltrace_b200.scenes import buie_csr_table
+    from stat_scenes import REFERENCE_CYCLE, REFERENCE_HITS
+    t, inten = buie_csr_table(0.1)
+    th = np.linspace(0.0, 30.0, 300_001)
+    accepted = 2.0 * np.pi * np.trapezoid(th * np.interp(th, t, inten), th) / (60.0 * 60.0)
+    calls_per_angle = 6.0 / accepted
+    assert 0.01 < accepted < 0.03
+    # sun rays per hit (~8, 4 calls each) are extra: a lower bound on the cycle use
+    assert REFERENCE_HITS["buie"] * calls_per_angle < REFERENCE_CYCLE
+    assert 10_000_000 * calls_per_angle > REFERENCE_CYCLE  # the device's 1e7 would not fit
