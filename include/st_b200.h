@@ -53,8 +53,13 @@ int st_b200_explicit_rays(st_context_t pcxt, st_uint_t n, const double *pos, con
  * absorbed_only selects absorbed intersections.  Returns the map index. */
 int st_b200_add_flux_map(st_context_t pcxt, int stage, int element, int kind, int nx, int ny, double x0, double x1,
                          double y0, double y1, int absorbed_only);
+/* The same map kept once per first-stage element: an intersection is binned into the map of
+ * the first-stage element its ray hit first (per heliostat, the flux image it puts on the
+ * receiver).  Its counts are n1 maps of nx*ny, [e][iy][ix], n1 the first stage's element count. */
+int st_b200_add_source_flux_map(st_context_t pcxt, int stage, int element, int kind, int nx, int ny, double x0,
+                                double x1, double y0, double y1, int absorbed_only);
 int st_b200_clear_flux_maps(st_context_t pcxt);
-/* nx*ny counts, row-major [iy][ix], of the last run. */
+/* nx*ny counts (per-source maps: n1*nx*ny), row-major [iy][ix], of the last run. */
 int st_b200_flux_counts(st_context_t pcxt, int map, unsigned long long *counts);
 
 typedef struct st_b200_stats {
@@ -189,6 +194,35 @@ int st_b200_batch_flux_counts(st_context_t pcxt, int map, int position, unsigned
 int st_b200_batch_absorbed(st_context_t pcxt, int position, int stage, unsigned long long *absorbed);
 /* the position's sun box in the sun frame (the power per ray is dni x box area / SunRayCount). */
 int st_b200_batch_sun_box(st_context_t pcxt, int position, double *xmin, double *xmax, double *ymin, double *ymax);
+
+/* Flux-surrogate network primitives (BF16 multilayer perceptron on the tensor cores, FP32
+ * accumulation).  No counterpart in the reference, which traces every ray; the plain trace
+ * makes the network's training data (st_b200_add_source_flux_map) and judges it.  All pointers
+ * are device memory of the current device, `stream` a cudaStream_t (NULL: legacy stream);
+ * calls are asynchronous.  Return 1, or -1 on a bad argument or launch failure.
+ *
+ * st_b200_mlp_gemm: C[m x n] = epilogue(A[m x k] B[n x k]^T), A(i, j) at A[i lam + j lak] and
+ *   B(i, j) at B[i lbn + j lbk] (bf16), C with leading dimension ldc; epilogue
+ *     0: C bf16 = max(acc + bias, 0)        1: C float = acc + bias
+ *     2: C bf16 = acc where aux bf16 > 0 (aux shaped as C), else 0
+ *     3: C float = acc                      4: C float += acc (atomic; splits > 1 allowed)
+ * st_b200_mlp_mse: dy bf16 = 2 (y - t) / (rows cols) and *loss += sum (y - t)^2 (double).
+ * st_b200_mlp_colsum: db[c] = sum over rows of dz bf16 [rows x cols].
+ * st_b200_mlp_adam: one Adam step of n float weights (w, moments m and v) from gradient g,
+ *   writing the bf16 copy w_bf16 when given; step counts from 1.
+ * st_b200_mlp_to_bf16: y bf16 = x float.
+ * st_b200_mlp_error: 1 when a GEMM's wait for its tensor-core products ran out since the
+ *   last call (the flag is then cleared), 0 otherwise. */
+int st_b200_mlp_gemm(int m, int n, int k, const void *A, long long lam, long long lak, const void *B, long long lbn,
+                     long long lbk, void *C, long long ldc, int epilogue, const float *bias, const void *aux, int splits,
+                     void *stream);
+int st_b200_mlp_mse(int rows, int cols, const float *y, const float *target, long long ldt, void *dy, double *loss,
+                    void *stream);
+int st_b200_mlp_colsum(int rows, int cols, const void *dz, float *db, void *stream);
+int st_b200_mlp_adam(long long n, float *w, const float *g, float *m, float *v, void *w_bf16, float lr, float beta1,
+                     float beta2, float eps, int step, void *stream);
+int st_b200_mlp_to_bf16(long long n, const float *x, void *y, void *stream);
+int st_b200_mlp_error(void);
 
 /* First-stage probe without device allocation.  No counterpart in the reference.
  *

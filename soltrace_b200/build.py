@@ -32,6 +32,7 @@ UNITS = {
     "st_kernels_mixed.cu": [],
     "st_kernels_common.cu": [],
     "st_noalloc.cu": [],
+    "st_mlp.cu": [],
     "st_stinput.cpp": [],
 }
 CLI = os.path.join(HERE, "strace_b200")  # command-line tracer (csrc/strace_main.cpp)

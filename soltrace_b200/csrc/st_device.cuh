@@ -1125,28 +1125,6 @@ __device__ __forceinline__ bool element_test_flat(const ElemRec &e, const double
     return true;
 }
 
-// Mixed precision, a sun ray on a flat first-stage element: the element-frame ray of sun-plane
-// point (xs, ys) from the element's folded map f (SceneDev::sun_fold: 12 multiply-adds for
-// the chain sun frame -> stage -> global -> stage -> element), then element_test_flat's
-// plane intersection, aperture and acceptance tests.  The hit point is (ox, oy, 0), the
-// incoming direction (f[9], f[10], f[11]).
-__device__ __forceinline__ bool fold_flat_test(const double *f, const ElemRec &e, double xs, double ys, double &t,
-                                               double &ox, double &oy) {
-    const double2 *f2 = reinterpret_cast<const double2 *>(f);
-    const double2 a0 = f2[0], a1 = f2[1], a2 = f2[2], a3 = f2[3], a4 = f2[4], a5 = f2[5], a6 = f2[6];
-    // columns: (a0.x, a0.y, a1.x) for xs, (a1.y, a2.x, a2.y) for ys; offset (a3.x, a3.y, a4.x);
-    // direction (a4.y, a5.x, a5.y); 1 / (cz + 1e-11) in a6.x
-    const double pz = fma(a1.x, xs, fma(a2.y, ys, a4.x));
-    t = (pz != 0.0) ? -pz * a6.x : 0.0;
-    if (t < 0) return false;
-    const double px = fma(a0.x, xs, fma(a1.y, ys, a3.x)), py = fma(a0.y, xs, fma(a2.x, ys, a3.y));
-    ox = fma(a4.y, t, px);
-    oy = fma(a5.x, t, py);
-    if (aperture_in<float>(e, float(ox), float(oy), false) != 1) return false;
-    const int s = e.surf | 0x20;
-    return 0.0 <= e.zap || s == 'm' || s == 'r';
-}
-
 // ------------------------------------------------------------------------------------
 // Error sampling (errors.cpp:60-226, surfacenormalerrors.cpp:58-167) with per-ray
 // inverse-CDF samplers: |theta| of a 2-D Gaussian is Rayleigh, a pillbox disc is

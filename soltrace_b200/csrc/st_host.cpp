@@ -174,11 +174,6 @@ void mulv(const double R[9], const double v[3], double o[3]) {
     o[1] = R[3] * v[0] + R[4] * v[1] + R[5] * v[2];
     o[2] = R[6] * v[0] + R[7] * v[1] + R[8] * v[2];
 }
-void mulvt(const double R[9], const double v[3], double o[3]) {
-    o[0] = R[0] * v[0] + R[3] * v[1] + R[6] * v[2];
-    o[1] = R[1] * v[0] + R[4] * v[1] + R[7] * v[2];
-    o[2] = R[2] * v[0] + R[5] * v[1] + R[8] * v[2];
-}
 inline double sq(double x) { return x * x; }
 
 double mono_at(const Elem &e, double x, double y) {
@@ -790,35 +785,6 @@ void fe_table(const std::vector<double> &nodes, std::vector<double> &out) {
 constexpr double kBeamHalfAngle = 0.1;  // rad
 constexpr size_t kBeamMaxList = 256;
 
-// The first stage's folded sun maps (SceneDev::sun_fold): sun-plane point (xs, ys, -10000)
-// -> stage (generateray.cpp:151-159, whose stage -> global -> stage round trip is the
-// identity) -> element frame (mathproc.cpp:115-173), composed once per element.
-void build_sun_fold(Context *cx, HostScene &hs) {
-    hs.sun_fold.clear();
-    if (cx->sun.point_source || hs.dev.n_stages < 1) return;
-    const StageRec &sr = hs.dev.stages[0];
-    const SunDev &sd = hs.dev.sun;
-    hs.sun_fold.assign(size_t(sr.n_elem) * kFoldStride, 0.0);
-    const double ex[3] = {1.0, 0.0, 0.0}, ey[3] = {0.0, 1.0, 0.0}, ez[3] = {0.0, 0.0, 1.0},
-                 p0[3] = {0.0, 0.0, -10000.0};
-    for (int k = 0; k < sr.n_elem; ++k) {
-        const ElemRec &e = hs.elems[size_t(sr.first_elem + k)];
-        double *f = &hs.sun_fold[size_t(k) * kFoldStride];
-        double t[3];
-        mulvt(sd.Rsun, ex, t);
-        mulv(e.R, t, f + 0);
-        mulvt(sd.Rsun, ey, t);
-        mulv(e.R, t, f + 3);
-        mulvt(sd.Rsun, ez, t);
-        mulv(e.R, t, f + 9);
-        mulvt(sd.Rsun, p0, t);
-        for (int q = 0; q < 3; ++q) t[q] += sd.pos_sun_stage[q] - e.o[q];
-        mulv(e.R, t, f + 6);
-        for (int q = 0; q < 3; ++q) f[6 + q] += 1.0e-5 * f[9 + q];
-        f[12] = 1.0 / (f[11] + 0.00000000001);
-    }
-}
-
 void build_beam_lists(Context *cx, HostScene &hs) {
     const size_t ne = hs.elems.size();
     hs.beam_axis.assign(ne, float4{0.f, 0.f, 0.f, 2.f});
@@ -1363,7 +1329,6 @@ bool flatten(Context *cx, HostScene &hs) {
     }
     if (!sun_setup(cx, hs)) return false;
     build_beam_lists(cx, hs);
-    build_sun_fold(cx, hs);
     hs.dev.sunshape_on = cx->err_sun;
     hs.dev.errors_on = cx->err_opt;
     return true;
@@ -1727,7 +1692,8 @@ int run(Context *cx, unsigned seed) {
     }
     S.readback_ms = rr.readback_ms + std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
     S.records = cx->records.size();
-    S.intersections = cx->want_records ? uint64_t(cx->records.size()) : rr.intersections;
+    // over several ranks the records are this rank's, the counts the whole run's
+    S.intersections = (cx->want_records && cx->nranks <= 1) ? uint64_t(cx->records.size()) : rr.intersections;
     return int(cx->records.size());
 }
 
@@ -1792,9 +1758,6 @@ bool build_position(const Context *cx, const HostScene &hs, const double sun_xyz
         for (int k = 0; k < sr.n_elem; ++k)
             for (int q = 0; q < 9; ++q) out.elems[size_t(sr.first_elem + k)].R[q] = st0.elems[size_t(k)].R[q];
     }
-    h.elems = target ? out.elems : hs.elems;
-    build_sun_fold(&c, h);
-    out.sun_fold.swap(h.sun_fold);
     return true;
 }
 
@@ -2438,18 +2401,27 @@ int st_b200_explicit_rays(st_context_t p, st_uint_t n, const double *pos, const 
     cx->ex_cos.assign(cos, cos + 3 * n);
     return int(n);
 }
-int st_b200_add_flux_map(st_context_t p, int stage, int element, int kind, int nx, int ny, double x0, double x1,
-                         double y0, double y1, int absorbed_only) {
-    CTX(p, -1);
+static int add_flux_map(Context *cx, int stage, int element, int kind, int nx, int ny, double x0, double x1,
+                        double y0, double y1, int absorbed_only, int per_source) {
     if (cx->flux.size() >= size_t(kMaxFluxMaps) || nx <= 0 || ny <= 0 || stage < 1 || element < 1 || kind < 0 ||
         kind > 3 || !(x1 > x0 || kind == 1 || kind == 3) || !(y1 > y0) || ((kind == 1 || kind == 3) && !(x1 > 0))) {
         cx->log("invalid flux map request");
         return -1;
     }
     FluxMap m;
-    m.req = FluxMapReq{stage - 1, element - 1, kind, nx, ny, absorbed_only ? 1 : 0, x0, x1, y0, y1};
+    m.req = FluxMapReq{stage - 1, element - 1, kind, nx, ny, absorbed_only ? 1 : 0, x0, x1, y0, y1, per_source};
     cx->flux.push_back(m);
     return int(cx->flux.size()) - 1;
+}
+int st_b200_add_flux_map(st_context_t p, int stage, int element, int kind, int nx, int ny, double x0, double x1,
+                         double y0, double y1, int absorbed_only) {
+    CTX(p, -1);
+    return add_flux_map(cx, stage, element, kind, nx, ny, x0, x1, y0, y1, absorbed_only, 0);
+}
+int st_b200_add_source_flux_map(st_context_t p, int stage, int element, int kind, int nx, int ny, double x0,
+                                double x1, double y0, double y1, int absorbed_only) {
+    CTX(p, -1);
+    return add_flux_map(cx, stage, element, kind, nx, ny, x0, x1, y0, y1, absorbed_only, 1);
 }
 int st_b200_clear_flux_maps(st_context_t p) {
     CTX(p, -1);
@@ -2460,7 +2432,8 @@ int st_b200_flux_counts(st_context_t p, int map, unsigned long long *counts) {
     CTX(p, -1);
     if (map < 0 || size_t(map) >= cx->flux.size() || !counts) return -1;
     const auto &c = cx->flux[map].counts;
-    const size_t n = size_t(cx->flux[map].req.nx) * cx->flux[map].req.ny;
+    size_t n = size_t(cx->flux[map].req.nx) * cx->flux[map].req.ny;
+    if (cx->flux[map].req.per_source) n *= cx->stages.empty() ? 0 : cx->stages[0].elems.size();
     for (size_t i = 0; i < n; ++i) counts[i] = i < c.size() ? c[i] : 0ull;
     return 1;
 }
@@ -2475,6 +2448,10 @@ int st_b200_flux_stats(st_context_t p, int map, double dni, st_b200_flux_stats_t
     const FluxMap &fm = cx->flux[map];
     const FluxMapReq &q = fm.req;
     const size_t nb = size_t(q.nx) * q.ny;
+    if (q.per_source) {
+        cx->log("flux statistics are computed for whole-element maps, not per-source maps");
+        return -1;
+    }
     if (fm.counts.size() != nb || cx->sun_rays == 0) {
         cx->log("flux statistics need a completed run");
         return -1;

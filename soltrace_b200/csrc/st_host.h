@@ -29,13 +29,13 @@ struct HostScene {
     std::vector<float4> cell_disc;  // sun-plane grid entries: disc centre x, y, radius, element
     std::vector<float4> cell_par;   // sun-plane grid entries: footprint parallelogram (dual basis rows)
     std::vector<double> inv_cdf;  // table-sunshape inverse CDF (kSunInvCells + 1 entries)
-    std::vector<double> sun_fold; // per first-stage element: sun plane -> element map (SceneDev::sun_fold)
     SceneDev dev;  // stages, sun scalars and flags; device pointers are filled by gpu_run
 };
 
 struct FluxMapReq {
     int stage, elem, kind, nx, ny, absorbed_only;
     double x0, x1, y0, y1;
+    int per_source = 0;  // one nx x ny map per first-stage element (the rays' first heliostat)
 };
 
 struct RunRequest {
@@ -84,14 +84,13 @@ struct RunResult {
 };
 
 // One sun position of a batched run (st_b200_sim_run_batch): the tables that depend on the
-// sun (sun frame and box, sun-plane grid, folded maps) and, when the first stage tracks the
+// sun (sun frame and box, sun-plane grid) and, when the first stage tracks the
 // sun, the scene's elements with the first stage re-aimed.
 struct SunPosition {
     SunDev sun;                       // device pointers are filled by gpu_run_batch
     std::vector<int> cell_start;
     std::vector<float4> cell_disc, cell_par;
     std::vector<ElemRec> elems;       // empty: the scene's elements
-    std::vector<double> sun_fold;
     uint64_t n_hits = 0;
     uint32_t seed = 0;
 };

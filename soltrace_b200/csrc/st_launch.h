@@ -30,25 +30,9 @@ __host__ __device__ inline int stage_search_kind(const StageRec &st) {
            ((!st.grid_on && st.bvh_off < 0) ? kSearchBrute : 0);
 }
 constexpr int kWfBruteMinBlocks = 8;      // search kernels of stages tested element by element
-#ifndef ST_BRUTE_SHADE_MIN_BLOCKS
-#define ST_BRUTE_SHADE_MIN_BLOCKS 6
-#endif
-// search kernels of brute-force flat or closed-form stages shade their hits in the same kernel
-#ifndef ST_SEARCH_SHADES
-#define ST_SEARCH_SHADES 1
-#endif
-// search kernels of brute-force flat or closed-form stages, which also shade their hits
-constexpr int kWfBruteShadeMinBlocks = ST_BRUTE_SHADE_MIN_BLOCKS;
 constexpr int kWfFlatSearchMinBlocks = 5;  // search kernels of flat-only stages
-#ifndef ST_FIRST_FLAT_MIN_BLOCKS
-#define ST_FIRST_FLAT_MIN_BLOCKS 8
-#endif
-constexpr int kWfFirstFlatMinBlocks = ST_FIRST_FLAT_MIN_BLOCKS;  // first kernel on a flat-only first stage
-// the first kernel on a heliostat field also searches and shades the rays that reach a
-// brute-force closed-form stage (the receiver) instead of queueing them
-#ifndef ST_FIRST_CONTINUE
-#define ST_FIRST_CONTINUE 0
-#endif
+constexpr int kWfFirstFlatMinBlocks = 8;   // first kernel on a flat-only first stage
+
 constexpr int kWfClosedShadeMinBlocks = 4; // shade kernel of scenes with closed-form surfaces only
 
 enum RunFlags : unsigned {

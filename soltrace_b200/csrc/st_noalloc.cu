@@ -171,7 +171,6 @@ extern "C" int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsig
     S.sun.cell_disc = d_cdisc;
     S.sun.cell_par = d_cpar;
     S.sun.inv_cdf = nullptr;
-    S.sun_fold = nullptr;
     S.optics = nullptr;
     S.tables = nullptr;
     S.seed = seed;

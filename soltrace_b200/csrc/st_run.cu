@@ -16,11 +16,6 @@
 #include "st_host.h"
 #include "st_launch.h"
 
-// mixed precision on flat first stages takes the folded sun -> element maps
-#ifndef ST_SUN_FOLD
-#define ST_SUN_FOLD 1
-#endif
-
 namespace stb {
 
 namespace {
@@ -72,9 +67,8 @@ struct Workspace {
     DevBuf wf_sid, wf_raynum, wf_draw, wf_meta, wf_fe0, wf_p, wf_c, wf_q0, wf_q1, wf_qs, wf_counts;
     DevBuf save_rows[2], save_count, replay_rows, replay_fe0;  // stage-data save / replay
     DevBuf ecount, ecursor, etotal, s_sid, s_el, s_idx;
-    DevBuf sun_fold;
     // batched runs: per-position sun tables, element copies, run states, counters, accumulators
-    DevBuf pos_cells, pos_disc, pos_par, pos_elems, pos_fold, pos_rs, pos_ctr, pos_acc;
+    DevBuf pos_cells, pos_disc, pos_par, pos_elems, pos_rs, pos_ctr, pos_acc;
     std::vector<cudaEvent_t> events;
     // autotuned kernel variants per precision (FP64, mixed), chosen on the first run
     struct Tuning {
@@ -257,11 +251,6 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     CK(upload(d_inv_cdf, hs.inv_cdf, st, out.h2d_bytes));
     CK(upload(d_expos, rq.ex_pos, st, out.h2d_bytes));
     CK(upload(d_excos, rq.ex_cos, st, out.h2d_bytes));
-    // mixed precision on a flat first stage culled by the sun-plane grid: the grid probe and
-    // the first trace kernel take the folded sun -> element maps
-    const bool fold = ST_SUN_FOLD && rq.precision && rq.ex_pos.empty() && !rq.replay && hs.dev.sun.grid_on &&
-                      !hs.dev.sun.point_source && hs.dev.stages[0].flat_only && !hs.sun_fold.empty();
-    if (fold) CK(upload(ws.sun_fold, hs.sun_fold, st, out.h2d_bytes));
 
     SceneDev S = hs.dev;
     S.elems = d_elems.as<ElemRec>();
@@ -288,15 +277,16 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     S.explicit_rays = explicit_mode ? 1 : 0;
     S.ex_pos = d_expos.as<double>();
     S.ex_cos = d_excos.as<double>();
-    S.sun_fold = fold ? ws.sun_fold.as<double>() : nullptr;
 
     // run-level accumulators: [first_hits | absorbed | delivered | flux bins of every map]
     const size_t ne = hs.elems.size();
     std::vector<size_t> flux_off;
     size_t acc_n = 3 * ne;
+    const size_t n_src0 = size_t(hs.dev.stages[0].n_elem);
+    auto map_size = [n_src0](const FluxMapReq &f) { return size_t(f.nx) * f.ny * (f.per_source ? n_src0 : 1); };
     for (const auto &f : rq.flux) {
         flux_off.push_back(acc_n);
-        acc_n += size_t(f.nx) * f.ny;
+        acc_n += map_size(f);
     }
     if (rq.flux.size() > size_t(kMaxFluxMaps)) {
         out.error = "too many flux maps";
@@ -373,6 +363,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             fd.nx = f.nx;
             fd.ny = f.ny;
             fd.absorbed_only = f.absorbed_only;
+            fd.n_src = f.per_source ? int(n_src0) : 0;
             fd.x0 = f.x0;
             fd.x1 = f.x1;
             fd.y0 = f.y0;
@@ -762,8 +753,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
         out.delivered.assign(accv.begin() + 2 * ne, accv.begin() + 3 * ne);
         out.flux.clear();
         for (size_t m = 0; m < rq.flux.size(); ++m)
-            out.flux.emplace_back(accv.begin() + flux_off[m],
-                                  accv.begin() + flux_off[m] + size_t(rq.flux[m].nx) * rq.flux[m].ny);
+            out.flux.emplace_back(accv.begin() + flux_off[m], accv.begin() + flux_off[m] + map_size(rq.flux[m]));
         out.readback_ms += ms_since(tr);
         if (fe_fail) {
             // the reference throws at such a query (vshot.cpp:177-178) and returns no result
@@ -792,7 +782,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     } while (0)
 
 // Batched run of K sun positions (st_b200_sim_run_batch).  Every position p has its own
-// scene view S_p (its sun frame, sun-plane grid, folded maps and, when tracking, elements),
+// scene view S_p (its sun frame, sun-plane grid and, when tracking, elements),
 // run state, counters and accumulators; its rays draw from the streams of its own seed, so
 // position p's results are those of a single run with that sun and seed.  Positions advance
 // in waves: a wave queues, for every position still short of its hits, the sun rays its hit
@@ -840,8 +830,7 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
     std::vector<int> cells;
     std::vector<float4> disc, par;
     std::vector<ElemRec> pelems;
-    std::vector<double> pfold;
-    std::vector<size_t> off_cells(K), off_disc(K), off_elems(K), off_fold(K);
+    std::vector<size_t> off_cells(K), off_disc(K), off_elems(K);
     for (size_t p = 0; p < K; ++p) {
         const SunPosition &sp = pos[p];
         off_cells[p] = cells.size();
@@ -851,14 +840,11 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
         par.insert(par.end(), sp.cell_par.begin(), sp.cell_par.end());
         off_elems[p] = sp.elems.empty() ? size_t(-1) : pelems.size();
         pelems.insert(pelems.end(), sp.elems.begin(), sp.elems.end());
-        off_fold[p] = sp.sun_fold.empty() ? size_t(-1) : pfold.size();
-        pfold.insert(pfold.end(), sp.sun_fold.begin(), sp.sun_fold.end());
     }
     CK(upload(ws.pos_cells, cells, st, h2d));
     CK(upload(ws.pos_disc, disc, st, h2d));
     CK(upload(ws.pos_par, par, st, h2d));
     CK(upload(ws.pos_elems, pelems, st, h2d));
-    CK(upload(ws.pos_fold, pfold, st, h2d));
 
     SceneDev S0 = hs.dev;
     S0.elems = ws.elems.as<ElemRec>();
@@ -877,15 +863,16 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
     S0.precision = rq.precision;
     S0.explicit_rays = 0;
     S0.ex_pos = S0.ex_cos = nullptr;
-    S0.sun_fold = nullptr;
 
     const int nst = S0.n_stages;
     const size_t ne = hs.elems.size();
     std::vector<size_t> flux_off;
     size_t acc_n = 3 * ne;
+    const size_t n_src0 = size_t(hs.dev.stages[0].n_elem);
+    auto map_size = [n_src0](const FluxMapReq &f) { return size_t(f.nx) * f.ny * (f.per_source ? n_src0 : 1); };
     for (const auto &f : rq.flux) {
         flux_off.push_back(acc_n);
-        acc_n += size_t(f.nx) * f.ny;
+        acc_n += map_size(f);
     }
     if (rq.flux.size() > size_t(kMaxFluxMaps)) {
         out.error = "too many flux maps";
@@ -915,10 +902,6 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
         S.sun.cell_par = ws.pos_par.as<float4>() + off_disc[p];
         S.sun.inv_cdf = hs.inv_cdf.empty() ? nullptr : ws.inv_cdf.as<double>();
         if (off_elems[p] != size_t(-1)) S.elems = ws.pos_elems.as<ElemRec>() + off_elems[p];
-        // the folded maps serve mixed-precision runs on flat first stages culled by the grid
-        if (ST_SUN_FOLD && rq.precision && off_fold[p] != size_t(-1) && S.sun.grid_on && !S.sun.point_source &&
-            S.stages[0].flat_only)
-            S.sun_fold = ws.pos_fold.as<double>() + off_fold[p];
         S.seed = pos[p].seed;
         unsigned long long *a = acc + p * acc_n;
         S.n_flux = int(rq.flux.size());
@@ -931,6 +914,7 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
             fd.nx = f.nx;
             fd.ny = f.ny;
             fd.absorbed_only = f.absorbed_only;
+            fd.n_src = f.per_source ? int(n_src0) : 0;
             fd.x0 = f.x0;
             fd.x1 = f.x1;
             fd.y0 = f.y0;
@@ -1104,7 +1088,7 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
         const unsigned long long *a = accv.data() + p * acc_n;
         r.absorbed.assign(a + ne, a + 2 * ne);
         for (size_t m = 0; m < rq.flux.size(); ++m)
-            r.flux.emplace_back(a + flux_off[m], a + flux_off[m] + size_t(rq.flux[m].nx) * rq.flux[m].ny);
+            r.flux.emplace_back(a + flux_off[m], a + flux_off[m] + map_size(rq.flux[m]));
     }
     if (rq.precision ? take_fe_failures_mixed() : take_fe_failures_fp64()) {
         out.error = "Interpolation failed to find nearby nodes to ray hit in FEA surface.";

@@ -23,8 +23,6 @@ constexpr int kMaxStages = 16;
 constexpr int kMaxFluxMaps = 8;
 constexpr int kSunCdfCells = 4096;
 constexpr int kSunInvCells = 8192;
-// doubles per first-stage element in SceneDev::sun_fold
-constexpr int kFoldStride = 16;
 
 // surface model codes after coretrace/input.cpp:288-366 translation
 enum SurfType : int {
@@ -106,6 +104,8 @@ struct BvhNode {
 struct FluxMapDev {
     int stage, elem;      // 0-based stage, 0-based element index within the stage
     int kind, nx, ny, absorbed_only;
+    int n_src;            // > 0: one map per first-stage element the ray first hit (n_src maps)
+    int pad_;
     double x0, x1, y0, y1;
     unsigned long long *bins;
 };
@@ -157,12 +157,6 @@ struct SceneDev {
     const double *ex_pos, *ex_cos;
     int n_flux;
     FluxMapDev flux[kMaxFluxMaps];
-    // Mixed precision, sun rays on a flat first stage culled by the sun-plane grid: per
-    // first-stage element, the affine map from the sun-plane point (xs, ys) to the element
-    // frame that the chain sun frame -> stage -> global -> stage -> element composes to
-    // (kFoldStride doubles: the columns of xs and ys, the offset with the 1e-5 nudge, the
-    // direction, 1 / (direction z + 1e-11)); null when unused
-    const double *sun_fold;
 };
 
 // One intersection record as the reference stores it (coretrace/types.h:239-246),

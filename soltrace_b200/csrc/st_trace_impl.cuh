@@ -326,14 +326,6 @@ __device__ inline int nearest_sun_grid_lazy(const SceneDev &S, const StageRec &s
         const int j = __float_as_int(sun.cell_disc[k].w);
         const ElemRec &e = S.elems[st.first_elem + j];
         if (!e.enabled) continue;
-        if (MIXED && ET == kEtFlat && S.sun_fold) {  // the folded sun -> element map
-            double t, ox, oy;
-            if (fold_flat_test(S.sun_fold + size_t(j) * kFoldStride, e, xs, ys, t, ox, oy) && t < bp) {
-                bp = t;
-                best = j;
-            }
-            continue;
-        }
         if (!have_ray) {
             sun_ray_in_stage(S, xs, ys, ps, cs);
             have_ray = true;
@@ -490,12 +482,15 @@ __host__ __device__ inline double gui_cyl_arc(double x, double z, double R) {
     return (x < 0) ? -(kPiD * R / 2.0 + R * acos(fabs(x) / R)) : kPiD * R / 2.0 + R * acos(x / R);
 }
 
+// fe0: the ray's first first-stage element (global index, first stage first; -1 none), which
+// selects the map of a per-source flux map
 template <int MIXED>
-__device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed, const double pe[3]) {
+__device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed, const double pe[3], int fe0) {
     for (int m = 0; m < S.n_flux; ++m) {
         const FluxMapDev &f = S.flux[m];
         if (f.stage != si || f.elem != ej) continue;
         if (f.absorbed_only && !absorbed) continue;
+        if (f.n_src > 0 && (fe0 < 0 || fe0 >= f.n_src)) continue;
         int ix, iy;
         if (f.kind >= 2) {  // the GUI's statistics rules, in double
             if (f.kind == 2) {
@@ -535,7 +530,8 @@ __device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed
             iy = int(dy);
         }
         if (ix < 0 || ix >= f.nx || iy < 0 || iy >= f.ny) continue;
-        atomicAdd(&f.bins[iy * f.nx + ix], 1ull);
+        const size_t src = f.n_src > 0 ? size_t(fe0) * size_t(f.nx) * size_t(f.ny) : 0;
+        atomicAdd(&f.bins[src + size_t(iy) * f.nx + ix], 1ull);
     }
 }
 
@@ -1303,7 +1299,7 @@ __device__ __forceinline__ int wf_shade_hit(const SceneDev &S, const TraceOut &O
             O.recs[slot] = rec;
         }
     }
-    if (S.n_flux) bin_flux<MIXED>(S, si, j, absorbed, h.pe);
+    if (S.n_flux) bin_flux<MIXED>(S, si, j, absorbed, h.pe, r.fe0);
     if (absorbed) {
         warp_count(O.absorbed, st.first_elem + j);
         if (si == S.n_stages - 1 && r.fe0 >= 0) warp_count(O.delivered, r.fe0);
@@ -1332,38 +1328,13 @@ __device__ __forceinline__ int wf_shade_hit(const SceneDev &S, const TraceOut &O
     return kWfSearch;
 }
 
-// The first shading of a sun ray on a flat first-stage element through its folded map
-// (mixed precision; the probe found the element with the same arithmetic).
-template <int MIXED, int RECORDS>
-__device__ __forceinline__ int wf_shade_fold(const SceneDev &S, const TraceOut &O, WfBlockCtr &c, WfRay &r, double xs,
-                                             double ys) {
-    const int j = r.next_j;
-    r.next_j = -1;
-    const ElemRec &e = S.elems[S.stages[0].first_elem + j];
-    const double *f = S.sun_fold + size_t(j) * kFoldStride;
-    Hit h;
-    double t, ox, oy;
-    if (!fold_flat_test(f, e, xs, ys, t, ox, oy)) return kWfDone;  // (as wf_exit_stage for a first-stage miss)
-    h.pe[0] = ox;
-    h.pe[1] = oy;
-    h.pe[2] = 0.0;
-    for (int q = 0; q < 3; ++q) h.ce[q] = f[9 + q];
-    h.back = (h.ce[2] < 0) ? 0 : 1;
-    h.n[0] = h.back ? -0.0 : 0.0;
-    h.n[1] = h.back ? -0.0 : 0.0;
-    h.n[2] = h.back ? -1.0 : 1.0;
-    h.plen = t;
-    return wf_shade_hit<MIXED, RECORDS>(S, O, c, r, e, j, h);
-}
-
 // First kernel: the batch's numbered rays (hit-list entries below the cut-off at the
 // requested hit count; k_advance applies the same rule after the trace) enter the first
 // stage and are shaded on the element the probe found.
 // FLAT 1: the first stage holds flat elements only; 2: besides, its search kind is
 // kSearchFlat, and the rays it reflects are searched for blocking in this kernel (their
 // results go to round 0's shade queue and to the search queue of the ray's stage).
-// FOLD (mixed precision, FLAT >= 1, S.sun_fold set): the first hit through the folded sun maps.
-template <int MIXED, int RECORDS, int FLAT, int FOLD = 0>
+template <int MIXED, int RECORDS, int FLAT>
 __global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kWfShadeMinBlocks) k_wf_first(
     const __grid_constant__ SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx, const uint32_t *total,
     const RunState *rs, TraceOut O, WfState W, const __grid_constant__ WfQueues Q) {
@@ -1382,11 +1353,9 @@ __global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kW
     const uint32_t stride = gridDim.x * kTraceBlock;
     // whole blocks in the loop (block-wide queue appends)
     const uint32_t n_round = (n + kTraceBlock - 1) / kTraceBlock * kTraceBlock;
-    constexpr bool fold = MIXED && FLAT && FOLD;
     for (uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x; i < n_round; i += stride) {
         bool live = false;
         WfRay r;
-        double xs = 0.0, ys = 0.0;
         if (i < n) {
             const uint32_t idx = hit_idx ? hit_idx[i] : i;
             live = idx < take;
@@ -1395,12 +1364,8 @@ __global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kW
                 r.raynum = raynum_base + idx + 1;
                 RayRng rng;
                 rng.init(S.seed, r.sid, 0);
-                if constexpr (fold) {  // only the sun-plane point: the folded map gives the element-frame ray
-                    xs = S.sun.xmin + (S.sun.xmax - S.sun.xmin) * rng.u();
-                    ys = S.sun.ymin + (S.sun.ymax - S.sun.ymin) * rng.u();
-                } else {
-                    make_ray(S, r.sid, rng, r.p, r.c, xs, ys);
-                }
+                double xs, ys;
+                make_ray(S, r.sid, rng, r.p, r.c, xs, ys);
                 r.draw = rng.k;
                 r.si = 0;
                 r.hits = 0;
@@ -1414,22 +1379,9 @@ __global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kW
         if (live) {
             wf_stage_enter(c, 0, r.raynum);
             // (an entry without a known element is searched in the first round)
-            if (r.next_j < 0)
-                status = kWfSearch;
-            else if constexpr (fold)
-                status = wf_shade_fold<MIXED, RECORDS>(S, O, c, r, xs, ys);
-            else
-                status = wf_shade<MIXED, RECORDS, FLAT ? 1 : 0>(S, O, c, r);
+            status = (r.next_j >= 0) ? wf_shade<MIXED, RECORDS, FLAT ? 1 : 0>(S, O, c, r) : int(kWfSearch);
             // FLAT 2: the ray still in the first stage is searched here (its blocking search)
             if (FLAT == 2 && status == kWfSearch && r.si == 0) status = wf_search<MIXED, RECORDS, kSearchFlat>(S, O, c, r);
-#if ST_FIRST_CONTINUE
-            // a ray that left the field for a brute-force stage of closed-form elements (the
-            // receiver) is searched and shaded there too, without storing its state
-            if (FLAT == 2 && status == kWfSearch && Q.queue_kind[Q.stage_queue[r.si]] == (kSearchBrute | kSearchClosed)) {
-                status = wf_search<MIXED, RECORDS, kSearchBrute | kSearchClosed>(S, O, c, r);
-                if (status == kWfShade) status = wf_shade<MIXED, RECORDS, 0, 1>(S, O, c, r);
-            }
-#endif
             if (status != kWfDone) {
                 wf_store(W, i, r, true);
                 if (status == kWfSearch) kb = Q.stage_queue[r.si];
@@ -1483,17 +1435,9 @@ __global__ void __launch_bounds__(kTraceBlock, kWfShadeMinBlocks) k_wf_replay(
 // Search kernel of search kind KIND, over queue k of round r: rays that find an element go
 // to the round's shade queue, those that move on to another stage to the next round's
 // search queue of that stage.
-// Brute-force stages of flat or closed-form elements (a receiver, a secondary mirror) are
-// shaded in their search kernel: the hit found is shaded at once, without a trip of the ray
-// state through the shade queue.
-template <int KIND>
-struct SearchShades {
-    static constexpr bool value = ST_SEARCH_SHADES && (KIND & kSearchBrute) && (KIND & (kSearchFlat | kSearchClosed));
-};
 template <int KIND>
 struct SearchBounds {
-    static constexpr int min_blocks = SearchShades<KIND>::value ? kWfBruteShadeMinBlocks
-                                      : (KIND & kSearchBrute) ? kWfBruteMinBlocks
+    static constexpr int min_blocks = (KIND & kSearchBrute) ? kWfBruteMinBlocks
                                       : (KIND & kSearchFlat)  ? kWfFlatSearchMinBlocks
                                                               : kWfSearchMinBlocks;
 };
@@ -1517,9 +1461,6 @@ __global__ void __launch_bounds__(kTraceBlock, SearchBounds<KIND>::min_blocks) k
             i = q_in[q];
             WfRay ray = wf_load(W, i);
             status = wf_search<MIXED, RECORDS, KIND>(S, O, c, ray);
-            if (SearchShades<KIND>::value && status == kWfShade)
-                status = wf_shade<MIXED, RECORDS, (KIND & kSearchFlat) ? 1 : 0, (KIND & kSearchClosed) ? 1 : 0>(S, O, c,
-                                                                                                            ray);
             if (status != kWfDone) wf_store(W, i, ray, false);
             if (status == kWfSearch) kb = Q.stage_queue[ray.si];
         }
@@ -1600,13 +1541,11 @@ static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t 
                      const uint32_t *total, const RunState *rs, const TraceOut &O, const WfState &W,
                      const WfQueues &Q, const ReplayIn *replay, cudaStream_t st) {
     // persistent grids: every block the kernels can keep resident on every SM
-    static int per_sm[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    static int per_sm[6] = {0, 0, 0, 0, 0, 0};
     if (per_sm[0] == 0) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_wf_first<MIXED, RECORDS, 0>, kTraceBlock, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[4], k_wf_first<MIXED, RECORDS, 1>, kTraceBlock, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[5], k_wf_first<MIXED, RECORDS, 2>, kTraceBlock, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[6], k_wf_first<MIXED, RECORDS, 1, 1>, kTraceBlock, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[7], k_wf_first<MIXED, RECORDS, 2, 1>, kTraceBlock, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_wf_shade<MIXED, RECORDS, 0>, kTraceBlock, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[3], k_wf_shade<MIXED, RECORDS, 1>, kTraceBlock, 0);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_wf_finish<MIXED, RECORDS>, kTraceBlock, 0);
@@ -1622,15 +1561,9 @@ static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t 
     cudaMemsetAsync(Q.counts, 0, sizeof(uint32_t) * (R + 1) * (nq + 1), st);
     if (replay)
         k_wf_replay<MIXED, RECORDS><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, O, W, *replay, Q);
-    else if (stage_search_kind(S.stages[0]) == kSearchFlat && MIXED && S.sun_fold)  // heliostat fields, folded maps
-        k_wf_first<MIXED, RECORDS, 2, 1><<<sms * per_sm[7], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total,
-                                                                                    rs, O, W, Q);
     else if (stage_search_kind(S.stages[0]) == kSearchFlat)  // heliostat fields: blocking search fused
         k_wf_first<MIXED, RECORDS, 2><<<sms * per_sm[5], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs,
                                                                                  O, W, Q);
-    else if (S.stages[0].flat_only && MIXED && S.sun_fold)  // a first stage of flat elements only, folded maps
-        k_wf_first<MIXED, RECORDS, 1, 1><<<sms * per_sm[6], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total,
-                                                                                    rs, O, W, Q);
     else if (S.stages[0].flat_only)  // a first stage of flat elements only
         k_wf_first<MIXED, RECORDS, 1><<<sms * per_sm[4], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs,
                                                                                  O, W, Q);

@@ -57,6 +57,8 @@ EXTENSIONS = {
     "st_b200_explicit_rays": (C.c_int, [C.c_void_p, st_uint_t, c_double_p, c_double_p]),
     "st_b200_add_flux_map": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
                                        C.c_double, C.c_double, C.c_double, C.c_int]),
+    "st_b200_add_source_flux_map": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double,
+                                              C.c_double, C.c_double, C.c_double, C.c_int]),
     "st_b200_clear_flux_maps": (C.c_int, [C.c_void_p]),
     "st_b200_flux_counts": (C.c_int, [C.c_void_p, C.c_int, _u64p]),
     "st_b200_run_stats": (C.c_int, [C.c_void_p, C.POINTER(Stats)]),
@@ -93,6 +95,13 @@ class B200Api(StApi):
         if rc < 0:
             raise RuntimeError("st_b200_flux_counts failed")
         return out.reshape(ny, nx)
+
+    def source_flux(self, ctx, idx: int, n_src: int, nx: int, ny: int) -> np.ndarray:
+        """Counts of a per-source flux map: (n_src, ny, nx)."""
+        out = np.zeros(n_src * nx * ny, dtype=np.uint64)
+        if self.st_b200_flux_counts(ctx, idx, out.ctypes.data_as(_u64p)) < 0:
+            raise RuntimeError("st_b200_flux_counts failed")
+        return out.reshape(n_src, ny, nx)
 
     def flux_stats(self, ctx, idx: int, dni: float) -> dict:
         """Peak/min/mean flux, sigma, uniformity and uncertainties of flux map `idx`."""
