@@ -158,7 +158,9 @@ bool read_sun(Reader &r) {
         for (int i = 0; i < n; ++i) {
             if (!r.next() || !two_numbers(r.line, ang[i], inten[i])) return r.fail("bad sunshape table row");
         }
-        if (st_sun_userdata(r.ctx, st_uint_t(n), ang.data(), inten.data()) < 0) return r.fail("st_sun_userdata failed");
+        // as the CLI does (strace/main.cpp:114-129), the setter's result is not checked: a table of
+        // two rows or fewer is refused by st_sun_userdata and leaves the sunshape table unset
+        st_sun_userdata(r.ctx, st_uint_t(n), ang.data(), inten.data());
     }
     return true;
 }

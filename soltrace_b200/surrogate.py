@@ -66,7 +66,6 @@ class Mlp:
         self.mb = [torch.zeros_like(b) for b in self.b]
         self.vb = [torch.zeros_like(b) for b in self.b]
         self.step_count = 0
-        self.stream = None  # the current torch stream, taken per call
         self.acts = []
 
     # ---- kernels ----
@@ -158,3 +157,146 @@ class Mlp:
 
     def error(self) -> int:
         return self.api.lib.st_b200_mlp_error()
+
+
+# ------------------------------------------------------------------------------------
+# Training data from the tracer
+# ------------------------------------------------------------------------------------
+RECEIVER_IMAGE = (2, 1, 1, IMG, IMG, 0.0, 4.0, -5.0, 5.0, 1)  # receiver: angle x height, absorbed rays
+
+
+class FieldTracer:
+    """The headline field (2,000 flat heliostats, cylindrical receiver, Buie CSR 0.1) in one
+    context of the product library, re-aimed per call: every heliostat aims at the receiver
+    centre plus its own offset (east, up) by the bisector rule, under a given sun and slope
+    error.  trace() returns every heliostat's receiver image in kW per bin at 1000 W/m2."""
+
+    def __init__(self, api, n_helio: int = 2000, tower_h: float = 150.0, precision: int = 1):
+        self.api, self.n, self.tower_h = api, n_helio, tower_h
+        self.sc = scenes.field_scene(n_helio, 1000, dynamic_group=False)
+        self.xy = scenes.field_layout(n_helio)
+        self.ctx = api.st_create_context()
+        scenes.push(api, self.ctx, self.sc)
+        api.st_b200_set_records(self.ctx, 0)
+        api.st_b200_set_precision(self.ctx, precision)
+        self.img = api.st_b200_add_source_flux_map(self.ctx, *RECEIVER_IMAGE)
+        self.whole = api.st_b200_add_flux_map(self.ctx, *RECEIVER_IMAGE)
+
+    def close(self):
+        self.api.st_free_context(self.ctx)
+
+    def aim(self, sun: np.ndarray, offsets: np.ndarray, sigma: float):
+        api, ctx = self.api, self.ctx
+        s = np.asarray(sun, dtype=np.float64) / np.linalg.norm(sun)
+        api.st_sun_xyz(ctx, *(1.0e4 * s))
+        for k, (x, y) in enumerate(self.xy):
+            pos = np.array([x, y, 5.0])
+            t = np.array([offsets[k, 0], 0.0, self.tower_h + offsets[k, 1]]) - pos
+            n = s + t / np.linalg.norm(t)
+            a = pos + 100.0 * n / np.linalg.norm(n)
+            api.st_element_aim(ctx, 0, k, float(a[0]), float(a[1]), float(a[2]))
+        from .scenes import OpticFace, OpticSet, push_optic
+        push_optic(api, ctx, 0, OpticSet("helio", OpticFace("g", refl=0.9, slope=sigma), OpticFace("g", refl=0.9, slope=sigma)))
+
+    def trace(self, sun, offsets, sigma: float, hits: int, seed: int):
+        """(per-heliostat images (n, 32, 32), whole-receiver map (32, 32)), kW per bin."""
+        api, ctx = self.api, self.ctx
+        self.aim(sun, offsets, sigma)
+        api.st_sim_params(ctx, int(hits), 2_000_000_000 - 1, 0)
+        api.st_b200_set_max_sun_rays(ctx, 40 * int(hits))
+        if api.run(ctx, seed) < 0:
+            raise RuntimeError("; ".join(api.messages(ctx)))
+        st = api.stats(ctx)
+        box = api.sun_stats(ctx)
+        ppr_kw = 1000.0 * (box["xmax"] - box["xmin"]) * (box["ymax"] - box["ymin"]) / st["sun_rays"] / 1000.0
+        imgs = api.source_flux(ctx, self.img, self.n, IMG, IMG).astype(np.float32) * ppr_kw
+        whole = api.flux(ctx, self.whole, IMG, IMG).astype(np.float64) * ppr_kw
+        return imgs, whole
+
+    def features(self, sun, offsets, sigma: float) -> np.ndarray:
+        """The network's inputs per heliostat: sun vector, position (km), aim offset (m),
+        slope sigma - 2 (mrad)."""
+        s = np.asarray(sun, dtype=np.float64) / np.linalg.norm(sun)
+        f = np.zeros((self.n, 8), dtype=np.float32)
+        f[:, 0:3] = s
+        f[:, 3:5] = self.xy / 1000.0
+        f[:, 5:7] = offsets
+        f[:, 7] = sigma - 2.0
+        return f
+
+
+def random_situation(rng, n: int):
+    """A random sun (elevation 20-80 deg, azimuth 100-260 deg from north), aim offsets
+    uniform in [-1, 1] m and slope error uniform in [1, 3] mrad."""
+    sun = scenes.sun_vector(rng.uniform(20.0, 80.0), rng.uniform(100.0, 260.0))
+    return sun, rng.uniform(-1.0, 1.0, size=(n, 2)), float(rng.uniform(1.0, 3.0))
+
+
+def make_dataset(tracer: FieldTracer, n_traces: int, hits: int, seed: int = 0):
+    """Inputs (n_traces * n, 8) float32 and target images (n_traces * n, 1024) float32 (kW per
+    bin), on the device."""
+    import torch
+    rng = np.random.default_rng(seed)
+    xs, ts = [], []
+    for i in range(n_traces):
+        sun, off, sig = random_situation(rng, tracer.n)
+        imgs, _ = tracer.trace(sun, off, sig, hits, seed * 100_003 + i)
+        xs.append(torch.from_numpy(tracer.features(sun, off, sig)).cuda())
+        ts.append(torch.from_numpy(imgs.reshape(tracer.n, IMG * IMG)).cuda())
+    return torch.cat(xs), torch.cat(ts)
+
+
+def train(net: Mlp, x, t, steps: int, batch: int = 8192, lr: float = 1e-3, seed: int = 0, target_scale: float = None):
+    """Adam on random minibatches, the learning rate decayed by 10 over the run.  Targets are
+    divided by target_scale (default: their 99.9th percentile) so the network sees O(1)
+    values; returns (scale, loss history)."""
+    import torch
+    if target_scale is None:
+        target_scale = float(torch.quantile(t.flatten()[:: max(1, t.numel() // 4_000_000)].float(), 0.999).item())
+        target_scale = max(target_scale, 1e-6)
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    xb = x.to(torch.bfloat16)
+    hist = []
+    for k in range(steps):
+        idx = torch.randint(0, x.shape[0], (batch,), device="cuda", generator=g)
+        step_lr = lr * (0.1 ** (k / max(steps - 1, 1)))
+        loss = net.train_step(xb[idx], t[idx] / target_scale, lr=step_lr)
+        if k % 50 == 0 or k == steps - 1:
+            hist.append(float(loss.item()))
+    return target_scale, hist
+
+
+def predict_images(net: Mlp, feats, target_scale: float):
+    """Per-heliostat images (n, 1024) in kW per bin (negative network outputs clipped to 0)."""
+    import torch
+    x = torch.as_tensor(feats).cuda().to(torch.bfloat16)
+    return torch.clamp(net.forward(x), min=0.0) * target_scale
+
+
+def peak_error(pred_map: np.ndarray, trace_map: np.ndarray) -> float:
+    """|peak(pred) - peak(trace)| / peak(trace) of two field maps (kW per bin)."""
+    return abs(float(pred_map.max()) - float(trace_map.max())) / max(float(trace_map.max()), 1e-30)
+
+
+def optimise_aims(net: Mlp, feats: np.ndarray, target_scale: float, iters: int = 60, step: float = 0.05):
+    """Aim offsets that flatten the predicted receiver map: gradient descent, through the
+    network's backward kernels to its inputs, on sum(F^4) / sum(F)^4 of the field map F (a
+    smooth stand-in for the peak over the total), offsets kept in [-1, 1] m.  Returns the
+    offsets (n, 2)."""
+    import torch
+    x = torch.as_tensor(feats).cuda().clone()
+    n = x.shape[0]
+    for _ in range(iters):
+        out = net.forward(x.to(torch.bfloat16))
+        y = torch.clamp(out, min=0.0)
+        f = y.sum(0).double()
+        s1, s4 = f.sum(), (f ** 4).sum()
+        dldf = 4 * f ** 3 / s1 ** 4 - 4 * s4 / s1 ** 5        # d(sum F^4 / (sum F)^4) / dF
+        dldf = (dldf / dldf.abs().max().clamp(min=1e-300)).float()
+        # every heliostat's image adds to F: the same dL/dF for each, through the clipping
+        dy = (dldf.unsqueeze(0) * (out > 0)).to(torch.bfloat16).contiguous()
+        _, _, dx = net.backward(dy, want_input_grad=True)
+        g = dx[:, 5:7]
+        g = g / g.abs().max().clamp(min=1e-30)
+        x[:, 5:7] = (x[:, 5:7] - step * g).clamp(-1.0, 1.0)
+    return x[:, 5:7].cpu().numpy().astype(np.float64)
