@@ -225,9 +225,9 @@ def config_lines(api, args) -> dict:
     """The other BASELINE configurations, each timed beside the reference on the host cores:
     C1 dish (FP64, 1e6 hits, 50 x 50 absorber map), C2 trough (FP64 and mixed, 1e7 hits,
     72 x 120 absorber-tube map), C4 batched annual beam-down trace (512 sun positions, tracking
-    field of 10,000 heliostats, 64 x 64 ground map, one st_b200_sim_run_batch call), and the
+    field of 10,000 heliostats, 64 x 64 ground map, one st_b200_sim_run_batch call), the
     headline field with records on (1e7 hits, st_locations & co. read back: what pysoltrace
-    pays)."""
+    pays), and the C5 flux surrogate."""
     out = {}
 
     def timed_runs(sc, maps, prec, seed, steps, records=False):
@@ -313,7 +313,51 @@ def config_lines(api, args) -> dict:
             except Exception as ex:  # noqa: BLE001
                 line["reference"] = {"unavailable": str(ex)}
     out["C1_dish"], out["C2_trough"], out["C4_batch"] = c1, c2, c4
+    out["C5_surrogate"] = surrogate_line(api)
     return out
+
+
+def surrogate_line(api) -> dict:
+    """C5: the BF16 flux surrogate (6 layers, width 256, 32 x 32 receiver image per heliostat)
+    trained on the device from 150 traces of the headline field (2e7 hits each), judged on 16
+    held-out situations traced at 1e7 hits, and timed predicting the field maps of 64 sun
+    positions x 2,000 heliostats in one fused pass against the plain trace of one position at
+    1e7 hits."""
+    import torch
+
+    from soltrace_b200 import surrogate as S
+    tracer = S.FieldTracer(api)
+    try:
+        net, scale, t_data, t_train = S.fit(tracer, 150, 20_000_000, 2500)
+        peaks, l1 = S.judge(net, tracer, scale, 16, 10_000_000)
+        untrained = S.Mlp(api, seed=77)
+        peaks0, l10 = S.judge(untrained, tracer, scale, 4, 10_000_000)
+        ms = S.time_fields(net, tracer, scale, n_suns=64)
+        rng = np.random.default_rng(5)
+        trace_ms = []
+        for i in range(4):
+            tracer.trace(*S.random_situation(rng, tracer.n), 10_000_000, 900 + i)
+            trace_ms.append(api.stats(tracer.ctx)["kernel_ms"])
+        assert net.error() == 0
+    finally:
+        tracer.close()
+    peaks_file = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    bf16 = None
+    if os.path.exists(peaks_file):
+        bf16 = json.load(open(peaks_file)).get("bf16_tflops")
+    flops = S.fused_flops(S.DIMS, 64 * 2000)
+    tflops = flops / (ms / 1e3) / 1e12
+    per_trace = float(np.median(trace_ms))
+    return {"workload": "C5 BF16 MLP flux surrogate (8 -> 5 x 256 -> 1024), field maps of 64 suns x 2,000 "
+                        "heliostats in one fused tcgen05 pass vs the trace of one sun at 1e7 hits",
+            "speedup": 64 * per_trace / ms, "surrogate_ms_64_suns": ms, "trace_ms_per_sun_1e7": per_trace,
+            "peak_error_max": max(peaks), "peak_error_mean": float(np.mean(peaks)),
+            "map_l1_error_mean": float(np.mean(l1)), "untrained_peak_error_mean": float(np.mean(peaks0)),
+            "untrained_map_l1_error_mean": float(np.mean(l10)), "train_traces": 150, "train_steps": 2500,
+            "trace_data_s": t_data, "train_s": t_train, "dtype": "bf16 (fp32 accumulate)",
+            "roofline": {"bound": "tensor", "kernel": "k_mlp_fused", "achieved": tflops,
+                         "peak": bf16, "unit": "TFLOP/s", "frac": tflops / bf16 if bf16 else None,
+                         "peak_source": "of measured (bf16 burst)" if bf16 else "unavailable"}}
 
 
 def run_reference_arm(args):
@@ -338,21 +382,6 @@ def run_reference_arm(args):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload(args),
             "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
-
-
-# ---------------------------------------------------------------------------------------
-def traffic_per_unit() -> dict:
-    """{group: DRAM bytes per unit} from the table in profiles/traffic.md."""
-    out = {}
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.md")) as f:
-            for line in f:
-                cells = [c.strip() for c in line.strip().strip("|").split("|")]
-                if len(cells) >= 3 and cells[0] in ("probe group", "trace group"):
-                    out[cells[0]] = float(cells[1])
-    except (OSError, ValueError):
-        pass
-    return out
 
 
 # B200 arm
@@ -462,14 +491,12 @@ def main():
     probe_tflops = pf / (probe_ms / 1e3) / 1e12
     trace_tflops = tf / (trace_ms / 1e3) / 1e12
     dominant = "k_probe" if probe_ms >= trace_ms else "k_trace"
-    # DRAM bytes per unit of each launch group, from the ncu captures summarised in
-    # profiles/traffic.md, scaled to this step's units
-    traffic = None
-    per_unit = traffic_per_unit()
-    if dominant == "k_probe" and "probe group" in per_unit:
-        traffic = per_unit["probe group"] * sun_rays / len(runs)
-    elif dominant == "k_trace" and "trace group" in per_unit:
-        traffic = per_unit["trace group"] * hits / len(runs)
+    # DRAM bytes per unit of each launch group (ncu captures at 2e6 hits), scaled to this
+    # step's units
+    if dominant == "k_probe":
+        traffic = fm.DRAM_BYTES_PER_SUN_RAY_PROBE * sun_rays / len(runs)
+    else:
+        traffic = fm.DRAM_BYTES_PER_HIT_TRACE * hits / len(runs)
     if dominant == "k_probe":
         ach, pk = probe_tflops, fm.NOMINAL_FP64_TFLOPS
         hbm_ach = fm.probe_bytes(sun_rays, hits) / (probe_ms / 1e3) / 1e9

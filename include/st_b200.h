@@ -49,7 +49,12 @@ int st_b200_explicit_rays(st_context_t pcxt, st_uint_t n, const double *pos, con
  *   kind 2: flat, the GUI's rule (app/src/project.cpp:1392-1403): bins (lower, upper]
  *           over [x0,x1] by [y0,y1];
  *   kind 3: full cylinder of radius x1, the GUI's unwrapped arc length over
- *           [-pi x1, pi x1] (project.cpp:1370-1378) by y, bins (lower, upper].
+ *           [-pi x1, pi x1] (project.cpp:1370-1378) by y, bins (lower, upper];
+ *   kind 4: tube of radius x1, the nearest node of the polar mesh of the trough example
+ *           (app/deploy/api/examples/parabolic-trough-tracking-timeseries/
+ *           st_processing_functions.py:174-250): arc r atan2(x, z - x1) against nx cell
+ *           centres over the circumference 2 pi x1, y - (y0 + y1)/2 against ny centres over
+ *           y1 - y0; every intersection lands in a bin (x0 unused).
  * absorbed_only selects absorbed intersections.  Returns the map index. */
 int st_b200_add_flux_map(st_context_t pcxt, int stage, int element, int kind, int nx, int ny, double x0, double x1,
                          double y0, double y1, int absorbed_only);
@@ -223,6 +228,26 @@ int st_b200_mlp_adam(long long n, float *w, const float *g, float *m, float *v, 
                      float beta2, float eps, int step, void *stream);
 int st_b200_mlp_to_bf16(long long n, const float *x, void *y, void *stream);
 int st_b200_mlp_error(void);
+
+/* Fused inference: the whole network in one persistent kernel (one CTA per SM), activations
+ * kept in shared memory between layers, weights streamed from a packed copy.  Shapes: 2 to 8
+ * layers, dims[0] (inputs) 1 to 16, every hidden width 256, the output width dims[n_layers] a
+ * multiple of 256 up to 4096.
+ *
+ * st_b200_mlp_packed_bytes: size of the packed weights for those dims, -1 if unsupported.
+ * st_b200_mlp_pack: lays the bf16 weights w[l] (dims[l+1] x dims[l], row-major) out in
+ *   `packed` in the order and shared-memory layout the fused kernel streams them.
+ * st_b200_mlp_forward_fused: y = the network applied to the m rows of x (bf16, leading
+ *   dimension ldx), bias[l] float; each output value becomes v = y scale (clamped to >= 0
+ *   when clamp is set) and
+ *     mode 0: out[r dims[n_layers] + j] = v                       (every row's output)
+ *     mode 1: out[(r / group_rows) dims[n_layers] + j] += v       (sum over groups of rows,
+ *             e.g. every heliostat of a field: the field's receiver map; out pre-zeroed) */
+long long st_b200_mlp_packed_bytes(int n_layers, const int *dims);
+int st_b200_mlp_pack(int n_layers, const int *dims, const void *const *w, void *packed, void *stream);
+int st_b200_mlp_forward_fused(int n_layers, const int *dims, const void *packed, const float *const *bias, int m,
+                              const void *x, long long ldx, float *out, int mode, int group_rows, float scale,
+                              int clamp, void *stream);
 
 /* First-stage probe without device allocation.  No counterpart in the reference.
  *

@@ -2811,12 +2811,85 @@ static double oracle_gui_arc(double x, double z, double R) {
     return (x < 0) ? -(kPi * R / 2.0 + R * acos(fabs(x) / R)) : kPi * R / 2.0 + R * acos(x / R);
 }
 
+// Kind 4, the trough example's nearest-node binning
+// (app/deploy/api/examples/parabolic-trough-tracking-timeseries/st_processing_functions.py):
+// create_polar_mesh_cyl (174-204) builds cell-centre nodes with numpy.arange -- for even n
+// arange(d/2, S/2, d), for odd n arange(0, S/2, d), mirrored and sorted -- and
+// compute_fluxmap (236-250) takes numpy.argmin(|nodes - v|), the first of equals.  The node
+// list is built as numpy fills an arange (start, start + step, then start + k (v1 - start))
+// and scanned whole.
+static std::vector<double> oracle_mesh_nodes(int n, double span) {
+    const double d = span / n;
+    const double start = (n % 2 == 0) ? 0.0 + d / 2 : 0.0;
+    const long len = (long)ceil((span / 2.0 - start) / d);
+    std::vector<double> pos(size_t(len > 0 ? len : 0));
+    for (long k = 0; k < len; ++k) pos[k] = k == 0 ? start : k == 1 ? start + d : start + double(k) * ((start + d) - start);
+    std::vector<double> nodes;
+    for (long k = len - 1; k >= (n % 2 == 0 ? 0 : 1); --k) nodes.push_back(-pos[k]);
+    for (long k = 0; k < len; ++k) nodes.push_back(pos[k]);
+    return nodes;
+}
+static int oracle_argmin_abs(const std::vector<double> &nodes, double v) {
+    int best = -1;
+    double bd = 0;
+    for (size_t i = 0; i < nodes.size(); ++i) {
+        const double dd = fabs(nodes[i] - v);
+        if (dd != dd) return int(i);  // numpy.argmin returns the first NaN
+        if (best < 0 || dd < bd) {
+            best = int(i);
+            bd = dd;
+        }
+    }
+    return best;
+}
+
+// Bin (ix, iy) of an element-local point for a map kind; 1 when it lands in the map, 0 not.
+int st_oracle_bin_point(int kind, int nx, int ny, double x0, double x1, double y0, double y1, double x, double y,
+                        double z, int *ix_out, int *iy_out) {
+    long ix = -1, iy = -1;
+    if (kind == 4) {
+        if (x != x || y != y || z != z) return 0;
+        const double r = x1;
+        ix = oracle_argmin_abs(oracle_mesh_nodes(nx, kPi * (2.0 * r)), r * atan2(x, z - r));
+        iy = oracle_argmin_abs(oracle_mesh_nodes(ny, y1 - y0), y - 0.5 * (y0 + y1));
+    } else if (kind >= 2) {
+        ix = kind == 2 ? oracle_gui_bin(x, x0, (x1 - x0) / nx, nx)
+                       : oracle_gui_bin(oracle_gui_arc(x, z, x1), -kPi * x1, 2.0 * kPi * x1 / nx, nx);
+        iy = oracle_gui_bin(y, y0, (y1 - y0) / ny, ny);
+    } else {
+        double u, u0, u1;
+        if (kind == 0) {
+            u = x;
+            u0 = x0;
+            u1 = x1;
+        } else {
+            u = atan2(x, z - x1) + kPi;
+            u0 = 0.0;
+            u1 = 2.0 * kPi;
+        }
+        const double fx = floor((u - u0) / (u1 - u0) * nx), fy = floor((y - y0) / (y1 - y0) * ny);
+        if (!(fx >= 0 && fx < nx && fy >= 0 && fy < ny)) return 0;
+        ix = long(fx);
+        iy = long(fy);
+    }
+    if (ix < 0 || ix >= nx || iy < 0 || iy >= ny) return 0;
+    *ix_out = int(ix);
+    *iy_out = int(iy);
+    return 1;
+}
+
 int st_oracle_flux(void *p, int stage, int element, int kind, int nx, int ny, double x0, double x1, double y0,
                    double y1, int absorbed_only, unsigned long long *bins) {
     CTX(p, -1);
     for (const Record &r : cx->all) {
         if (r.stage != stage) continue;
         if (absorbed_only ? r.element != -element : (r.element != element && r.element != -element)) continue;
+        if (kind == 4) {
+            int ix, iy;
+            if (st_oracle_bin_point(kind, nx, ny, x0, x1, y0, y1, r.loc[0], r.loc[1], r.loc[2], &ix, &iy))
+                bins[size_t(iy) * nx + ix]++;
+            continue;
+        }
         if (kind >= 2) {
             const int ix = kind == 2 ? oracle_gui_bin(r.loc[0], x0, (x1 - x0) / nx, nx)
                                      : oracle_gui_bin(oracle_gui_arc(r.loc[0], r.loc[2], x1), -kPi * x1,

@@ -2404,7 +2404,7 @@ int st_b200_explicit_rays(st_context_t p, st_uint_t n, const double *pos, const 
 static int add_flux_map(Context *cx, int stage, int element, int kind, int nx, int ny, double x0, double x1,
                         double y0, double y1, int absorbed_only, int per_source) {
     if (cx->flux.size() >= size_t(kMaxFluxMaps) || nx <= 0 || ny <= 0 || stage < 1 || element < 1 || kind < 0 ||
-        kind > 3 || !(x1 > x0 || kind == 1 || kind == 3) || !(y1 > y0) || ((kind == 1 || kind == 3) && !(x1 > 0))) {
+        kind > 4 || !(x1 > x0 || kind == 1 || kind >= 3) || !(y1 > y0) || (kind != 0 && kind != 2 && !(x1 > 0))) {
         cx->log("invalid flux map request");
         return -1;
     }
@@ -2457,7 +2457,7 @@ int st_b200_flux_stats(st_context_t p, int map, double dni, st_b200_flux_stats_t
         return -1;
     }
     const double two_pi = 2.0 * 3.14159265358979323846;
-    const double bx = (q.kind == 1 || q.kind == 3) ? two_pi * q.x1 / q.nx : (q.x1 - q.x0) / q.nx;
+    const double bx = (q.kind == 1 || q.kind >= 3) ? two_pi * q.x1 / q.nx : (q.x1 - q.x0) / q.nx;
     const double by = (q.y1 - q.y0) / q.ny;
     st_b200_flux_stats_t r;
     memset(&r, 0, sizeof r);

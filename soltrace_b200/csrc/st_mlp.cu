@@ -304,6 +304,365 @@ __global__ void k_to_bf16(long long n, const float *x, __nv_bfloat16 *y) {
         y[i] = __float2bfloat16_rn(x[i]);
 }
 
+// ---------------------------------------------------------------------------------------
+// Fused inference: every layer in one persistent kernel
+// ---------------------------------------------------------------------------------------
+// A CTA (one per SM) walks 128-row tiles.  The tile's activations X (128 x 256 bf16, the
+// K-major core-matrix layout the tensor cores read) stay in shared memory from layer to
+// layer; the weights stream through a ring of shared-memory stages, each one bulk copy
+// (cp.async.bulk, completion counted on the stage's mbarrier) of a block that the packing
+// kernel already laid out in that layout.  Roles:
+//   warps 0-3 (epilogue): load the tile's inputs into X; per layer read the accumulator back
+//     (warp w owns tensor-memory lanes 32w..32w+31, thread = row), add the bias, ReLU, round
+//     to bf16 and write X for the next layer; on the output layer apply scale/clamp and write
+//     the rows or add them into their group's sums;
+//   warp 4, one thread (loader): issues the weight stages, kRing ahead of their use, across
+//     layers and tiles (the next layer's weights arrive while the epilogue runs);
+//   warp 5, one thread (MMA issuer): per layer waits for X, per stage for its weights, issues
+//     the tcgen05.mma (128 x 256 x 16 each) and commits the stage back to the loader; the
+//     accumulator's commit wakes the epilogue.
+// Two accumulators (2 x 256 tensor-memory columns) alternate between units (a layer, or a
+// 256-wide chunk of the output layer), so an output chunk's epilogue overlaps the next
+// chunk's products.  Every wait is bounded; one that runs out sets the error flag and a shared
+// abort flag that ends every role's loop, and the CTA drains its own copies and products
+// before freeing tensor memory.
+constexpr int kWidth = 256;                       // hidden width: the MMA N and the next layer's K
+constexpr int kRing = 4;                          // weight stages in flight
+constexpr int kStageBytes = kWidth * kBK * 2;     // 32 KB: a 256 x 64 weight block
+constexpr int kFirstBytes = kWidth * 16 * 2;      // 8 KB: the first layer's 256 x 16 block
+constexpr int kXBytes = kBM * kWidth * 2;         // 64 KB: a 128-row activation tile
+constexpr int kFusedThreads = 192;
+constexpr int kMaxLayers = 8;
+constexpr int kMaxOut = 4096;
+
+struct FusedArgs {
+    const __nv_bfloat16 *x;
+    long long ldx;
+    int M, d_in, n_layers, n_out;
+    const unsigned char *packed;
+    const float *bias[kMaxLayers];
+    float *out;
+    int mode, group_rows, clamp;
+    float scale;
+    unsigned *err;
+};
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// one bulk copy global -> this CTA's shared memory, its bytes counted on `bar`
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// bounded wait that also gives up as soon as another role raised the abort flag
+__device__ __forceinline__ bool mbar_wait_or_abort(uint64_t *bar, unsigned parity, volatile int *abort) {
+    const uint32_t a = smem_u32(bar);
+    for (unsigned it = 0; it < kSpinLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (*abort) return false;
+    }
+    return false;
+}
+
+// weight stages of one tile: the first layer's block, 4 per hidden layer, 4 per output chunk
+__host__ __device__ inline int stages_per_tile(int n_layers, int n_out) {
+    return 1 + 4 * (n_layers - 2) + 4 * (n_out / kWidth);
+}
+__device__ __forceinline__ uint32_t stage_bytes(int j) { return j == 0 ? kFirstBytes : kStageBytes; }
+__device__ __forceinline__ size_t stage_offset(int j) {
+    return j == 0 ? 0 : size_t(kFirstBytes) + size_t(j - 1) * kStageBytes;
+}
+
+__global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(FusedArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *X = smem;
+    unsigned char *ring = smem + kXBytes;
+    __shared__ __align__(8) uint64_t full[kRing], empty[kRing], acc_full[2], acc_free[2], x_ready, drain;
+    __shared__ uint32_t tmem_sh;
+    __shared__ volatile int abort_flag;
+    __shared__ unsigned issued_sh, consumed_sh;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n_tiles = (g.M + kBM - 1) / kBM;
+    const int L = g.n_layers, NC = g.n_out / kWidth;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kRing; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&acc_full[i], 1);
+            mbar_init(&acc_free[i], 128);
+        }
+        mbar_init(&x_ready, 128);
+        mbar_init(&drain, 1);
+        abort_flag = 0;
+        issued_sh = consumed_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {  // two 128 x 256 FP32 accumulators
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_sh)),
+                     "r"(uint32_t(2 * kWidth)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_sh;
+    const int S = stages_per_tile(L, g.n_out);
+
+    if (warp == 4) {
+        // ---- loader ----
+        if (lane == 0) {
+            unsigned q = 0;
+            for (int t = blockIdx.x; t < n_tiles && !abort_flag; t += gridDim.x) {
+                for (int j = 0; j < S; ++j, ++q) {
+                    const int slot = q % kRing;
+                    if (q >= kRing && !mbar_wait_or_abort(&empty[slot], ((q / kRing) - 1) & 1u, &abort_flag)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    mbar_expect_tx(&full[slot], stage_bytes(j));
+                    bulk_load(ring + slot * kStageBytes, g.packed + stage_offset(j), stage_bytes(j), &full[slot]);
+                }
+            }
+            issued_sh = q;
+        }
+    } else if (warp == 5) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            constexpr uint32_t idesc = instr_desc(kWidth);
+            unsigned q = 0, u = 0, xr = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+                for (int l = 0; l < L && ok; ++l) {
+                    if (!mbar_wait_or_abort(&x_ready, xr & 1u, &abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    ++xr;
+                    const int chunks = (l == L - 1) ? NC : 1;
+                    const int nst = (l == 0) ? 1 : kWidth / kBK;
+                    for (int c = 0; c < chunks && ok; ++c, ++u) {
+                        const int b = u & 1;
+                        if (u >= 2 && !mbar_wait_or_abort(&acc_free[b], ((u >> 1) - 1) & 1u, &abort_flag)) {
+                            ok = false;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        for (int s = 0; s < nst; ++s, ++q) {
+                            const int slot = q % kRing;
+                            if (!mbar_wait_or_abort(&full[slot], (q / kRing) & 1u, &abort_flag)) {
+                                ok = false;
+                                break;
+                            }
+                            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                            const uint32_t wb = smem_u32(ring + slot * kStageBytes);
+                            const int steps = (l == 0) ? 1 : kBK / 16;
+                            for (int j = 0; j < steps; ++j) {
+                                // X: K chunk kc at kc * 2048 (16 row groups of 128 B); weight block: K
+                                // chunk at kc * 4096 (32 row groups); a K = 16 step spans two chunks
+                                const int kstep = s * (kBK / 16) + j;
+                                const uint64_t ad = smem_desc(smem_u32(X) + uint32_t(kstep * 2 * 2048), 2048, 128);
+                                const uint64_t bd = smem_desc(wb + uint32_t(j * 2 * 4096), 4096, 128);
+                                mma_bf16(tmem + uint32_t(b * kWidth), ad, bd, idesc, (s > 0 || j > 0) ? 1u : 0u);
+                            }
+                            mma_commit(&empty[slot]);
+                        }
+                        if (ok) mma_commit(&acc_full[b]);
+                    }
+                }
+            }
+            if (!ok) abort_flag = 1;
+            consumed_sh = q;
+            // every product this thread issued has finished before the CTA frees its memory
+            mma_commit(&drain);
+            mbar_wait(&drain, 0);
+        }
+    } else {
+        // ---- epilogue: warps 0-3, thread = row of the tile ----
+        const int r = threadIdx.x;
+        unsigned u = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < n_tiles && ok; t += gridDim.x) {
+            const int row = t * kBM + r;
+            // inputs, zero-padded to K = 16 (two core-matrix columns)
+            {
+                unsigned short h[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e)
+                    h[e] = (row < g.M && e < g.d_in) ? __bfloat16_as_ushort(g.x[row * g.ldx + e]) : (unsigned short)0;
+#pragma unroll
+                for (int kc = 0; kc < 2; ++kc) {
+                    const uint4 v = make_uint4(h[8 * kc] | (uint32_t(h[8 * kc + 1]) << 16),
+                                               h[8 * kc + 2] | (uint32_t(h[8 * kc + 3]) << 16),
+                                               h[8 * kc + 4] | (uint32_t(h[8 * kc + 5]) << 16),
+                                               h[8 * kc + 6] | (uint32_t(h[8 * kc + 7]) << 16));
+                    *reinterpret_cast<uint4 *>(X + (kc * 16 + r / 8) * 128 + (r % 8) * 16) = v;
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(&x_ready);
+            for (int l = 0; l < L && ok; ++l) {
+                const int chunks = (l == L - 1) ? NC : 1;
+                const float *bias = g.bias[l];
+                for (int c = 0; c < chunks; ++c, ++u) {
+                    const int b = u & 1;
+                    // warp-uniform: the tensor-memory loads below are warp-collective
+                    if (!__all_sync(0xffffffffu, mbar_wait_or_abort(&acc_full[b], (u >> 1) & 1u, &abort_flag))) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t ta = tmem + (uint32_t(warp * 32) << 16) + uint32_t(b * kWidth);
+                    if (l < L - 1) {
+                        for (int c0 = 0; c0 < kWidth; c0 += 16) {
+                            float v[16];
+                            tmem_ld16(ta + uint32_t(c0), v);
+                            uint32_t p[8];
+#pragma unroll
+                            for (int i = 0; i < 8; ++i) {
+                                const float a0 = fmaxf(v[2 * i] + __ldg(bias + c0 + 2 * i), 0.f);
+                                const float a1 = fmaxf(v[2 * i + 1] + __ldg(bias + c0 + 2 * i + 1), 0.f);
+                                p[i] = uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(a0))) |
+                                       (uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(a1))) << 16);
+                            }
+                            const int kc = c0 / 8;
+                            *reinterpret_cast<uint4 *>(X + (kc * 16 + r / 8) * 128 + (r % 8) * 16) =
+                                make_uint4(p[0], p[1], p[2], p[3]);
+                            *reinterpret_cast<uint4 *>(X + ((kc + 1) * 16 + r / 8) * 128 + (r % 8) * 16) =
+                                make_uint4(p[4], p[5], p[6], p[7]);
+                        }
+                        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                        mbar_arrive(&acc_free[b]);
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        mbar_arrive(&x_ready);
+                    } else {
+                        const int n0 = c * kWidth;
+                        const bool valid = row < g.M;
+                        const long long grp = (long long)(valid ? row : g.M - 1) / (g.mode == 1 ? g.group_rows : 1);
+                        const long long grp0 = __shfl_sync(0xffffffffu, grp, 0);
+                        const bool uniform = __all_sync(0xffffffffu, grp0 == grp) && g.mode == 1;
+                        for (int c0 = 0; c0 < kWidth; c0 += 16) {
+                            float v[16];
+                            tmem_ld16(ta + uint32_t(c0), v);
+#pragma unroll
+                            for (int i = 0; i < 16; ++i) {
+                                float y = (v[i] + __ldg(bias + n0 + c0 + i)) * g.scale;
+                                if (g.clamp) y = fmaxf(y, 0.f);
+                                v[i] = valid ? y : 0.f;
+                            }
+                            const int col = n0 + c0;
+                            if (g.mode == 0) {
+                                if (valid) {
+                                    float4 *o = reinterpret_cast<float4 *>(g.out + (long long)row * g.n_out + col);
+#pragma unroll
+                                    for (int i = 0; i < 4; ++i)
+                                        o[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                                }
+                            } else if (uniform) {
+                                // the warp's 32 rows share a group: halve the 16 columns' sums across
+                                // lanes (16 shuffles), then one atomic per column
+#pragma unroll
+                                for (int d = 16, w = 8; d >= 2; d >>= 1, w >>= 1) {
+#pragma unroll
+                                    for (int i = 0; i < w; ++i) {
+                                        const bool hi = (lane & d) != 0;
+                                        const float send = hi ? v[i] : v[i + w];
+                                        const float keep = hi ? v[i + w] : v[i];
+                                        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, d);
+                                    }
+                                }
+                                v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+                                const int k = ((lane & 16) ? 8 : 0) + ((lane & 8) ? 4 : 0) + ((lane & 4) ? 2 : 0) +
+                                              ((lane & 2) ? 1 : 0);
+                                if ((lane & 1) == 0) atomicAdd(g.out + grp * g.n_out + col + k, v[0]);
+                            } else if (valid) {
+#pragma unroll
+                                for (int i = 0; i < 16; ++i) atomicAdd(g.out + grp * g.n_out + col + i, v[i]);
+                            }
+                        }
+                        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                        mbar_arrive(&acc_free[b]);
+                    }
+                }
+            }
+        }
+        if (!ok) abort_flag = 1;
+    }
+    __syncthreads();
+    if (abort_flag) {
+        if (threadIdx.x == 0) {
+            atomicExch(g.err, 1u);
+            // weight copies issued but never consumed land before their shared memory goes away
+            for (unsigned q = consumed_sh; q < issued_sh; ++q) mbar_wait(&full[q % kRing], (q / kRing) & 1u);
+        }
+        __syncthreads();
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(uint32_t(2 * kWidth)));
+}
+
+// packed weights, in bf16 elements: the first layer's 256 x 16 block, then per hidden layer
+// and per output chunk four 256 x 64 blocks (K slices 0-63, ..., 192-255), each block K-major
+// core matrices: element (n, k) at byte ((k / 8) 32 + n / 8) 128 + (n % 8) 16 + (k % 8) 2
+struct PackArgs {
+    const __nv_bfloat16 *w[kMaxLayers];
+    int dims[kMaxLayers + 1];
+    int n_layers;
+    long long n_elems;
+    __nv_bfloat16 *out;
+};
+
+__global__ void k_mlp_pack(PackArgs a) {
+    constexpr long long kFirst = kFirstBytes / 2, kBlock = kStageBytes / 2;
+    const int L = a.n_layers;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < a.n_elems;
+         e += (long long)gridDim.x * blockDim.x) {
+        int l, n, k;
+        long long off;
+        if (e < kFirst) {
+            l = 0;
+            off = e * 2;
+            n = int((off % 4096) / 128) * 8 + int((off % 128) / 16);
+            k = int(off / 4096) * 8 + int((off % 16) / 2);
+        } else {
+            const long long blk = (e - kFirst) / kBlock;
+            off = ((e - kFirst) % kBlock) * 2;
+            int chunk = 0, slice;
+            if (blk < 4LL * (L - 2)) {
+                l = 1 + int(blk / 4);
+                slice = int(blk % 4);
+            } else {
+                l = L - 1;
+                chunk = int((blk - 4LL * (L - 2)) / 4);
+                slice = int((blk - 4LL * (L - 2)) % 4);
+            }
+            n = chunk * kWidth + int((off % 4096) / 128) * 8 + int((off % 128) / 16);
+            k = slice * kBK + int(off / 4096) * 8 + int((off % 16) / 2);
+        }
+        const int din = a.dims[l], dout = a.dims[l + 1];
+        a.out[e] = (n < dout && k < din) ? a.w[l][(long long)n * din + k] : __float2bfloat16_rn(0.f);
+    }
+}
+
 __device__ unsigned g_mlp_err = 0;
 
 unsigned *err_flag() {
@@ -330,6 +689,34 @@ int launch_gemm(const GemmArgs &a, int splits, cudaStream_t st) {
     }
     const dim3 grid((a.M + kBM - 1) / kBM, (a.N + BN - 1) / BN, splits);
     k_mlp_gemm<BN><<<grid, kThreads, smem, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+}
+
+// the fused kernel's shape rules; -1 or the packed size in bf16 elements
+long long packed_elems(int n_layers, const int *dims) {
+    if (!dims || n_layers < 2 || n_layers > kMaxLayers) return -1;
+    if (dims[0] < 1 || dims[0] > 16) return -1;
+    for (int l = 1; l < n_layers; ++l)
+        if (dims[l] != kWidth) return -1;
+    const int n_out = dims[n_layers];
+    if (n_out < kWidth || n_out > kMaxOut || n_out % kWidth) return -1;
+    return kFirstBytes / 2 + (long long)(stages_per_tile(n_layers, n_out) - 1) * (kStageBytes / 2);
+}
+
+int launch_fused(const FusedArgs &a, cudaStream_t st) {
+    constexpr int smem = kXBytes + kRing * kStageBytes;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return -1;
+    static int sms[64] = {0};
+    if (!sms[dev]) {
+        if (cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+            return -1;
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) return -1;
+        sms[dev] = n;
+    }
+    const int tiles = (a.M + kBM - 1) / kBM;
+    k_mlp_fused<<<tiles < sms[dev] ? tiles : sms[dev], kFusedThreads, smem, st>>>(a);
     return cudaGetLastError() == cudaSuccess ? 1 : -1;
 }
 
@@ -401,6 +788,55 @@ int st_b200_mlp_to_bf16(long long n, const float *x, void *y, void *stream) {
     if (n <= 0 || !x || !y) return -1;
     k_to_bf16<<<592, 256, 0, static_cast<cudaStream_t>(stream)>>>(n, x, static_cast<__nv_bfloat16 *>(y));
     return cudaGetLastError() == cudaSuccess ? 1 : -1;
+}
+
+long long st_b200_mlp_packed_bytes(int n_layers, const int *dims) {
+    const long long e = packed_elems(n_layers, dims);
+    return e < 0 ? -1 : 2 * e;
+}
+
+int st_b200_mlp_pack(int n_layers, const int *dims, const void *const *w, void *packed, void *stream) {
+    const long long e = packed_elems(n_layers, dims);
+    if (e < 0 || !w || !packed) return -1;
+    PackArgs a;
+    for (int l = 0; l < n_layers; ++l) {
+        if (!w[l]) return -1;
+        a.w[l] = static_cast<const __nv_bfloat16 *>(w[l]);
+    }
+    for (int l = 0; l <= n_layers; ++l) a.dims[l] = dims[l];
+    a.n_layers = n_layers;
+    a.n_elems = e;
+    a.out = static_cast<__nv_bfloat16 *>(packed);
+    k_mlp_pack<<<592, 256, 0, static_cast<cudaStream_t>(stream)>>>(a);
+    return cudaGetLastError() == cudaSuccess ? 1 : -1;
+}
+
+int st_b200_mlp_forward_fused(int n_layers, const int *dims, const void *packed, const float *const *bias, int m,
+                              const void *x, long long ldx, float *out, int mode, int group_rows, float scale,
+                              int clamp, void *stream) {
+    if (packed_elems(n_layers, dims) < 0 || !packed || !bias || m <= 0 || !x || ldx < dims[0] || !out) return -1;
+    if (mode < 0 || mode > 1 || (mode == 1 && group_rows < 1)) return -1;
+    if ((reinterpret_cast<uintptr_t>(packed) & 15) || (reinterpret_cast<uintptr_t>(out) & 15)) return -1;
+    FusedArgs a;
+    for (int l = 0; l < n_layers; ++l) {
+        if (!bias[l]) return -1;
+        a.bias[l] = bias[l];
+    }
+    a.x = static_cast<const __nv_bfloat16 *>(x);
+    a.ldx = ldx;
+    a.M = m;
+    a.d_in = dims[0];
+    a.n_layers = n_layers;
+    a.n_out = dims[n_layers];
+    a.packed = static_cast<const unsigned char *>(packed);
+    a.out = out;
+    a.mode = mode;
+    a.group_rows = mode == 1 ? group_rows : 1;
+    a.clamp = clamp ? 1 : 0;
+    a.scale = scale;
+    a.err = err_flag();
+    if (!a.err) return -1;
+    return launch_fused(a, static_cast<cudaStream_t>(stream));
 }
 
 // the GEMM error flag of the current device (1: a wait ran out), cleared by the read

@@ -482,6 +482,48 @@ __host__ __device__ inline double gui_cyl_arc(double x, double z, double R) {
     return (x < 0) ? -(kPiD * R / 2.0 + R * acos(fabs(x) / R)) : kPiD * R / 2.0 + R * acos(x / R);
 }
 
+// Value k of numpy.arange(start, stop, step) as numpy fills it: start, start + step, then
+// start + k ((start + step) - start).
+__host__ __device__ inline double arange_value(double start, double step, int k) {
+    if (k == 0) return start;
+    const double v1 = start + step;
+    return k == 1 ? v1 : start + double(k) * (v1 - start);
+}
+
+// Node i (ascending) of the cell-centre mesh of n cells over a span S centred on 0, built as
+// the trough example's create_polar_mesh_cyl builds it
+// (app/deploy/api/examples/parabolic-trough-tracking-timeseries/st_processing_functions.py:
+// 174-204): even n: +-(d/2 + k d), odd n: 0, +-k d, with d = S / n.
+__host__ __device__ inline double mesh_node(int i, int n, double S) {
+    const double d = S / n;
+    if (n % 2 == 0) {
+        const int m = n / 2;
+        return i < m ? -arange_value(0.0 + d / 2, d, m - 1 - i) : arange_value(0.0 + d / 2, d, i - m);
+    }
+    const int m = (n + 1) / 2;
+    return i < m - 1 ? -arange_value(0.0, d, m - 1 - i) : arange_value(0.0, d, i - (m - 1));
+}
+
+// The node nearest to v, the first of equals (numpy.argmin of |node - v|, the example's
+// compute_fluxmap, st_processing_functions.py:245-250); every finite v has one.  The nodes are
+// d apart up to rounding, so the nearest is within one of the estimate: the five around it
+// are compared in order.  -1 for NaN.
+__host__ __device__ inline int mesh_nearest(double v, int n, double S) {
+    if (!(v == v)) return -1;
+    const double est = v / (S / n) + 0.5 * (n - 1);
+    const int i0 = !(est > 0.0) ? 0 : (est >= double(n - 1) ? n - 1 : int(est + 0.5));
+    int best = -1;
+    double bd = 0.0;
+    for (int i = (i0 > 2 ? i0 - 2 : 0); i <= (i0 + 2 < n - 1 ? i0 + 2 : n - 1); ++i) {
+        const double dd = fabs(mesh_node(i, n, S) - v);
+        if (best < 0 || dd < bd) {
+            best = i;
+            bd = dd;
+        }
+    }
+    return best;
+}
+
 // fe0: the ray's first first-stage element (global index, first stage first; -1 none), which
 // selects the map of a per-source flux map
 template <int MIXED>
@@ -493,13 +535,19 @@ __device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed
         if (f.n_src > 0 && (fe0 < 0 || fe0 >= f.n_src)) continue;
         int ix, iy;
         if (f.kind >= 2) {  // the GUI's statistics rules, in double
-            if (f.kind == 2) {
-                ix = gui_bin(pe[0], f.x0, (f.x1 - f.x0) / f.nx, f.nx);
-            } else {
+            if (f.kind == 4) {  // nearest node of the tube's polar mesh: arc r atan2(x, z - r) by y
                 const double R = f.x1;
-                ix = gui_bin(gui_cyl_arc(pe[0], pe[2], R), -kPiD * R, 2.0 * kPiD * R / f.nx, f.nx);
+                ix = mesh_nearest(R * atan2(pe[0], pe[2] - R), f.nx, kPiD * (2.0 * R));
+                iy = mesh_nearest(pe[1] - 0.5 * (f.y0 + f.y1), f.ny, f.y1 - f.y0);
+            } else {
+                if (f.kind == 2) {
+                    ix = gui_bin(pe[0], f.x0, (f.x1 - f.x0) / f.nx, f.nx);
+                } else {
+                    const double R = f.x1;
+                    ix = gui_bin(gui_cyl_arc(pe[0], pe[2], R), -kPiD * R, 2.0 * kPiD * R / f.nx, f.nx);
+                }
+                iy = gui_bin(pe[1], f.y0, (f.y1 - f.y0) / f.ny, f.ny);
             }
-            iy = gui_bin(pe[1], f.y0, (f.y1 - f.y0) / f.ny, f.ny);
         } else if (MIXED) {
             float u, u0, u1;
             if (f.kind == 0) {

@@ -41,6 +41,17 @@ NOMINAL_FP64_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
+# DRAM bytes (read + written) per unit, measured: ncu --set full captures of every main-batch
+# launch of the headline field at 2,000 heliostats and 2e6 hits (the command
+# `python bench.py --hits 2000000 --steps 1 --warmup 1 --no-cpu-baseline --no-extra`),
+# dram__bytes_read.sum + dram__bytes_write.sum summed over each launch group and divided by
+# the units the launches processed (15.32 M sun rays; 1.867 M first-stage hits).  The probe
+# figure is a lower bound at full size (its lists fit in L2 at 2e6 hits); the trace figure is
+# the wavefront's ray state, read and written at every kernel step.
+DRAM_BYTES_PER_SUN_RAY_PROBE = 4.17
+DRAM_BYTES_PER_HIT_TRACE = 368.0
+
+
 def probe_flops(sun_rays: int) -> float:
     return float(sun_rays) * PROBE_FLOPS_PER_SUN_RAY
 

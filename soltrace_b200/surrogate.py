@@ -38,6 +38,11 @@ MLP_SIGNATURES = {
                                    C.c_float, C.c_float, C.c_float, C.c_int, C.c_void_p]),
     "st_b200_mlp_to_bf16": (C.c_int, [C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p]),
     "st_b200_mlp_error": (C.c_int, []),
+    "st_b200_mlp_packed_bytes": (C.c_longlong, [C.c_int, C.c_void_p]),
+    "st_b200_mlp_pack": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "st_b200_mlp_forward_fused": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                            C.c_longlong, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int,
+                                            C.c_void_p]),
 }
 
 
@@ -67,6 +72,7 @@ class Mlp:
         self.vb = [torch.zeros_like(b) for b in self.b]
         self.step_count = 0
         self.acts = []
+        self._packed, self._packed_step = None, -1
 
     # ---- kernels ----
     def _s(self):
@@ -99,6 +105,40 @@ class Mlp:
             acts.append(out)
         self.acts = acts
         return acts[-1]
+
+    def packed(self):
+        """The bf16 weights laid out for the fused forward; rebuilt after training steps (the
+        layout is a copy: edit weights through train_step, or drop _packed after editing wb)."""
+        torch = self.torch
+        if self._packed is None or self._packed_step != self.step_count:
+            dims = (C.c_int * len(self.dims))(*self.dims)
+            nbytes = self.api.lib.st_b200_mlp_packed_bytes(len(self.w), dims)
+            if nbytes < 0:
+                raise ValueError(f"dims {self.dims} not supported by the fused forward")
+            blob = torch.empty(nbytes // 2, dtype=torch.bfloat16, device=self.device)
+            ptrs = (C.c_void_p * len(self.wb))(*[w.data_ptr() for w in self.wb])
+            self._check(self.api.lib.st_b200_mlp_pack(len(self.w), dims, ptrs, _ptr(blob), self._s()), "pack")
+            self._packed, self._packed_step = blob, self.step_count
+        return self._packed
+
+    def forward_fused(self, x, group_rows: int = 0, scale: float = 1.0, clamp: bool = False, out=None):
+        """Inference through the fused kernel (all layers in one launch).  x: (B, dims[0]) bf16.
+        group_rows 0: every row's output (B, dims[-1]); otherwise the sums over consecutive
+        groups of group_rows rows (ceil(B / group_rows), dims[-1]), added into `out` when given.
+        Outputs are scaled by `scale` and, with clamp, clipped to >= 0 before any sum."""
+        torch = self.torch
+        B, n_out = x.shape[0], self.dims[-1]
+        blob = self.packed()
+        dims = (C.c_int * len(self.dims))(*self.dims)
+        bias = (C.c_void_p * len(self.b))(*[b.data_ptr() for b in self.b])
+        if out is None:
+            rows = B if group_rows <= 0 else -(-B // group_rows)
+            out = torch.zeros(rows, n_out, dtype=torch.float32, device=self.device)
+        rc = self.api.lib.st_b200_mlp_forward_fused(len(self.w), dims, _ptr(blob), bias, B, _ptr(x), x.stride(0),
+                                                     _ptr(out), 0 if group_rows <= 0 else 1, max(group_rows, 1),
+                                                     float(scale), 1 if clamp else 0, self._s())
+        self._check(rc, "st_b200_mlp_forward_fused")
+        return out
 
     def backward(self, dy, want_input_grad: bool = False):
         """dy: (B, dims[-1]) bf16 gradient of the loss at the output.  Returns (dW list, db list,
@@ -273,6 +313,14 @@ def predict_images(net: Mlp, feats, target_scale: float):
     return torch.clamp(net.forward(x), min=0.0) * target_scale
 
 
+def predict_fields(net: Mlp, feats, n_helio: int, target_scale: float):
+    """Field receiver maps (n_situations, 1024) in kW per bin: the per-heliostat images
+    (clipped to >= 0) of every n_helio consecutive rows summed inside the fused kernel."""
+    import torch
+    x = torch.as_tensor(feats).cuda().to(torch.bfloat16)
+    return net.forward_fused(x, group_rows=n_helio, scale=target_scale, clamp=True)
+
+
 def peak_error(pred_map: np.ndarray, trace_map: np.ndarray) -> float:
     """|peak(pred) - peak(trace)| / peak(trace) of two field maps (kW per bin)."""
     return abs(float(pred_map.max()) - float(trace_map.max())) / max(float(trace_map.max()), 1e-30)
@@ -300,3 +348,69 @@ def optimise_aims(net: Mlp, feats: np.ndarray, target_scale: float, iters: int =
         g = g / g.abs().max().clamp(min=1e-30)
         x[:, 5:7] = (x[:, 5:7] - step * g).clamp(-1.0, 1.0)
     return x[:, 5:7].cpu().numpy().astype(np.float64)
+
+
+# ------------------------------------------------------------------------------------
+# Fitting and judging against the trace
+# ------------------------------------------------------------------------------------
+def fit(tracer: FieldTracer, n_traces: int, hits: int, steps: int, seed: int = 1, dims=DIMS, batch: int = 8192,
+        lr: float = 2e-3):
+    """A network trained on n_traces random situations traced at `hits` first-stage hits each:
+    (net, target_scale, seconds spent tracing, seconds spent training)."""
+    import time
+
+    import torch
+    t0 = time.perf_counter()
+    x, t = make_dataset(tracer, n_traces, hits, seed=seed)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    net = Mlp(tracer.api, dims=dims, seed=seed)
+    scale, _ = train(net, x, t, steps=steps, batch=batch, lr=lr)
+    torch.cuda.synchronize()
+    return net, scale, t1 - t0, time.perf_counter() - t1
+
+
+def judge(net: Mlp, tracer: FieldTracer, target_scale: float, n: int, hits: int, seed: int = 999):
+    """Field maps predicted for n held-out random situations (half of them with every aim
+    offset 0) against traces of the same situations at `hits` hits: per situation the
+    relative peak error |peak(pred) - peak(trace)| / peak(trace) and the relative L1 map
+    error sum |pred - trace| / sum trace."""
+    rng = np.random.default_rng(seed)
+    peaks, l1 = [], []
+    for i in range(n):
+        sun, off, sig = random_situation(rng, tracer.n)
+        if i % 2 == 0:
+            off[:] = 0.0
+        _, whole = tracer.trace(sun, off, sig, hits, 5000 + i)
+        pred = predict_fields(net, tracer.features(sun, off, sig), tracer.n, target_scale)[0]
+        pred = pred.reshape(IMG, IMG).double().cpu().numpy()
+        peaks.append(peak_error(pred, whole))
+        l1.append(float(np.abs(pred - whole).sum() / max(whole.sum(), 1e-30)))
+    return peaks, l1
+
+
+def fused_flops(dims, rows: int) -> float:
+    """Multiply-adds x 2 of one forward pass over `rows` inputs (the input layer at its true
+    width, not the 16 the kernel pads it to)."""
+    return 2.0 * rows * sum(a * b for a, b in zip(dims[:-1], dims[1:]))
+
+
+def time_fields(net: Mlp, tracer: FieldTracer, target_scale: float, n_suns: int = 64, reps: int = 20, seed: int = 3):
+    """Device milliseconds of one fused pass that predicts n_suns field maps of tracer.n
+    heliostats each (CUDA events on the launching stream, after 3 warm-up passes)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    feats = np.concatenate([tracer.features(*random_situation(rng, tracer.n)) for _ in range(n_suns)])
+    x = torch.as_tensor(feats).cuda().to(torch.bfloat16)
+    out = torch.zeros(n_suns, IMG * IMG, dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        net.forward_fused(x, group_rows=tracer.n, scale=target_scale, clamp=True, out=out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        out.zero_()
+        net.forward_fused(x, group_rows=tracer.n, scale=target_scale, clamp=True, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps

@@ -141,3 +141,14 @@ def test_geometry_errors_reported_before_any_device_work(product):
     assert product.run(ctx, 1) == -1
     assert "invalid optical property set name" in product.messages(ctx)[0]
     product.st_free_context(ctx)
+
+
+def test_fused_forward_rejects_unsupported_shapes(product):
+    """The fused forward's shape rules are checked on the host (no device needed)."""
+    fn = product.lib.st_b200_mlp_packed_bytes
+    fn.restype, fn.argtypes = C.c_longlong, [C.c_int, C.c_void_p]
+    for dims in [(8, 128, 256), (32, 256, 256), (8, 256, 300), (8, 256), (8,) + (256,) * 9]:
+        arr = (C.c_int * len(dims))(*dims)
+        assert fn(len(dims) - 1, arr) == -1, dims
+    arr = (C.c_int * 4)(8, 256, 256, 1024)
+    assert fn(3, arr) == 2 * (4096 + 16384 * (4 + 16))

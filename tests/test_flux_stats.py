@@ -95,6 +95,26 @@ def test_gui_bins_equal_oracle_and_stats_match(product, oracle, case):
         product.st_free_context(ctx)
 
 
+@pytest.mark.parametrize("mesh", [(72, 120), (5, 4), (1, 3)])
+def test_trough_mesh_bins_equal_oracle(product, oracle, mesh):
+    """Kind 4, the trough example's nearest-node rule on the absorber tube (radius 35 mm,
+    12 m), on the device against the oracle's restatement of the example's functions (pinned
+    to them in tests/test_binning_kat.py): the same rays land in the same nodes; every
+    absorbed hit is binned."""
+    nx, ny = mesh
+    m = (3, 2, 4, nx, ny, 0.0, 0.035, -6.0, 6.0, 1)
+    sc = scenes.trough_scene(40000)
+    ctx = _product(product, sc, 9, [m])
+    try:
+        got = product.flux(ctx, 0, nx, ny)
+        rec = product.records(ctx)
+        absorbed = int(np.sum((np.asarray(rec["stage"]) == 3) & (np.asarray(rec["element"]) == -2)))
+    finally:
+        product.st_free_context(ctx)
+    np.testing.assert_array_equal(got, _oracle_bins(oracle, sc, 9, m))
+    assert got.sum() == absorbed > 0
+
+
 def test_flux_stats_without_records_counts_intersections(product):
     """With records off the run still counts its intersections for the mean-flux uncertainty."""
     sc = scenes.dish_scene(30000)
@@ -117,7 +137,8 @@ def test_flux_stats_rejects_bad_requests(product):
     ctx = product.st_create_context()
     try:
         scenes.push(product, ctx, scenes.dish_scene(100))
-        assert product.st_b200_add_flux_map(ctx, 2, 1, 4, 10, 10, 0.0, 1.0, 0.0, 1.0, 1) == -1  # kind
+        assert product.st_b200_add_flux_map(ctx, 2, 1, 5, 10, 10, 0.0, 1.0, 0.0, 1.0, 1) == -1  # kind
+        assert product.st_b200_add_flux_map(ctx, 2, 1, 4, 10, 10, 0.0, 0.0, 0.0, 1.0, 1) == -1  # radius
         assert product.st_b200_add_flux_map(ctx, 2, 1, 2, 10, 10, 1.0, 0.0, 0.0, 1.0, 1) == -1  # x range
         m = product.st_b200_add_flux_map(ctx, *DISH_GUI)
         with pytest.raises(RuntimeError):

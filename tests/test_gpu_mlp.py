@@ -141,3 +141,41 @@ def test_network_learns_teacher(product):
     torch.cuda.synchronize()
     assert net.error() == 0
     assert last.item() < first / 10, (first, last.item())
+
+
+FUSED_CASES = [  # (rows, dims, group_rows)
+    (77, (8, 256, 256, 1024), 0),                       # one partial tile
+    (40_000, (8, 256, 256, 256, 256, 256, 1024), 0),    # more tiles than SMs: the persistent loop
+    (5_000, (3, 256, 256, 256, 512), 0),
+    (6_000, (8, 256, 256, 256, 256, 256, 1024), 2000),  # field sums: warps straddle group edges
+    (1_000, (16, 256, 256), 7),                         # every warp straddles one
+]
+
+
+@pytest.mark.parametrize("case", FUSED_CASES, ids=[f"{c[0]}-{len(c[1]) - 1}L-{c[1][-1]}-g{c[2]}" for c in FUSED_CASES])
+def test_fused_forward_matches_layers(product, case):
+    """The fused kernel (all layers in one launch, activations kept on chip) gives the per-layer
+    GEMM path's output: the same bf16 roundings between layers and the same K order in the
+    accumulator, so rows agree to float rounding; group sums agree with summing those rows."""
+    import torch
+    from soltrace_b200.surrogate import Mlp
+    rows, dims, group = case
+    net = Mlp(product, dims=dims, seed=rows)
+    rng = np.random.default_rng(rows)
+    for b in net.b:
+        b.copy_(torch.from_numpy(rng.normal(scale=0.1, size=b.numel()).astype(np.float32)))
+    x = torch.from_numpy(rng.normal(size=(rows, dims[0])).astype(np.float32)).to(torch.bfloat16).cuda()
+    want = net.forward(x).double()
+    scale = 0.5
+    got = net.forward_fused(x, group_rows=group, scale=scale, clamp=group > 0)
+    torch.cuda.synchronize()
+    assert net.error() == 0
+    if group == 0:
+        err = (got.double() - scale * want).abs().max().item()
+        assert err <= 1e-5 * (scale * want).abs().max().item(), err
+    else:
+        per_row = (scale * want).clamp(min=0.0)
+        sums = torch.stack([per_row[i:i + group].sum(0) for i in range(0, rows, group)])
+        err = (got.double() - sums).abs().max().item()
+        assert err <= 1e-5 * sums.abs().max().item(), err
+
