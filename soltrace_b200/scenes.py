@@ -321,16 +321,40 @@ BEAM_DOWN_HEIGHT = 120.0     # secondary vertex height (m)
 BEAM_DOWN_ECC = 1.3          # hyperboloid eccentricity
 BEAM_DOWN_DIAM = 20.0        # secondary aperture diameter (m)
 LIP_RA, LIP_RS = 10.0, 0.5   # torus lip: annular and cross-section radius (m)
-GROUND_MAP = (3, 1, 0, 64, 64, -8.0, 8.0, -8.0, 8.0, 1)  # ground receiver, 64 x 64 over 16 m x 16 m, absorbed
+FOCUS_BELOW_RIM = 1.0        # upper focus this far below the secondary's rim plane (m)
+GROUND_HALF = 32.0           # ground receiver half-width (m): holds the beam diverging from the lower focus
+GROUND_MAP = (3, 1, 0, 64, 64, -GROUND_HALF, GROUND_HALF, -GROUND_HALF, GROUND_HALF, 1)  # 64 x 64, absorbed
+
+
+def _hyperboloid_sag(R: float, kappa: float, r: float) -> float:
+    """Height above the vertex of x^2 + y^2 + kappa z^2 - 2 R z = 0 at radius r (the root
+    nearest the vertex)."""
+    return (R - math.sqrt(R * R - kappa * r * r)) / kappa
 
 
 def beam_down_geometry(height: float = BEAM_DOWN_HEIGHT, ecc: float = BEAM_DOWN_ECC):
-    """(vertex curvature c, kappa, upper focus height) of a convex hyperboloid whose vertex is
-    at `height` and whose lower focus is on the ground.  SolTrace's 'o' surface is
-    x^2 + y^2 + kappa z^2 - 2 z / c = 0 (kappa = 1 - e^2); the foci lie R/(1+e) above and
-    R/(e-1) below the vertex, R = 1/c, so R = height (e - 1)."""
-    R = height * (ecc - 1.0)
-    return 1.0 / R, 1.0 - ecc * ecc, height + R / (1.0 + ecc)
+    """(vertex curvature c, kappa, upper focus height, lower focus height) of the convex
+    hyperboloid secondary.  SolTrace's 'o' surface is x^2 + y^2 + kappa z^2 - 2 z / c = 0
+    (kappa = 1 - e^2); its foci lie R/(1+e) above and R/(e-1) below the vertex, R = 1/c.
+    A ray aimed at the upper focus meets the mirror only if that focus lies inside the bowl,
+    below the rim plane: rays from heliostats 1 km out rise about 1.2 m over the last 10 m,
+    so R is chosen (by bisection) to put the upper focus FOCUS_BELOW_RIM under the rim.
+    The lower focus is then ~91 m up, and the beam spreads from it to the ground receiver."""
+    kappa = 1.0 - ecc * ecc
+    r = BEAM_DOWN_DIAM / 2.0
+
+    def gap(R):  # focus height above the vertex minus (rim height - FOCUS_BELOW_RIM)
+        return R / (1.0 + ecc) - (_hyperboloid_sag(R, kappa, r) - FOCUS_BELOW_RIM)
+
+    lo, hi = 0.5, 10.0 * r
+    for _ in range(100):
+        mid = 0.5 * (lo + hi)
+        if (gap(lo) <= 0.0) == (gap(mid) <= 0.0):
+            lo = mid
+        else:
+            hi = mid
+    R = 0.5 * (lo + hi)
+    return 1.0 / R, kappa, height + R / (1.0 + ecc), height - R / (ecc - 1.0)
 
 
 def beam_down_scene(n_helio: int = 10000, raycount: int = 1_000_000, sun_xyz=None, r_min: float = 100.0,
@@ -339,11 +363,14 @@ def beam_down_scene(n_helio: int = 10000, raycount: int = 1_000_000, sun_xyz=Non
     (same density), a convex hyperboloid secondary (eccentricity 1.3, kappa = -0.69, 20 m
     aperture, vertex at 120 m, surface 'o' of quadricsurfaceclosedform.cpp:129-148) with an
     absorbing torus lip (surface 'd', annular radius 10 m, cross-section 0.5 m, aperture 'a'
-    as input.cpp:349-355 requires) around its rim, and a flat ground receiver at the lower
-    focus.  The heliostats are aimed at the upper focus for `sun_xyz` (default: 45 deg
+    as input.cpp:349-355 requires) around its rim, and a flat 64 m x 64 m ground receiver
+    under the lower focus (beam_down_geometry).  The secondary's stage is single-hit: the 'o'
+    surface equation also holds on the hyperboloid's second sheet, 25 m under the vertex and
+    inside the circular aperture, which rays reflected toward the lower focus would otherwise
+    meet.  The heliostats are aimed at the upper focus for `sun_xyz` (default: 45 deg
     elevation, south); st_b200_sim_run_batch re-aims them per sun position with that focus
     as its tracking target (beam_down_target)."""
-    c, kappa, f1 = beam_down_geometry()
+    c, kappa, f1, _ = beam_down_geometry()
     if r_max is None:  # the density of the 2,000-heliostat field over 100-1000 m
         r_max = math.sqrt(n_helio / 2000.0 * (1000.0 ** 2 - r_min ** 2) + r_min ** 2)
     xy = field_layout(n_helio, r_min=r_min, r_max=r_max)
@@ -364,7 +391,8 @@ def beam_down_scene(n_helio: int = 10000, raycount: int = 1_000_000, sun_xyz=Non
     lip = Element(origin=(0.0, 0.0, rim - LIP_RS), aim=(0.0, 0.0, rim + 100.0), aperture="a",
                   aperture_params=(0.0, 0.0, 360.0), surface="d", surface_params=(LIP_RA, LIP_RS), interaction=2,
                   optic="lip")
-    ground = Element(origin=(0.0, 0.0, 0.0), aim=(0.0, 0.0, 100.0), aperture="r", aperture_params=(16.0, 16.0),
+    ground = Element(origin=(0.0, 0.0, 0.0), aim=(0.0, 0.0, 100.0), aperture="r",
+                     aperture_params=(2.0 * GROUND_HALF, 2.0 * GROUND_HALF),
                      surface="f", interaction=2, optic="receiver")
     optics = [OpticSet("helio", OpticFace("g", refl=0.9, slope=slope), OpticFace("g", refl=0.9, slope=slope)),
               OpticSet("secondary", OpticFace("g", refl=0.95, slope=0.5), OpticFace("g", refl=0.95, slope=0.5)),
@@ -372,17 +400,14 @@ def beam_down_scene(n_helio: int = 10000, raycount: int = 1_000_000, sun_xyz=Non
               OpticSet("receiver", OpticFace("g", refl=0.0), OpticFace("g", refl=0.0))]
     t_, inten = buie_csr_table(csr)
     sun = Sun("d", 0.0, tuple(1.0e4 * s), table=(t_, inten))
-    return Scene(sun, optics, [Stage(helios), Stage([secondary, lip]), Stage([ground])], raycount=raycount,
-                 raymax=2_000_000_000 - 1, dynamic_group=True, name="beam_down")
+    return Scene(sun, optics, [Stage(helios), Stage([secondary, lip], multihit=False), Stage([ground])],
+                 raycount=raycount, raymax=2_000_000_000 - 1, dynamic_group=True, name="beam_down")
 
 
 def beam_down_rim_height() -> float:
-    """Height of the secondary's rim (r = 10 m) on x^2 + y^2 + kappa z^2 - 2 z / c = 0."""
-    c, kappa, _ = beam_down_geometry()
-    r2 = (BEAM_DOWN_DIAM / 2.0) ** 2
-    # kappa z^2 - (2/c) z + r2 = 0, the root nearest the vertex
-    b = 2.0 / c
-    return BEAM_DOWN_HEIGHT + (b - math.sqrt(b * b - 4.0 * kappa * r2)) / (2.0 * kappa)
+    """Height of the secondary's rim (r = 10 m)."""
+    c, kappa, _, _ = beam_down_geometry()
+    return BEAM_DOWN_HEIGHT + _hyperboloid_sag(1.0 / c, kappa, BEAM_DOWN_DIAM / 2.0)
 
 
 def beam_down_target() -> np.ndarray:
