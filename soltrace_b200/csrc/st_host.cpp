@@ -1,6 +1,6 @@
 // Host side of coretrace_api.so: the SolTrace context and its C API
-// (coretrace/stapi.h:68-176), geometry set-up, acceleration structures and
-// the assembly of the records the device returns into the reference's order.
+// (coretrace/stapi.h:68-176), geometry set-up, acceleration structures and the
+// readback of the records the device puts in the reference's order (st_run.cu).
 //
 // The scene model follows coretrace/types.h:85-343; set-up follows
 // coretrace/input.cpp (InitGeometries 153-286, TranslateSurfaceParams 288-366,
@@ -92,7 +92,7 @@ struct Context {
     bool dyn = false, err_sun = true, err_opt = true;
     std::vector<std::string> messages;
     // results
-    std::vector<RecordDev> records;  // reference order
+    RecordColumns rec;  // the last run's records in the reference's order (host memory of the workspace)
     uint64_t sun_rays = 0;
     int precision = ST_B200_FP64;
     bool want_records = true;
@@ -1334,78 +1334,6 @@ bool flatten(Context *cx, HostScene &hs) {
     return true;
 }
 
-// reference record order: per stage sorted by (ray number, hit index), then the
-// block merge of TRayData::Merge (types.cpp:311-355)
-void assemble_records(Context *cx, RunResult &rr, bool replay) {
-    const int nst = int(cx->stages.size());
-    std::vector<RecordDev> &recs = rr.records;
-    const uint32_t N = uint32_t(rr.ray_hits);
-    // the reference traces no later stage when the only ray carried out of the first
-    // stage is the last numbered one (raytrace.cpp:786-797 never marks it); a replay does
-    // not trace the first stage
-    const bool drop_later = !replay && nst > 1 && rr.stage_entries.size() > 1 && rr.stage_entries[1] == 1 &&
-                            rr.max_enter[1] == N;
-    std::vector<std::vector<RecordDev>> per(nst);
-    for (const RecordDev &r : recs) {
-        const int s = r.stage - 1;
-        if (s < 0 || s >= nst) continue;
-        if (drop_later && s >= 1) continue;
-        // the last ray of a trace-through stage that misses leaves no record (raytrace.cpp:810-811)
-        if (s >= 1 && cx->stages[s].tracethrough && r.element == 0 && rr.max_ttmiss[s] != 0 &&
-            rr.max_ttmiss[s] == rr.max_enter[s] && r.raynum == rr.max_enter[s])
-            continue;
-        per[s].push_back(r);
-    }
-    for (auto &v : per)
-        std::sort(v.begin(), v.end(), [](const RecordDev &a, const RecordDev &b) {
-            return a.raynum != b.raynum ? a.raynum < b.raynum : a.seq < b.seq;
-        });
-    const size_t B = 8192;
-    struct Blk {
-        int stage;
-        size_t off, n;  // contiguous piece of one stage
-        std::vector<std::pair<int, size_t>> pieces;  // (stage, start) of each record when mixed
-    };
-    // A block holds up to B records as a list of (stage, start, count) runs.
-    struct Run {
-        int s;
-        size_t start, n;
-    };
-    std::vector<std::vector<Run>> all;
-    auto blk_size = [](const std::vector<Run> &b) {
-        size_t t = 0;
-        for (auto &r : b) t += r.n;
-        return t;
-    };
-    for (int s = 0; s < nst; ++s) {
-        std::vector<std::vector<Run>> src;
-        for (size_t i = 0; i < per[s].size(); i += B) src.push_back({Run{s, i, std::min(B, per[s].size() - i)}});
-        std::vector<std::vector<Run>> full, partial;
-        for (auto &b : all) (blk_size(b) == B ? full : partial).push_back(b);
-        for (auto &b : src) (blk_size(b) == B ? full : partial).push_back(b);
-        all = full;
-        for (auto &b : partial)
-            for (const Run &r : b) {
-                size_t done = 0;
-                while (done < r.n) {
-                    if (all.empty() || blk_size(all.back()) == B) all.push_back({});
-                    const size_t room = B - blk_size(all.back());
-                    const size_t k = std::min(room, r.n - done);
-                    all.back().push_back(Run{r.s, r.start + done, k});
-                    done += k;
-                }
-            }
-    }
-    cx->records.clear();
-    size_t total = 0;
-    for (auto &v : per) total += v.size();
-    cx->records.reserve(total);
-    for (auto &b : all)
-        for (const Run &r : b) cx->records.insert(cx->records.end(), per[r.s].begin() + r.start, per[r.s].begin() + r.start + r.n);
-    recs.clear();
-    recs.shrink_to_fit();
-}
-
 // Saved second-stage input as the reference leaves it (raytrace.cpp:1064-1078): the stage's
 // ray array at the end of stage 2 holds, in ray order, the rays that left stage 2 in its
 // first positions (written back in place as they were produced) and the rays that entered
@@ -1540,7 +1468,7 @@ bool ensure_scene(Context *cx) {
 }
 
 int run(Context *cx, unsigned seed) {
-    cx->records.clear();
+    cx->rec = RecordColumns{};
     memset(&cx->stats, 0, sizeof cx->stats);
     cx->stage_s0.clear();
     cx->stage_s1.clear();
@@ -1603,6 +1531,28 @@ int run(Context *cx, unsigned seed) {
                 rq.replay_fe0[k] = f0 + it->second - 1;
         }
         rq.replay_sun_rays = n0 ? uint64_t(cx->replay_s0[8 * (n0 - 1) + 7]) : 0;
+        // the saved stage-1 records are the replay's stage-1 records (raytrace.cpp:554-565)
+        if (rq.records) {
+            double last = -1;
+            uint32_t seq = 0;
+            rq.pre_records.reserve(n0);
+            for (size_t k = 0; k < n0; ++k) {
+                const double *row = cx->replay_s0.data() + 8 * k;
+                RecordDev r;
+                memset(&r, 0, sizeof r);
+                for (int q = 0; q < 3; ++q) {
+                    r.pos[q] = row[q];
+                    r.cos[q] = row[3 + q];
+                }
+                r.element = int(row[6]);
+                r.stage = 1;
+                r.raynum = uint32_t(row[7]);
+                seq = (row[7] == last) ? seq + 1 : 0;
+                last = row[7];
+                r.seq = seq;
+                rq.pre_records.push_back(r);
+            }
+        }
     }
     RunResult rr;
     const double host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
@@ -1617,28 +1567,6 @@ int run(Context *cx, unsigned seed) {
     const int nst = int(cx->stages.size());
     const uint32_t N = uint32_t(rr.ray_hits);
     const bool drop_later = !cx->replaying && nst > 1 && rr.stage_entries[1] == 1 && rr.max_enter[1] == N;
-    if (cx->replaying) {
-        // the saved stage-1 records are the replay's stage-1 records (raytrace.cpp:554-565)
-        const size_t n0 = cx->replay_s0.size() / 8;
-        double last = -1;
-        uint32_t seq = 0;
-        for (size_t k = 0; k < n0; ++k) {
-            const double *row = cx->replay_s0.data() + 8 * k;
-            RecordDev r;
-            memset(&r, 0, sizeof r);
-            for (int q = 0; q < 3; ++q) {
-                r.pos[q] = row[q];
-                r.cos[q] = row[3 + q];
-            }
-            r.element = int(row[6]);
-            r.stage = 1;
-            r.raynum = uint32_t(row[7]);
-            seq = (row[7] == last) ? seq + 1 : 0;
-            last = row[7];
-            r.seq = seq;
-            rr.records.push_back(r);
-        }
-    }
     // flux maps and per-element counts
     for (size_t m = 0; m < cx->flux.size(); ++m) {
         cx->flux[m].counts = rr.flux[m];
@@ -1678,23 +1606,24 @@ int run(Context *cx, unsigned seed) {
     S.trace_variant = rr.trace_variant;
     if (rr.flags & 1u) cx->log("warning: a ray reached the limit of intersections per stage; it was stopped there");
     const auto ta = std::chrono::steady_clock::now();
-    if (cx->want_records) assemble_records(cx, rr, cx->replaying);
+    cx->rec = rr.rec;  // ordered on the device (gpu_run)
+    const RecordColumns &R = cx->rec;
     if (cx->save_stage_data) {
         // stage-1 records in ray order (the records of stage 1 keep that order in the merged
         // readback) and the second stage's input as the reference saves it
-        for (const RecordDev &r : cx->records)
-            if (r.stage == 1) {
-                const double row[8] = {r.pos[0], r.pos[1], r.pos[2], r.cos[0], r.cos[1], r.cos[2], double(r.element),
-                                       double(r.raynum)};
+        for (size_t i = 0; i < R.n; ++i)
+            if (R.stage[i] == 1) {
+                const double row[8] = {R.x[i], R.y[i], R.z[i], R.cx[i], R.cy[i], R.cz[i], double(R.element[i]),
+                                       double(R.raynum[i])};
                 cx->stage_s0.insert(cx->stage_s0.end(), row, row + 8);
             }
         if (nst >= 2) cx->stage_s1 = saved_second_stage(rr.saved[0], rr.saved[1]);
     }
     S.readback_ms = rr.readback_ms + std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
-    S.records = cx->records.size();
+    S.records = R.n;
     // over several ranks the records are this rank's, the counts the whole run's
-    S.intersections = (cx->want_records && cx->nranks <= 1) ? uint64_t(cx->records.size()) : rr.intersections;
-    return int(cx->records.size());
+    S.intersections = (cx->want_records && cx->nranks <= 1) ? uint64_t(R.n) : rr.intersections;
+    return int(R.n);
 }
 
 // Batched runs keep every position's sun-plane grid on the device at once (per chunk of
@@ -2280,41 +2209,44 @@ int st_sun_userdata(st_context_t p, st_uint_t n, double angle[], double intensit
     }
     return int(n);
 }
+// readback (stapi.cpp:570-647): the caller's arrays hold st_num_intersections() entries;
+// each is one copy of a column of the ordered records
 int st_num_intersections(st_context_t p) {
     CTX(p, -1);
-    return int(cx->records.size());
+    return int(cx->rec.n);
+}
+static void copy_col(void *dst, const void *src, size_t bytes) {
+    if (dst && src && bytes) memcpy(dst, src, bytes);
 }
 int st_locations(st_context_t p, double *x, double *y, double *z) {
     CTX(p, -1);
-    for (size_t i = 0; i < cx->records.size(); ++i) {
-        x[i] = cx->records[i].pos[0];
-        y[i] = cx->records[i].pos[1];
-        z[i] = cx->records[i].pos[2];
-    }
+    const size_t b = cx->rec.n * sizeof(double);
+    copy_col(x, cx->rec.x, b);
+    copy_col(y, cx->rec.y, b);
+    copy_col(z, cx->rec.z, b);
     return 1;
 }
 int st_cosines(st_context_t p, double *x, double *y, double *z) {
     CTX(p, -1);
-    for (size_t i = 0; i < cx->records.size(); ++i) {
-        x[i] = cx->records[i].cos[0];
-        y[i] = cx->records[i].cos[1];
-        z[i] = cx->records[i].cos[2];
-    }
+    const size_t b = cx->rec.n * sizeof(double);
+    copy_col(x, cx->rec.cx, b);
+    copy_col(y, cx->rec.cy, b);
+    copy_col(z, cx->rec.cz, b);
     return 1;
 }
 int st_elementmap(st_context_t p, int *m) {
     CTX(p, -1);
-    for (size_t i = 0; i < cx->records.size(); ++i) m[i] = cx->records[i].element;
+    copy_col(m, cx->rec.element, cx->rec.n * sizeof(int));
     return 1;
 }
 int st_stagemap(st_context_t p, int *m) {
     CTX(p, -1);
-    for (size_t i = 0; i < cx->records.size(); ++i) m[i] = cx->records[i].stage;
+    copy_col(m, cx->rec.stage, cx->rec.n * sizeof(int));
     return 1;
 }
 int st_raynumbers(st_context_t p, int *m) {
     CTX(p, -1);
-    for (size_t i = 0; i < cx->records.size(); ++i) m[i] = int(cx->records[i].raynum);
+    copy_col(m, cx->rec.raynum, cx->rec.n * sizeof(int));
     return 1;
 }
 int st_sun_stats(st_context_t p, double *xmin, double *xmax, double *ymin, double *ymax, int *nsun) {

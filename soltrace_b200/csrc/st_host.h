@@ -55,6 +55,7 @@ struct RunRequest {
     std::vector<double> replay_rows;    // 7 doubles per ray: global position, direction, ray number
     std::vector<int> replay_fe0;        // per ray: global index of its first first-stage element, -1
     uint64_t replay_sun_rays = 0;       // SunRayCount of a replay (the last saved stage-1 ray number)
+    std::vector<RecordDev> pre_records; // replay: the saved stage-1 records, ordered with the traced ones
     // one rank of a run split over several GPUs (st_b200_set_ranks): this rank traces its
     // contiguous slice of every batch's sun-ray range and exchanges through the callbacks
     int rank = 0, nranks = 1;
@@ -63,12 +64,20 @@ struct RunRequest {
     void *comm_user = nullptr;
 };
 
+// The records of a run in the reference's readback order (TRayData::Merge), as columns in
+// host memory that the context's workspace owns; valid until its next run.
+struct RecordColumns {
+    const double *x = nullptr, *y = nullptr, *z = nullptr, *cx = nullptr, *cy = nullptr, *cz = nullptr;
+    const int *element = nullptr, *stage = nullptr, *raynum = nullptr;
+    size_t n = 0;
+};
+
 struct RunResult {
     bool ok = false;
     bool cancelled = false;
     std::string error;
     uint64_t sun_rays = 0, ray_hits = 0;
-    std::vector<RecordDev> records;  // unordered, as produced by the device
+    RecordColumns rec;               // the run's records in the reference's order (host memory of the workspace)
     std::vector<uint64_t> stage_entries;
     std::vector<uint32_t> max_enter, max_ttmiss;
     std::vector<std::vector<unsigned long long>> flux;

@@ -167,6 +167,36 @@ void launch_scan(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_
                  cudaStream_t st);
 constexpr int kScanChunk = 2048, kScanBlock = 256;
 constexpr size_t scan_parts(uint32_t nb) { return (size_t(nb) + kScanChunk - 1) / kScanChunk + 1; }
+// the same scan for arrays of any length (up to 2^31 entries): chunk sums, their scan, and
+// the chunks' scans from it.  offsets may be counts (in place).  parts holds
+// scan_parts(nb) entries, parts2 scan_parts(scan_parts(nb)).
+void launch_scan_large(const uint32_t *counts, uint32_t nb, uint32_t *offsets, uint32_t *total, uint32_t *parts,
+                       uint32_t *parts2, cudaStream_t st);
+
+// Ordering of a run's records on the device (the reference's readback order,
+// TRayData::Merge in types.cpp:311-355): records are counted per (stage, ray number), the
+// counts scanned into the first slot of every key, and each record is written to the slot
+// of its key plus its hit index, mapped through the block-merge runs of its stage, as
+// columns.
+struct RecOrder {
+    const RecordDev *recs;
+    unsigned long long n;
+    uint32_t rb;                     // ray numbers 0..rb per stage (key space nst * (rb + 1))
+    int nst;
+    int drop_later;                  // the records of every stage after the first are dropped
+    uint32_t tt_drop[kMaxStages];    // per stage: the ray number whose miss record is dropped (0: none)
+    uint32_t *key;                   // per key: count, then (after the scan) its first slot
+    unsigned long long *stage_count; // kept records per stage
+    const uint32_t *run_src, *run_dst;  // merge runs, stage by stage, by start in the stage's order
+    const int *run_seg;              // the runs of stage s are [run_seg[s], run_seg[s + 1])
+    double *col_d;                   // x, y, z, cx, cy, cz: 6 columns of `total` doubles
+    int *col_i;                      // element, stage, ray number: 3 columns of `total` ints
+    unsigned long long total;        // kept records
+    unsigned int *bad;               // set when a record lies outside the key space
+};
+void launch_rec_count(const RecOrder &o, cudaStream_t st);
+void launch_rec_scatter(const RecOrder &o, cudaStream_t st);
+
 void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uint32_t *counts,
                     const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st);
 // cut-off and run state after a batch; the last numbered sun ray is read from the

@@ -26,14 +26,39 @@ struct DevBuf {
     ~DevBuf() {
         if (p) cudaFree(p);
     }
+    // at least b bytes; a buffer that must grow gets a quarter more than asked, so that runs
+    // whose sizes drift by a little (batch sizes planned from the last run's hit rate) do not
+    // reallocate (cudaFree waits for the whole device)
     cudaError_t ensure(size_t b) {
         if (b <= bytes && p) return cudaSuccess;
         if (p) cudaFree(p);
         p = nullptr;
         bytes = 0;
-        cudaError_t e = cudaMalloc(&p, b ? b : 16);
-        if (e == cudaSuccess) bytes = b;
+        const size_t want = b ? b + b / 4 : 16;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {  // without the headroom
+            cudaGetLastError();
+            e = cudaMalloc(&p, b ? b : 16);
+            if (e == cudaSuccess) bytes = b ? b : 16;
+            return e;
+        }
+        bytes = want;
         return e;
+    }
+    // grow to at least b bytes keeping the first `keep` bytes (stream-ordered copy)
+    cudaError_t grow_keep(size_t b, size_t keep, cudaStream_t s) {
+        if (b <= bytes && p) return cudaSuccess;
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, b ? b : 16);
+        if (e != cudaSuccess) return e;
+        if (p && keep && (e = cudaMemcpyAsync(q, p, std::min(keep, bytes), cudaMemcpyDeviceToDevice, s))) {
+            cudaFree(q);
+            return e;
+        }
+        if (p) cudaFree(p);  // waits for the copy
+        p = q;
+        bytes = b;
+        return cudaSuccess;
     }
     template <typename T>
     T *as() const {
@@ -67,6 +92,11 @@ struct Workspace {
     DevBuf wf_sid, wf_raynum, wf_draw, wf_meta, wf_fe0, wf_p, wf_c, wf_q0, wf_q1, wf_qs, wf_counts;
     DevBuf save_rows[2], save_count, replay_rows, replay_fe0;  // stage-data save / replay
     DevBuf ecount, ecursor, etotal, s_sid, s_el, s_idx;
+    // record ordering: key counts / slots, scan partials, per-stage counts, merge runs, columns
+    DevBuf rec_key, rec_parts, rec_parts2, rec_stage, rec_runs, rec_cols, rec_bad;
+    void *rec_host = nullptr;  // the ordered records' columns in host memory (pinned when possible)
+    size_t rec_host_bytes = 0;
+    bool rec_host_pinned = false;
     // batched runs: per-position sun tables, element copies, run states, counters, accumulators
     DevBuf pos_cells, pos_disc, pos_par, pos_elems, pos_rs, pos_ctr, pos_acc;
     std::vector<cudaEvent_t> events;
@@ -78,6 +108,12 @@ struct Workspace {
     DevBuf tune_rs;
     ~Workspace() {
         if (device >= 0) cudaSetDevice(device);
+        if (rec_host) {
+            if (rec_host_pinned)
+                cudaFreeHost(rec_host);
+            else
+                free(rec_host);
+        }
         for (auto e : events) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -199,6 +235,176 @@ static cudaError_t wf_buffers(Workspace &ws, const SceneDev &S, uint64_t cap, Wf
     W.c = ws.wf_c.as<double>();
     W.cap = uint32_t(cap);
     return cudaSuccess;
+}
+
+// TRayData::Merge (types.cpp:311-355): a stage's records are kept in blocks of 8192; merging
+// the stages in turn puts the full blocks of all stages so far first and packs the partial
+// blocks' records after them.  Returns the runs of the merged order: (stage, start in the
+// stage's sorted order, length), in output order.
+struct MergeRun {
+    int s;
+    uint64_t start, n;
+};
+static std::vector<MergeRun> merge_runs(const std::vector<uint64_t> &per_stage) {
+    const uint64_t B = 8192;
+    auto blk_size = [](const std::vector<MergeRun> &b) {
+        uint64_t t = 0;
+        for (auto &r : b) t += r.n;
+        return t;
+    };
+    std::vector<std::vector<MergeRun>> all;
+    for (int s = 0; s < int(per_stage.size()); ++s) {
+        const uint64_t n = per_stage[size_t(s)];
+        std::vector<std::vector<MergeRun>> full, partial;
+        for (auto &b : all) (blk_size(b) == B ? full : partial).push_back(b);
+        for (uint64_t i = 0; i < n; i += B) {
+            std::vector<MergeRun> b{MergeRun{s, i, std::min(B, n - i)}};
+            (b[0].n == B ? full : partial).push_back(b);
+        }
+        all = full;
+        for (auto &b : partial)
+            for (const MergeRun &r : b) {
+                uint64_t done = 0;
+                while (done < r.n) {
+                    if (all.empty() || blk_size(all.back()) == B) all.push_back({});
+                    const uint64_t k = std::min(B - blk_size(all.back()), r.n - done);
+                    all.back().push_back(MergeRun{r.s, r.start + done, k});
+                    done += k;
+                }
+            }
+    }
+    std::vector<MergeRun> out;
+    for (auto &b : all)
+        for (const MergeRun &r : b) {
+            if (!out.empty() && out.back().s == r.s && out.back().start + out.back().n == r.start)
+                out.back().n += r.n;  // contiguous pieces of one stage
+            else
+                out.push_back(r);
+        }
+    return out;
+}
+
+// Put the run's nrec device records into the reference's readback order (per stage by ray
+// number and hit index, then the block merge), dropping the records the reference does not
+// write (drop_later: every record after the first stage; tt_drop[s]: the miss record of that
+// ray number in trace-through stage s), as columns in the workspace's host buffer.
+static std::string order_records(Workspace &ws, const RecordDev *recs, unsigned long long nrec, int nst,
+                                 bool drop_later, const uint32_t *tt_drop, uint32_t rb, RecordColumns &col,
+                                 uint64_t &d2h, cudaStream_t st) {
+    col = RecordColumns{};
+    const uint64_t nkeys = uint64_t(nst) * (uint64_t(rb) + 1);
+    if (nkeys >= (uint64_t(1) << 31) || nrec >= (uint64_t(1) << 31))
+        return "too many records to order (at most 2^31 records and stages x ray numbers)";
+    cudaError_t e;
+    RecOrder o{};
+    o.recs = recs;
+    o.n = nrec;
+    o.rb = rb;
+    o.nst = nst;
+    o.drop_later = drop_later ? 1 : 0;
+    for (int s = 0; s < nst; ++s) o.tt_drop[s] = tt_drop[s];
+    if ((e = ws.rec_key.ensure(nkeys * 4)) || (e = ws.rec_stage.ensure(kMaxStages * 8)) ||
+        (e = ws.rec_bad.ensure(8)) || (e = ws.rec_parts.ensure(scan_parts(uint32_t(nkeys)) * 4)) ||
+        (e = ws.rec_parts2.ensure(scan_parts(uint32_t(scan_parts(uint32_t(nkeys)))) * 4)))
+        return std::string("CUDA error: ") + cudaGetErrorString(e);
+    o.key = ws.rec_key.as<uint32_t>();
+    o.stage_count = ws.rec_stage.as<unsigned long long>();
+    o.bad = ws.rec_bad.as<unsigned int>();
+    cudaMemsetAsync(o.key, 0, nkeys * 4, st);
+    cudaMemsetAsync(o.stage_count, 0, kMaxStages * 8, st);
+    cudaMemsetAsync(o.bad, 0, 8, st);
+    if (nrec) launch_rec_count(o, st);
+    unsigned long long cnt[kMaxStages] = {0};
+    unsigned int bad = 0;
+    cudaMemcpyAsync(cnt, o.stage_count, kMaxStages * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&bad, o.bad, 4, cudaMemcpyDeviceToHost, st);
+    // the key slots: exclusive scan of the counts, in place (runs while the host plans the merge)
+    launch_scan_large(o.key, uint32_t(nkeys), o.key, ws.rec_bad.as<uint32_t>() + 1, ws.rec_parts.as<uint32_t>(),
+                      ws.rec_parts2.as<uint32_t>(), st);
+    if ((e = cudaStreamSynchronize(st))) return std::string("CUDA error: ") + cudaGetErrorString(e);
+    if (bad) return "a record's ray number lies outside the run's ray numbers";
+    std::vector<uint64_t> per(static_cast<size_t>(nst));
+    uint64_t total = 0;
+    for (int s = 0; s < nst; ++s) total += (per[size_t(s)] = cnt[s]);
+    // merge runs per stage, by start: (source start, destination) pairs and per-stage segments
+    const std::vector<MergeRun> runs = merge_runs(per);
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> by_stage(static_cast<size_t>(nst));
+    uint64_t dst = 0;
+    for (const MergeRun &r : runs) {
+        by_stage[size_t(r.s)].push_back({uint32_t(r.start), uint32_t(dst)});
+        dst += r.n;
+    }
+    std::vector<uint32_t> table;  // run_src | run_dst | run_seg (as uint32)
+    std::vector<uint32_t> src, dsts;
+    std::vector<int> seg(static_cast<size_t>(nst) + 1, 0);
+    for (int s = 0; s < nst; ++s) {
+        auto &v = by_stage[size_t(s)];
+        std::sort(v.begin(), v.end());
+        seg[size_t(s)] = int(src.size());
+        for (auto &pr : v) {
+            src.push_back(pr.first);
+            dsts.push_back(pr.second);
+        }
+        if (v.empty()) {  // a stage without records: one empty run keeps the search in range
+            src.push_back(0);
+            dsts.push_back(0);
+        }
+    }
+    seg[size_t(nst)] = int(src.size());
+    const size_t nr = src.size();
+    table.resize(2 * nr + seg.size());
+    std::copy(src.begin(), src.end(), table.begin());
+    std::copy(dsts.begin(), dsts.end(), table.begin() + nr);
+    for (size_t k = 0; k < seg.size(); ++k) table[2 * nr + k] = uint32_t(seg[k]);
+    const size_t col_bytes = size_t(total) * (6 * sizeof(double) + 3 * sizeof(int));
+    if ((e = ws.rec_runs.ensure(table.size() * 4)) || (e = ws.rec_cols.ensure(std::max<size_t>(col_bytes, 16))))
+        return std::string("CUDA error: ") + cudaGetErrorString(e);
+    if ((e = cudaMemcpyAsync(ws.rec_runs.p, table.data(), table.size() * 4, cudaMemcpyHostToDevice, st)))
+        return std::string("CUDA error: ") + cudaGetErrorString(e);
+    o.run_src = ws.rec_runs.as<uint32_t>();
+    o.run_dst = o.run_src + nr;
+    o.run_seg = reinterpret_cast<const int *>(o.run_src + 2 * nr);
+    o.col_d = ws.rec_cols.as<double>();
+    o.col_i = reinterpret_cast<int *>(o.col_d + 6 * total);
+    o.total = total;
+    if (nrec && total) launch_rec_scatter(o, st);
+    // host buffer (grows only; page-locked when the system allows it)
+    if (ws.rec_host_bytes < col_bytes) {
+        if (ws.rec_host) {
+            if (ws.rec_host_pinned)
+                cudaFreeHost(ws.rec_host);
+            else
+                free(ws.rec_host);
+        }
+        ws.rec_host = nullptr;
+        ws.rec_host_bytes = 0;
+        ws.rec_host_pinned = cudaMallocHost(&ws.rec_host, col_bytes) == cudaSuccess;
+        if (!ws.rec_host_pinned) {
+            cudaGetLastError();
+            ws.rec_host = malloc(col_bytes);
+        }
+        if (!ws.rec_host) return "out of host memory for the records";
+        ws.rec_host_bytes = col_bytes;
+    }
+    if (col_bytes && (e = cudaMemcpyAsync(ws.rec_host, ws.rec_cols.p, col_bytes, cudaMemcpyDeviceToHost, st)))
+        return std::string("CUDA error: ") + cudaGetErrorString(e);
+    cudaMemcpyAsync(&bad, o.bad, 4, cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st))) return std::string("CUDA error: ") + cudaGetErrorString(e);
+    if (bad) return "the records could not be put in order";
+    d2h += col_bytes + 8 * kMaxStages + 8;
+    const double *cd = static_cast<const double *>(ws.rec_host);
+    const int *ci = reinterpret_cast<const int *>(cd + 6 * total);
+    col.x = cd;
+    col.y = cd + total;
+    col.z = cd + 2 * total;
+    col.cx = cd + 3 * total;
+    col.cy = cd + 4 * total;
+    col.cz = cd + 5 * total;
+    col.element = ci;
+    col.stage = ci + total;
+    col.raynum = ci + 2 * total;
+    col.n = size_t(total);
+    return "";
 }
 
 #define CK(x)                                                                                 \
@@ -333,9 +539,18 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     CK(cudaStreamSynchronize(st));
     out.setup_ms = ms_since(t_setup);
 
+    // room for `need` records in the run's record buffer, keeping the first `keep`
+    auto rec_room = [&](unsigned long long need, unsigned long long keep) -> cudaError_t {
+        if (need <= rec_cap) return cudaSuccess;
+        const unsigned long long cap = std::max(need, rec_cap + rec_cap / 2);
+        cudaError_t e = d_recs.grow_keep(cap * sizeof(RecordDev), keep * sizeof(RecordDev), st);
+        if (e == cudaSuccess) rec_cap = cap;
+        return e;
+    };
+    double rec_per_ray = 2.0 * nst;  // records per numbered ray expected when sizing the buffer
     for (int attempt = 0; attempt < 4; ++attempt) {
         bool restart = false;
-        out.records.clear();
+        out.rec = RecordColumns{};
         out.stage_entries.assign(nst, 0);
         out.max_enter.assign(nst, 0);
         out.max_ttmiss.assign(nst, 0);
@@ -345,6 +560,20 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
         CK(d_ctr.ensure(sizeof(RunCounters)));
         CK(d_rs.ensure(sizeof(RunState)));
         CK(d_rec_count.ensure(8));
+        // the run's records accumulate on the device over its batches and are put in order at
+        // the end; a replay's saved stage-1 records come first
+        const unsigned long long n_pre = rq.pre_records.size();
+        unsigned long long nrec_run = 0;  // records written so far (read after every batch)
+        if (rq.records) {
+            CK(d_recs.ensure(std::max<unsigned long long>(rec_cap, n_pre + 4096) * sizeof(RecordDev)));
+            rec_cap = d_recs.bytes / sizeof(RecordDev);
+            if (n_pre)
+                CK(cudaMemcpyAsync(d_recs.p, rq.pre_records.data(), n_pre * sizeof(RecordDev),
+                                   cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(d_rec_count.p, &n_pre, 8, cudaMemcpyHostToDevice, st));
+            out.h2d_bytes += n_pre * sizeof(RecordDev) + 8;
+            nrec_run = n_pre;
+        }
         CK(cudaMemsetAsync(d_acc.p, 0, std::max<size_t>(acc_n, 1) * 8, st));
         CK(cudaMemsetAsync(d_ctr.p, 0, sizeof(RunCounters), st));
         RunState rs0;
@@ -447,11 +676,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             const uint64_t n1 = rq.replay_rows.size() / 7;
             CK(upload(ws.replay_rows, rq.replay_rows, st, out.h2d_bytes));
             CK(upload(ws.replay_fe0, rq.replay_fe0, st, out.h2d_bytes));
-            if (rq.records) {
-                if (rec_cap == 0) rec_cap = std::max<uint64_t>(n1, 1) * uint64_t(nst) * 2 + 4096;
-                CK(d_recs.ensure(rec_cap * sizeof(RecordDev)));
-                CK(cudaMemsetAsync(d_rec_count.p, 0, 8, st));
-            }
+            if (rq.records) CK(rec_room(nrec_run + std::max<uint64_t>(n1, 1) * uint64_t(nst) * 2 + 4096, nrec_run));
             O.recs = rq.records ? d_recs.as<RecordDev>() : nullptr;
             O.rec_cap = rq.records ? rec_cap : 0;
             WfState W;
@@ -484,11 +709,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             bool save_over = false;
             CK(save_collect(save_over));
             if (save_over) continue;
-            if (nrec) {
-                out.records.resize(nrec);
-                out.d2h_bytes += nrec * sizeof(RecordDev);
-                CK(cudaMemcpy(out.records.data(), d_recs.p, nrec * sizeof(RecordDev), cudaMemcpyDeviceToHost));
-            }
+            nrec_run = nrec;
             rs.hits_done = rs.sun_rays = rq.replay_sun_rays;
             rs.reached = 1;
             done = true;
@@ -536,9 +757,11 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 CK(d_s_el.ensure(n * 4));
                 CK(d_s_idx.ensure(n * 4));
                 if (rq.records) {
-                    if (rec_cap == 0) rec_cap = std::min<uint64_t>(n, uint64_t(1) << 22) * uint64_t(nst) * 2 + 4096;
-                    CK(d_recs.ensure(rec_cap * sizeof(RecordDev)));
-                    CK(cudaMemsetAsync(d_rec_count.p, 0, 8, st));
+                    // room for this batch's records: its numbered rays at the records per ray seen so far
+                    const uint64_t numbered = multi ? global_done : rs.hits_done;
+                    const uint64_t left = explicit_mode ? n : rq.n_hits - std::min<uint64_t>(rq.n_hits, numbered);
+                    const double est = double(std::min<uint64_t>(n, left)) * rec_per_ray;
+                    CK(rec_room(nrec_run + uint64_t(est) + 4096, nrec_run));
                 }
                 O.recs = rq.records ? d_recs.as<RecordDev>() : nullptr;
                 O.rec_cap = rq.records ? rec_cap : 0;
@@ -623,6 +846,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                     unsigned long long nrec = 0;
                     if (rq.records) CK(cudaMemcpyAsync(&nrec, d_rec_count.p, 8, cudaMemcpyDeviceToHost, st));
                     CK(cudaStreamSynchronize(st));
+                    const unsigned long long nrec_local = nrec;
                     bool overflow = rq.records && nrec > rec_cap;
                     if (multi) {  // a rank out of record room makes every rank re-run, in step
                         std::vector<unsigned long long> got;
@@ -647,15 +871,11 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                         restart = true;
                         break;
                     }
-                    if (nrec) {
-                        const auto tr = std::chrono::steady_clock::now();
-                        const size_t old = out.records.size();
-                        out.records.resize(old + nrec);
-                        out.d2h_bytes += nrec * sizeof(RecordDev);
-                        CK(cudaMemcpyAsync(out.records.data() + old, d_recs.p, nrec * sizeof(RecordDev),
-                                           cudaMemcpyDeviceToHost, st));
-                        CK(cudaStreamSynchronize(st));
-                        out.readback_ms += ms_since(tr);
+                    if (rq.records) {
+                        nrec_run = nrec_local;
+                        out.d2h_bytes += 8;
+                        if (!multi && rs.hits_done > 0)
+                            rec_per_ray = std::max(1.0, 1.5 * double(nrec_run - n_pre) / double(rs.hits_done));
                     }
                     if (rq.callback &&
                         !rq.callback((unsigned long)rs.sun_rays, (unsigned long)rs.hits_done,
@@ -763,6 +983,30 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
         if (out.flags & kFlagBadInteraction) {
             out.error = "Bad optical interaction type (only 1 = refraction and 2 = reflection are traced)";
             return false;
+        }
+        if (rq.records) {
+            // the records the reference writes, in its order: the ray that alone left the first
+            // stage as the last numbered one is not traced further (raytrace.cpp:786-797); the
+            // last ray of a trace-through stage that misses leaves no record (810-811)
+            const auto to = std::chrono::steady_clock::now();
+            const uint32_t N = uint32_t(out.ray_hits);
+            const bool drop_later = !rq.replay && nst > 1 && out.stage_entries[1] == 1 && out.max_enter[1] == N;
+            uint32_t tt_drop[kMaxStages] = {0};
+            uint32_t rb = N;
+            for (int s = 0; s < nst; ++s) {
+                rb = std::max(rb, out.max_enter[size_t(s)]);
+                if (s >= 1 && S.stages[s].tracethrough && out.max_ttmiss[size_t(s)] != 0 &&
+                    out.max_ttmiss[size_t(s)] == out.max_enter[size_t(s)])
+                    tt_drop[s] = out.max_enter[size_t(s)];
+            }
+            for (const RecordDev &r : rq.pre_records) rb = std::max(rb, r.raynum);
+            const std::string err = order_records(ws, d_recs.as<RecordDev>(), std::min(nrec_run, rec_cap), nst,
+                                                  drop_later, tt_drop, rb, out.rec, out.d2h_bytes, st);
+            if (!err.empty()) {
+                out.error = err;
+                return false;
+            }
+            out.readback_ms += ms_since(to);
         }
         out.ok = true;
         return true;
