@@ -1087,9 +1087,13 @@ bool sun_setup(Context *cx, HostScene &hs) {
     // sun-plane grid over the first stage: every element whose bounding disc (centre
     // = projected origin, radius = accept radius) overlaps a cell is listed there
     sd.grid_on = 0;
+    sd.exact_flat = 0;
     hs.cell_start.assign(2, 0);
     hs.cell_disc.clear();
     hs.cell_par.clear();
+    hs.cell_xa.clear();
+    hs.cell_xb.clear();
+    hs.cell_xc.clear();
     if (!sun.point_source && st.elems.size() >= 4) {
         bool bounded = true;
         double rmax = 0;
@@ -1189,24 +1193,75 @@ bool sun_setup(Context *cx, HostScene &hs) {
                 memcpy(&w, &bits, 4);
                 disc[j] = float4{float(ccx), float(ccy), float(fr), w};
             }
+            // Exact footprints for first stages of flat rectangles (the mixed-precision probe
+            // decides hit and nearest element in float and defers to double within its
+            // rounding margins): a sun-frame ray (x, y) meets the plane of element j at depth
+            // z0 + gx qx + gy qy, q = (x, y) - centre, inside the rectangle when
+            // |i00 qx + i01 qy| <= 1 and |i10 qx + i11 qy| <= 1 (the rectangle's half-axes
+            // projected along the sun's z, inverted).  Coordinates are taken relative to the
+            // lower corner of the entry's cell, so that floats hold them to ~1e-6 m.
+            bool exact = true;
+            for (const Elem &e : st.elems)
+                if (e.stype != 3 || char(tolower(e.shape)) != 'r') exact = false;
+            std::vector<float4> xb(exact ? st.elems.size() : 0), xc(exact ? st.elems.size() : 0);
+            std::vector<double> ecx(exact ? st.elems.size() : 0), ecy(exact ? st.elems.size() : 0);
+            if (exact) {
+                for (size_t j = 0; j < st.elems.size(); ++j) {
+                    const Elem &e = st.elems[j];
+                    double c2[3], a2[3], b2[3], n2[3], ax3[3], ay3[3], nz3[3];
+                    for (int q = 0; q < 3; ++q) {
+                        ax3[q] = e.p[0] / 2.0 * e.R[q];
+                        ay3[q] = e.p[1] / 2.0 * e.R[3 + q];
+                        nz3[q] = e.R[6 + q];
+                    }
+                    mulv(Rs, e.origin, c2);
+                    mulv(Rs, ax3, a2);
+                    mulv(Rs, ay3, b2);
+                    mulv(Rs, nz3, n2);
+                    const double det = a2[0] * b2[1] - a2[1] * b2[0];
+                    const double la = sqrt(sq(a2[0]) + sq(a2[1])), lb = sqrt(sq(b2[0]) + sq(b2[1]));
+                    ecx[j] = c2[0];
+                    ecy[j] = c2[1];
+                    xb[j] = float4{0.f, 0.f, 0.f, 0.f};
+                    if (!e.enabled || !(0.0 <= e.zap)) {
+                        xc[j] = float4{0.f, 0.f, INFINITY, 0.f};  // never accepted (element_test_flat)
+                    } else if (!(fabs(det) > 1e-3 * la * lb) || !(fabs(n2[2]) > 1e-3)) {
+                        xc[j] = float4{0.f, 0.f, NAN, 0.f};  // near edge-on: always decided in double
+                    } else {
+                        xb[j] = float4{float(b2[1] / det), float(-b2[0] / det), float(-a2[1] / det),
+                                       float(a2[0] / det)};
+                        xc[j] = float4{float(-n2[0] / n2[2]), float(-n2[1] / n2[2]), float(c2[2]), 0.f};
+                    }
+                }
+            }
             // (start, end) pair per cell: cell c at [2c, 2c + 1], read on the device as one int2
             hs.cell_start.assign(2 * size_t(nx) * ny, 0);
             int at = 0;
             for (size_t c = 0; c < cells.size(); ++c) {
                 hs.cell_start[2 * c] = at;
+                const int gxc = int(c % size_t(nx)), gyc = int(c / size_t(nx));
+                const double x0c = sun.xmin + gxc * cell, y0c = sun.ymin + gyc * cell;
                 for (int j : cells[c]) {
                     hs.cell_disc.push_back(disc[j]);
                     hs.cell_par.push_back(par[j]);
+                    if (exact) {
+                        const float r = disc[j].z;
+                        hs.cell_xa.push_back(float4{float(ecx[j] - x0c), float(ecy[j] - y0c), r * r, disc[j].w});
+                        hs.cell_xb.push_back(xb[j]);
+                        hs.cell_xc.push_back(xc[j]);
+                    }
                 }
                 at += int(cells[c].size());
                 hs.cell_start[2 * c + 1] = at;
             }
+            sd.exact_flat = exact ? 1 : 0;
             sd.grid_on = 1;
             sd.gnx = nx;
             sd.gny = ny;
             sd.gx0 = sun.xmin;
             sd.gy0 = sun.ymin;
             sd.ginv = 1.0 / cell;
+            sd.gcell = cell;
         }
     }
     return true;
@@ -1681,6 +1736,9 @@ bool build_position(const Context *cx, const HostScene &hs, const double sun_xyz
     out.cell_start.swap(h.cell_start);
     out.cell_disc.swap(h.cell_disc);
     out.cell_par.swap(h.cell_par);
+    out.cell_xa.swap(h.cell_xa);
+    out.cell_xb.swap(h.cell_xb);
+    out.cell_xc.swap(h.cell_xc);
     if (target) {
         out.elems = hs.elems;
         const StageRec &sr = hs.dev.stages[0];

@@ -28,6 +28,7 @@ struct HostScene {
     std::vector<float4> elem_sphere;  // per element: origin (stage coordinates), padded bounding radius
     std::vector<float4> cell_disc;  // sun-plane grid entries: disc centre x, y, radius, element
     std::vector<float4> cell_par;   // sun-plane grid entries: footprint parallelogram (dual basis rows)
+    std::vector<float4> cell_xa, cell_xb, cell_xc;  // sun-plane grid entries: exact flat footprints (SunDev)
     std::vector<double> inv_cdf;  // table-sunshape inverse CDF (kSunInvCells + 1 entries)
     SceneDev dev;  // stages, sun scalars and flags; device pointers are filled by gpu_run
 };
@@ -98,7 +99,7 @@ struct RunResult {
 struct SunPosition {
     SunDev sun;                       // device pointers are filled by gpu_run_batch
     std::vector<int> cell_start;
-    std::vector<float4> cell_disc, cell_par;
+    std::vector<float4> cell_disc, cell_par, cell_xa, cell_xb, cell_xc;
     std::vector<ElemRec> elems;       // empty: the scene's elements
     uint64_t n_hits = 0;
     uint32_t seed = 0;

@@ -23,6 +23,16 @@ int launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, const ProbeOu
                        cudaStream_t st) {
     const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;
     if (S.sun.grid_on && !S.explicit_rays && !S.sun.point_source) {
+        if (S.sun.exact_flat && S.stages[0].flat_only && o.amb) {  // flat rectangles: float probe
+            cudaMemsetAsync(o.cand_count, 0, sizeof(uint32_t), st);
+            cudaMemsetAsync(o.amb_count, 0, sizeof(uint32_t), st);
+            k_sun_probe_exact<1><<<(n + kCandRays - 1) / kCandRays, kProbeBlock, 0, st>>>(S, s0, n, o, rs);
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            k_sun_resolve_amb<1><<<sms, kResolveBlock, 0, st>>>(S, s0, o);
+            return 2;
+        }
         launch_sun_candidates(S, s0, n, o, rs, st);
         // first stages of flat elements only (heliostat fields) take the flat-only variant
         const bool flat = S.stages[0].flat_only != 0;

@@ -34,6 +34,10 @@ constexpr int kWfFlatSearchMinBlocks = 5;  // search kernels of flat-only stages
 constexpr int kWfFirstFlatMinBlocks = 8;   // first kernel on a flat-only first stage
 
 constexpr int kWfClosedShadeMinBlocks = 4; // shade kernel of scenes with closed-form surfaces only
+#ifndef ST_EXACT_PROBE_MINB
+#define ST_EXACT_PROBE_MINB 8
+#endif
+constexpr int kExactProbeMinBlocks = ST_EXACT_PROBE_MINB;  // mixed probe of flat rectangles (k_sun_probe_exact)
 
 enum RunFlags : unsigned {
     kFlagHitCap = 1u,         // a ray reached kMaxHitsPerStage in one stage
@@ -120,12 +124,14 @@ struct ReplayIn {
 //   cand, cand_count  the probe's ray list (room for n entries) and its length: the grid
 //                 probe's candidates, or (with cand_el) every ray of the other probes;
 //   cand_el       optional: element + 1 or 0 per list entry;
-//   hit_mask      optional: one bit per ray, set for a hit (hit_mask_words(n) words).
+//   hit_mask      optional: one bit per ray, set for a hit (hit_mask_words(n) words);
+//   amb, amb_count  room for n ray indices and their count (k_sun_probe_exact only).
 struct ProbeOut {
     uint32_t *block_counts;
     uint32_t *hit_elem;
     uint32_t *cand, *cand_count, *cand_el;
     uint32_t *hit_mask;
+    uint32_t *amb, *amb_count;  // mixed probe of flat rectangles: rays left to the double search
 };
 constexpr size_t hit_mask_words(uint64_t n) { return size_t((n + kCandRays - 1) / kCandRays) * (kCandRays / 32); }
 

@@ -170,6 +170,7 @@ extern "C" int st_b200_probe_noalloc(st_context_t pcxt, unsigned int seed, unsig
     S.sun.cell_start = d_cells;
     S.sun.cell_disc = d_cdisc;
     S.sun.cell_par = d_cpar;
+    S.sun.exact_flat = 0;  // FP64 probe: the exact flat footprints are not carved out
     S.sun.inv_cdf = nullptr;
     S.optics = nullptr;
     S.tables = nullptr;

@@ -88,6 +88,7 @@ struct Workspace {
     DevBuf cand;      // probe's ray list: count, then one sun-ray index per entry
     DevBuf cand_el;   // probe's result per list entry (element + 1, 0 for a miss)
     DevBuf hit_mask;  // one bit per sun ray of the batch, set for a hit
+    DevBuf amb;       // mixed probe: count, then the rays left to the double-precision search
     // trace state and queues (one slot per hit-list entry of a batch)
     DevBuf wf_sid, wf_raynum, wf_draw, wf_meta, wf_fe0, wf_p, wf_c, wf_q0, wf_q1, wf_qs, wf_counts;
     DevBuf save_rows[2], save_count, replay_rows, replay_fe0;  // stage-data save / replay
@@ -98,7 +99,8 @@ struct Workspace {
     size_t rec_host_bytes = 0;
     bool rec_host_pinned = false;
     // batched runs: per-position sun tables, element copies, run states, counters, accumulators
-    DevBuf pos_cells, pos_disc, pos_par, pos_elems, pos_rs, pos_ctr, pos_acc;
+    DevBuf pos_cells, pos_disc, pos_par, pos_xa, pos_xb, pos_xc, pos_elems, pos_rs, pos_ctr, pos_acc;
+    DevBuf cell_xa, cell_xb, cell_xc;  // exact flat footprints of the sun-plane grid
     std::vector<cudaEvent_t> events;
     // autotuned kernel variants per precision (FP64, mixed), chosen on the first run
     struct Tuning {
@@ -134,9 +136,11 @@ static cudaError_t probe_buffers(Workspace &ws, uint64_t n, ProbeOut &o) {
     const size_t nb = size_t((n + kProbeBlock - 1) / kProbeBlock);
     cudaError_t e;
     if ((e = ws.counts.ensure(nb * 4)) || (e = ws.cand.ensure((n + 1) * 4)) || (e = ws.cand_el.ensure(n * 4)) ||
-        (e = ws.hit_mask.ensure(hit_mask_words(n) * 4)))
+        (e = ws.hit_mask.ensure(hit_mask_words(n) * 4)) || (e = ws.amb.ensure((n + 1) * 4)))
         return e;
     o = ProbeOut{};
+    o.amb_count = ws.amb.as<uint32_t>();
+    o.amb = o.amb_count + 1;
     o.block_counts = ws.counts.as<uint32_t>();
     o.cand_count = ws.cand.as<uint32_t>();
     o.cand = o.cand_count + 1;
@@ -454,6 +458,9 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     CK(upload(d_cell_start, hs.cell_start, st, out.h2d_bytes));
     CK(upload(d_cell_disc, hs.cell_disc, st, out.h2d_bytes));
     CK(upload(ws.cell_par, hs.cell_par, st, out.h2d_bytes));
+    CK(upload(ws.cell_xa, hs.cell_xa, st, out.h2d_bytes));
+    CK(upload(ws.cell_xb, hs.cell_xb, st, out.h2d_bytes));
+    CK(upload(ws.cell_xc, hs.cell_xc, st, out.h2d_bytes));
     CK(upload(d_inv_cdf, hs.inv_cdf, st, out.h2d_bytes));
     CK(upload(d_expos, rq.ex_pos, st, out.h2d_bytes));
     CK(upload(d_excos, rq.ex_cos, st, out.h2d_bytes));
@@ -475,6 +482,10 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     S.sun.cell_start = d_cell_start.as<int>();
     S.sun.cell_disc = d_cell_disc.as<float4>();
     S.sun.cell_par = ws.cell_par.as<float4>();
+    S.sun.cell_xa = ws.cell_xa.as<float4>();
+    S.sun.cell_xb = ws.cell_xb.as<float4>();
+    S.sun.cell_xc = ws.cell_xc.as<float4>();
+    if (hs.cell_xa.size() != hs.cell_disc.size() || hs.cell_xa.empty()) S.sun.exact_flat = 0;
     S.sun.inv_cdf = hs.inv_cdf.empty() ? nullptr : d_inv_cdf.as<double>();
     S.seed = rq.seed;
     S.precision = rq.precision;
@@ -1072,9 +1083,12 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
     CK(upload(ws.inv_cdf, hs.inv_cdf, st, h2d));
     // every position's tables, concatenated
     std::vector<int> cells;
-    std::vector<float4> disc, par;
+    std::vector<float4> disc, par, xa, xb, xc;
     std::vector<ElemRec> pelems;
     std::vector<size_t> off_cells(K), off_disc(K), off_elems(K);
+    bool all_exact = true;
+    for (const SunPosition &sp : pos)
+        if (!sp.sun.exact_flat || sp.cell_xa.size() != sp.cell_disc.size() || sp.cell_xa.empty()) all_exact = false;
     for (size_t p = 0; p < K; ++p) {
         const SunPosition &sp = pos[p];
         off_cells[p] = cells.size();
@@ -1082,12 +1096,20 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
         off_disc[p] = disc.size();
         disc.insert(disc.end(), sp.cell_disc.begin(), sp.cell_disc.end());
         par.insert(par.end(), sp.cell_par.begin(), sp.cell_par.end());
+        if (all_exact) {
+            xa.insert(xa.end(), sp.cell_xa.begin(), sp.cell_xa.end());
+            xb.insert(xb.end(), sp.cell_xb.begin(), sp.cell_xb.end());
+            xc.insert(xc.end(), sp.cell_xc.begin(), sp.cell_xc.end());
+        }
         off_elems[p] = sp.elems.empty() ? size_t(-1) : pelems.size();
         pelems.insert(pelems.end(), sp.elems.begin(), sp.elems.end());
     }
     CK(upload(ws.pos_cells, cells, st, h2d));
     CK(upload(ws.pos_disc, disc, st, h2d));
     CK(upload(ws.pos_par, par, st, h2d));
+    CK(upload(ws.pos_xa, xa, st, h2d));
+    CK(upload(ws.pos_xb, xb, st, h2d));
+    CK(upload(ws.pos_xc, xc, st, h2d));
     CK(upload(ws.pos_elems, pelems, st, h2d));
 
     SceneDev S0 = hs.dev;
@@ -1144,6 +1166,10 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
         S.sun.cell_start = ws.pos_cells.as<int>() + off_cells[p];
         S.sun.cell_disc = ws.pos_disc.as<float4>() + off_disc[p];
         S.sun.cell_par = ws.pos_par.as<float4>() + off_disc[p];
+        S.sun.exact_flat = all_exact ? 1 : 0;
+        S.sun.cell_xa = all_exact ? ws.pos_xa.as<float4>() + off_disc[p] : nullptr;
+        S.sun.cell_xb = all_exact ? ws.pos_xb.as<float4>() + off_disc[p] : nullptr;
+        S.sun.cell_xc = all_exact ? ws.pos_xc.as<float4>() + off_disc[p] : nullptr;
         S.sun.inv_cdf = hs.inv_cdf.empty() ? nullptr : ws.inv_cdf.as<double>();
         if (off_elems[p] != size_t(-1)) S.elems = ws.pos_elems.as<ElemRec>() + off_elems[p];
         S.seed = pos[p].seed;

@@ -128,6 +128,16 @@ struct SunDev {
     const float4 *cell_par;         // per cell entry: rows (a, b), (c, d) of the footprint's
                                     // dual basis; (x, y) about the centre is kept when
                                     // |a x + b y| <= 1 and |c x + d y| <= 1 (all zero: disc only)
+    double gcell;                   // cell size (1 / ginv)
+    // first stages of flat rectangles only (exact_flat), per cell entry: the footprint centre
+    // relative to the cell's lower corner, the padded disc radius squared and the element
+    // (xa); the exact footprint's dual basis rows, unpadded (xb); the depth slopes along the
+    // sun's z and the depth at the centre (xc; z +inf: the element accepts no hit, NaN: no
+    // exact footprint, the float test defers to double)
+    int exact_flat;
+    const float4 *cell_xa;          // centre x, y (cell-relative), r^2, element (int bits)
+    const float4 *cell_xb;          // i00, i01, i10, i11
+    const float4 *cell_xc;          // dz/dx, dz/dy, z at the centre, unused
 };
 
 struct SceneDev {

@@ -663,6 +663,164 @@ __global__ void __launch_bounds__(kResolveBlock, MINB) k_sun_resolve(const __gri
     }
 }
 
+// Mixed-precision probe of sun rays on a first stage of flat rectangles (SunDev::exact_flat)
+// in one kernel.  Each grid entry whose padded disc holds the sun-plane point is tested
+// against the element's exact footprint and plane in float: inside the rectangle when
+// |u|, |v| <= 1 for (u, v) the point in the projected half-axes' basis, at depth
+// z0 + gx qx + gy qy along the sun's z (the nearest accepted element wins, as the path
+// lengths of raytrace.cpp:745 order them).  A point within the float rounding margins of a
+// footprint edge, an entry without an exact footprint, or two accepted elements within
+// rounding of one depth leave the ray undecided: it goes to a list that k_sun_resolve_amb
+// searches in double, so the element found is the FP64 probe's.  Output as k_sun_resolve
+// leaves it: hitting rays listed with their element, one hit-mask bit per ray, hits per
+// kProbeBlock rays.  kCandPerThread sun rays per thread at kProbeBlock apart, kCandRays per
+// block.
+template <int MIXED>
+__global__ void __launch_bounds__(kProbeBlock, kExactProbeMinBlocks) k_sun_probe_exact(const __grid_constant__ SceneDev S, uint64_t s0,
+                                                                  uint32_t n, ProbeOut o, const RunState *rs) {
+    const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (rs->reached) {  // the requested hits are numbered: this batch is surplus
+        if (threadIdx.x < kCandPerThread && blockIdx.x * kCandPerThread + threadIdx.x < nb)
+            o.block_counts[blockIdx.x * kCandPerThread + threadIdx.x] = 0;
+        if (o.hit_mask && threadIdx.x < kCandRays / 32) o.hit_mask[blockIdx.x * (kCandRays / 32) + threadIdx.x] = 0;
+        return;
+    }
+    const SunDev &sun = S.sun;
+    // per ray of the block its result, per warp and ray group the hit ballot
+    constexpr uint32_t kUndecided = 0xffffffffu;
+    __shared__ uint32_t hsh[kCandPerThread][kProbeBlock];
+    __shared__ unsigned wb[kCandPerThread][kProbeBlock / 32];
+    __shared__ uint32_t wn[kProbeBlock / 32], base;
+    // pass 1, float only: element + 1, 0 for a miss, kUndecided for the double-precision search
+#pragma unroll 1
+    for (int m = 0; m < kCandPerThread; ++m) {
+        const uint32_t i = blockIdx.x * kCandRays + m * kProbeBlock + threadIdx.x;
+        uint32_t h = 0;
+        if (i < n) {
+            RayRng rng;
+            rng.init(S.seed, s0 + i, 0);
+            const double xs = sun.xmin + (sun.xmax - sun.xmin) * rng.u();
+            const double ys = sun.ymin + (sun.ymax - sun.ymin) * rng.u();
+            int cx = int(floor((xs - sun.gx0) * sun.ginv)), cy = int(floor((ys - sun.gy0) * sun.ginv));
+            cx = min(max(cx, 0), sun.gnx - 1);
+            cy = min(max(cy, 0), sun.gny - 1);
+            const int2 range = reinterpret_cast<const int2 *>(sun.cell_start)[cy * sun.gnx + cx];
+            // the point relative to the cell's lower corner (entries hold their centres so)
+            const float xr = float(xs - (sun.gx0 + cx * sun.gcell)), yr = float(ys - (sun.gy0 + cy * sun.gcell));
+            int best = -1;
+            float bz = INFINITY;
+            for (int k = range.x; k < range.y; ++k) {
+                const float4 a = sun.cell_xa[k];
+                const float qx = xr - a.x, qy = yr - a.y;
+                if (qx * qx + qy * qy > a.z) continue;  // outside the padded disc
+                const float4 c = sun.cell_xc[k];
+                if (isnan(c.z)) {  // no exact footprint
+                    best = -2;
+                    break;
+                }
+                if (c.z == INFINITY) continue;  // an element that accepts no hit
+                const float4 e0 = sun.cell_xb[k];
+                const float u1 = e0.x * qx, u2 = e0.y * qy, v1 = e0.z * qx, v2 = e0.w * qy;
+                const float au = fabsf(u1 + u2), av = fabsf(v1 + v2);
+                const float mu = 2e-6f * (fabsf(u1) + fabsf(u2)) + 1e-6f;
+                const float mv = 2e-6f * (fabsf(v1) + fabsf(v2)) + 1e-6f;
+                if (au > 1.f + mu || av > 1.f + mv) continue;  // surely outside
+                if (au >= 1.f - mu || av >= 1.f - mv) {         // within rounding of an edge
+                    best = -2;
+                    break;
+                }
+                const float g1 = c.x * qx, g2 = c.y * qy;
+                const float z = c.z + g1 + g2;
+                const float tol = 1e-6f * (fabsf(c.z) + fabsf(g1) + fabsf(g2)) + 1e-5f;
+                if (fabsf(z - bz) <= tol) {  // two elements within rounding of one depth
+                    best = -2;
+                    break;
+                }
+                if (z < bz) {
+                    bz = z;
+                    best = __float_as_int(a.w);
+                }
+            }
+            h = best == -2 ? kUndecided : uint32_t(best + 1);
+        }
+        hsh[m][threadIdx.x] = h;
+    }
+    // pass 2: undecided rays (a few per million) to the double-precision list; ballots, mask
+    uint32_t mine = 0;
+#pragma unroll 1
+    for (int m = 0; m < kCandPerThread; ++m) {
+        const uint32_t i = blockIdx.x * kCandRays + m * kProbeBlock + threadIdx.x;
+        uint32_t h = hsh[m][threadIdx.x];
+        if (h == kUndecided) {
+            o.amb[atomicAdd(o.amb_count, 1u)] = i;
+            h = 0;
+            hsh[m][threadIdx.x] = 0;
+        }
+        if (o.hit_elem && i < n) o.hit_elem[i] = h;
+        const unsigned bal = __ballot_sync(0xffffffffu, h != 0);
+        if (lane == 0) {
+            if (o.hit_mask) o.hit_mask[(blockIdx.x * kCandRays + m * kProbeBlock) / 32 + w] = bal;
+            wb[m][w] = bal;
+        }
+        mine += __popc(bal);
+    }
+    // one reservation in the list per block: warp counts, their prefix, one atomic
+    if (lane == 0) wn[w] = mine;
+    __syncthreads();
+    if (threadIdx.x < kCandPerThread && blockIdx.x * kCandPerThread + threadIdx.x < nb) {
+        uint32_t c = 0;
+        for (int k = 0; k < kProbeBlock / 32; ++k) c += __popc(wb[threadIdx.x][k]);
+        o.block_counts[blockIdx.x * kCandPerThread + threadIdx.x] = c;
+    }
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int k = 0; k < kProbeBlock / 32; ++k) {
+            const uint32_t x = wn[k];
+            wn[k] = t;
+            t += x;
+        }
+        base = t ? atomicAdd(o.cand_count, t) : 0u;
+    }
+    __syncthreads();
+    uint32_t at = base + wn[w];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int m = 0; m < kCandPerThread; ++m) {
+        const unsigned bal = wb[m][w];
+        if ((bal >> lane) & 1u) {
+            const uint32_t pos = at + __popc(bal & lt);
+            o.cand[pos] = blockIdx.x * kCandRays + m * kProbeBlock + threadIdx.x;
+            if (o.cand_el) o.cand_el[pos] = hsh[m][threadIdx.x];
+        }
+        at += __popc(bal);
+    }
+}
+
+// The rays k_sun_probe_exact left undecided, searched in double (the FP64 probe's arithmetic):
+// a hit is appended to the probe's list and counted in its block count and hit mask.
+template <int MIXED>
+__global__ void __launch_bounds__(kResolveBlock) k_sun_resolve_amb(const __grid_constant__ SceneDev S, uint64_t s0,
+                                                                   ProbeOut o) {
+    const uint32_t na = *o.amb_count;
+    const SunDev &sun = S.sun;
+    for (uint32_t c = blockIdx.x * kResolveBlock + threadIdx.x; c < na; c += gridDim.x * kResolveBlock) {
+        const uint32_t i = o.amb[c];
+        RayRng rng;
+        rng.init(S.seed, s0 + i, 0);
+        const double xs = sun.xmin + (sun.xmax - sun.xmin) * rng.u();
+        const double ys = sun.ymin + (sun.ymax - sun.ymin) * rng.u();
+        const int b = nearest_sun_grid_lazy<0, kEtFlat>(S, S.stages[0], xs, ys);
+        if (b < 0) continue;
+        const uint32_t h = uint32_t(b + 1);
+        if (o.hit_elem) o.hit_elem[i] = h;
+        const uint32_t pos = atomicAdd(o.cand_count, 1u);
+        o.cand[pos] = i;
+        if (o.cand_el) o.cand_el[pos] = h;
+        atomicAdd(&o.block_counts[i / kProbeBlock], 1u);
+        if (o.hit_mask) atomicOr(&o.hit_mask[i / 32], 1u << (i & 31));
+    }
+}
+
 #ifdef ST_COMMON_KERNELS
 // first kernel of the grid probe (above): candidates listed, hit-mask words cleared
 __global__ void __launch_bounds__(kProbeBlock) k_sun_candidates(const __grid_constant__ SceneDev S, uint64_t s0,

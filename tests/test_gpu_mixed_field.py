@@ -88,3 +88,28 @@ def test_philox_field_mixed_follows_oracle(product, oracle):
     assert len(sa) == len(sb) == hits
     same = sum(1 for r in sb if sa.get(r) == sb[r])
     assert same / hits >= 0.995, same / hits
+
+
+def test_mixed_probe_finds_the_fp64_elements(product):
+    """The mixed-precision probe of flat rectangles (float footprints and depths, rays within
+    rounding of an edge or a depth tie decided in double) numbers the same sun rays and finds
+    the same first-stage element for every ray as the FP64 probe."""
+    hits = 200_000
+    sc = scenes.field_scene(2000, hits, dynamic_group=False)
+    a = run_scene(product, sc, 21, lambda api, c: api.st_b200_set_precision(c, 1))
+    b = run_scene(product, sc, 21, lambda api, c: api.st_b200_set_precision(c, 0))
+    assert a[2]["nsunrays"] == b[2]["nsunrays"]
+
+    def first_elements(rec):
+        m = rec["stage"] == 1
+        rn, el = rec["raynum"][m], np.abs(rec["element"][m])
+        first = np.full(hits + 1, -1)
+        order = np.argsort(rn, kind="stable")
+        rn, el = rn[order], el[order]
+        keep = np.r_[True, rn[1:] != rn[:-1]]
+        first[rn[keep]] = el[keep]
+        return first
+
+    fa, fb = first_elements(a[1]), first_elements(b[1])
+    assert np.array_equal(fa, fb)
+    assert (fa[1:] > 0).all()
