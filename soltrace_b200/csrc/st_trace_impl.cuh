@@ -579,7 +579,12 @@ __device__ inline void bin_flux(const SceneDev &S, int si, int ej, bool absorbed
         }
         if (ix < 0 || ix >= f.nx || iy < 0 || iy >= f.ny) continue;
         const size_t src = f.n_src > 0 ? size_t(fe0) * size_t(f.nx) * size_t(f.ny) : 0;
-        atomicAdd(&f.bins[src + size_t(iy) * f.nx + ix], 1ull);
+        // one atomic per distinct bin among the warp's lanes here: a focusing optic sends most
+        // rays of a warp into a few bins, whose single-address atomics would serialise
+        unsigned long long *bin = &f.bins[src + size_t(iy) * f.nx + ix];
+        const unsigned active = __activemask();
+        const unsigned peers = __match_any_sync(active, reinterpret_cast<unsigned long long>(bin));
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(bin, (unsigned long long)__popc(peers));
     }
 }
 
