@@ -135,7 +135,7 @@ void launch_advance(const uint32_t *total, const uint64_t *hit_sid, uint64_t s0,
 }
 void launch_list_sort(uint64_t s0, const ProbeOut &o, const uint32_t *offsets, const uint32_t *total, RunState *rs,
                       uint32_t n_elem0, uint32_t *elem_count, uint32_t *elem_cursor, uint32_t *scratch_total,
-                      uint64_t *s_sid, uint32_t *s_el, uint32_t *s_idx, uint32_t max_n, cudaStream_t st) {
+                      HitRec *hits, uint32_t max_n, cudaStream_t st) {
     cudaMemsetAsync(elem_count, 0, size_t(n_elem0) * 4, st);
     if (n_elem0 <= uint32_t(kSortBins)) {
         int dev = 0, sms = 148;
@@ -144,13 +144,12 @@ void launch_list_sort(uint64_t s0, const ProbeOut &o, const uint32_t *offsets, c
         const uint32_t blocks = std::max(1u, std::min<uint32_t>((max_n + 4095) / 4096, uint32_t(2 * sms)));
         k_list_hist_sh<<<blocks, kSortBlock, 0, st>>>(o.cand_count, o.cand_el, n_elem0, elem_count);
         k_offsets<<<1, 1024, 0, st>>>(elem_count, n_elem0, elem_cursor, scratch_total);
-        k_list_scatter_sh<<<blocks, kSortBlock, 0, st>>>(s0, o, offsets, total, rs, n_elem0, elem_cursor, s_sid, s_el,
-                                                          s_idx);
+        k_list_scatter_sh<<<blocks, kSortBlock, 0, st>>>(s0, o, offsets, total, rs, n_elem0, elem_cursor, hits);
         return;
     }
     const uint32_t blocks = std::max(1u, std::min<uint32_t>((max_n + 255) / 256, 148u * 8u));
     k_list_hist<<<blocks, 256, 0, st>>>(o.cand_count, o.cand_el, elem_count);
     k_offsets<<<1, 1024, 0, st>>>(elem_count, n_elem0, elem_cursor, scratch_total);
-    k_list_scatter<<<blocks, 256, 0, st>>>(s0, o, offsets, total, rs, elem_cursor, s_sid, s_el, s_idx);
+    k_list_scatter<<<blocks, 256, 0, st>>>(s0, o, offsets, total, rs, elem_cursor, hits);
 }
 }  // namespace stb

@@ -50,11 +50,11 @@ int launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, const ProbeOu
     return 1;
 }
 
-int launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
-                      const uint32_t *hit_idx, const uint32_t *total, const RunState *rs, const TraceOut &O,
-                      const WfState &W, const WfQueues &Q, const ReplayIn *replay, cudaStream_t st) {
-    return records ? wf_launch<1, 1>(S, hit_sid, hit_el, hit_idx, total, rs, O, W, Q, replay, st)
-                   : wf_launch<1, 0>(S, hit_sid, hit_el, hit_idx, total, rs, O, W, Q, replay, st);
+int launch_trace_mixed(bool records, const SceneDev &S, const HitRec *hits, const uint32_t *total,
+                      const RunState *rs, const TraceOut &O, const WfState &W, const WfQueues &Q,
+                      const ReplayIn *replay, cudaStream_t st) {
+    return records ? wf_launch<1, 1>(S, hits, total, rs, O, W, Q, replay, st)
+                   : wf_launch<1, 0>(S, hits, total, rs, O, W, Q, replay, st);
 }
 // finite-element queries of this precision's kernels that found too few nodes since the
 // last call (the flag is cleared)

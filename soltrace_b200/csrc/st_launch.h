@@ -126,6 +126,14 @@ struct ReplayIn {
 //   cand_el       optional: element + 1 or 0 per list entry;
 //   hit_mask      optional: one bit per ray, set for a hit (hit_mask_words(n) words);
 //   amb, amb_count  room for n ray indices and their count (k_sun_probe_exact only).
+// One numbered hit of a batch, sorted by first-stage element: its sun-ray index, the element
+// and its rank among the batch's hits in sun-ray order (its ray number less the batch's base);
+// one 16-byte store per hit when the sort scatters it.
+struct __align__(16) HitRec {
+    unsigned long long sid;
+    uint32_t el, rank;
+};
+
 struct ProbeOut {
     uint32_t *block_counts;
     uint32_t *hit_elem;
@@ -144,25 +152,25 @@ int launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, const ProbeOu
 // first kernel of the grid probe (shared by both precisions)
 void launch_sun_candidates(const SceneDev &S, uint64_t s0, uint32_t n, const ProbeOut &o, const RunState *rs,
                            cudaStream_t st);
-// Trace of a batch's numbered rays (hit-list entries below the cut-off at the requested
-// hit count): the first kernel, `Q.rounds` rounds of search and shade kernels, and the
-// finishing kernel.  Returns the number of kernels launched.
+// Trace of a batch's numbered rays (sorted hits whose rank lies below the cut-off at the
+// requested hit count): the first kernel, `Q.rounds` rounds of search and shade kernels,
+// and the finishing kernel.  Returns the number of kernels launched.
 // With `replay` (non-null) the rays enter the second stage from saved rows instead of the
-// hit list (the hit-list arguments are then unused).
-int launch_trace_fp64(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
-                      const uint32_t *hit_idx, const uint32_t *total, const RunState *rs, const TraceOut &O,
+// hit list (hits and total are then unused).
+int launch_trace_fp64(bool records, const SceneDev &S, const HitRec *hits, const uint32_t *total,
+                      const RunState *rs, const TraceOut &O,
                       const WfState &W, const WfQueues &Q, const ReplayIn *replay, cudaStream_t st);
-int launch_trace_mixed(bool records, const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el,
-                       const uint32_t *hit_idx, const uint32_t *total, const RunState *rs, const TraceOut &O,
+int launch_trace_mixed(bool records, const SceneDev &S, const HitRec *hits, const uint32_t *total,
+                       const RunState *rs, const TraceOut &O,
                        const WfState &W, const WfQueues &Q, const ReplayIn *replay, cudaStream_t st);
 // The batch's hits, from the probe's list (cand, cand_el, hit_mask) and the exclusive
 // scan of its block counts (offsets, total), counting-sorted by first-stage element into
-// s_sid (sun-ray index), s_el (element) and s_idx (rank of the hit in sun-ray order); the
+// `hits` (sun-ray index, element, rank of the hit in sun-ray order); the
 // hit ranked last below the cut-off at the requested hit count leaves its sun-ray index in
 // rs->cut_sid.  max_n bounds the list length (grid sizing).
 void launch_list_sort(uint64_t s0, const ProbeOut &o, const uint32_t *offsets, const uint32_t *total, RunState *rs,
                       uint32_t n_elem0, uint32_t *elem_count, uint32_t *elem_cursor, uint32_t *scratch_total,
-                      uint64_t *s_sid, uint32_t *s_el, uint32_t *s_idx, uint32_t max_n, cudaStream_t st);
+                      HitRec *hits, uint32_t max_n, cudaStream_t st);
 // finite-element interpolation failures flagged by the kernels since the last call
 unsigned take_fe_failures_fp64();
 unsigned take_fe_failures_mixed();

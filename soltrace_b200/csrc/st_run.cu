@@ -92,7 +92,7 @@ struct Workspace {
     // trace state and queues (one slot per hit-list entry of a batch)
     DevBuf wf_sid, wf_raynum, wf_draw, wf_meta, wf_fe0, wf_p, wf_c, wf_q0, wf_q1, wf_qs, wf_counts;
     DevBuf save_rows[2], save_count, replay_rows, replay_fe0;  // stage-data save / replay
-    DevBuf ecount, ecursor, etotal, s_sid, s_el, s_idx;
+    DevBuf ecount, ecursor, etotal, s_hits;  // the batch's hits sorted by first-stage element (HitRec)
     // record ordering: key counts / slots, scan partials, per-stage counts, merge runs, columns
     DevBuf rec_key, rec_parts, rec_parts2, rec_stage, rec_runs, rec_cols, rec_bad;
     void *rec_host = nullptr;  // the ordered records' columns in host memory (pinned when possible)
@@ -536,8 +536,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
     // the batch's hits are grouped by first-stage element (the rays of a warp then leave
     // one element and walk the same candidates)
     const uint32_t n_elem0 = uint32_t(S.stages[0].n_elem);
-    DevBuf &d_ecount = ws.ecount, &d_ecursor = ws.ecursor, &d_etotal = ws.etotal, &d_s_sid = ws.s_sid,
-           &d_s_el = ws.s_el, &d_s_idx = ws.s_idx;
+    DevBuf &d_ecount = ws.ecount, &d_ecursor = ws.ecursor, &d_etotal = ws.etotal, &d_s_hits = ws.s_hits;
     CK(d_ecount.ensure(size_t(n_elem0) * 4));
     CK(d_ecursor.ensure(size_t(n_elem0) * 4));
     CK(d_etotal.ensure(8));
@@ -702,10 +701,10 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
             CK(cudaEventRecord(p1, st));
             if (rq.precision)
                 out.gpu_launches +=
-                    launch_trace_mixed(rq.records, S, nullptr, nullptr, nullptr, nullptr, drs, O, W, Q, &rin, st);
+                    launch_trace_mixed(rq.records, S, nullptr, nullptr, drs, O, W, Q, &rin, st);
             else
                 out.gpu_launches +=
-                    launch_trace_fp64(rq.records, S, nullptr, nullptr, nullptr, nullptr, drs, O, W, Q, &rin, st);
+                    launch_trace_fp64(rq.records, S, nullptr, nullptr, drs, O, W, Q, &rin, st);
             CK(cudaEventRecord(p2, st));
             CK(cudaGetLastError());
             trace_ev.push_back({p1, p2});
@@ -764,9 +763,7 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 CK(d_offsets.ensure(size_t(nb) * 4));
                 CK(ws.scan_parts.ensure(scan_parts(nb) * 4));
                 CK(d_total.ensure(8));
-                CK(d_s_sid.ensure(n * 8));
-                CK(d_s_el.ensure(n * 4));
-                CK(d_s_idx.ensure(n * 4));
+                CK(d_s_hits.ensure(std::max<uint64_t>(n, 1) * sizeof(HitRec)));
                 if (rq.records) {
                     // room for this batch's records: its numbered rays at the records per ray seen so far
                     const uint64_t numbered = multi ? global_done : rs.hits_done;
@@ -820,12 +817,11 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 if (n > 0) {
                     launch_list_sort(s0, po, d_offsets.as<uint32_t>(), d_total.as<uint32_t>(), drs, n_elem0,
                                      d_ecount.as<uint32_t>(), d_ecursor.as<uint32_t>(), d_etotal.as<uint32_t>(),
-                                     d_s_sid.as<uint64_t>(), d_s_el.as<uint32_t>(), d_s_idx.as<uint32_t>(),
+                                     d_s_hits.as<HitRec>(),
                                      uint32_t(n), st);
                     out.gpu_launches += 3;  // element counts, their scan, scatter
                 }
-                const uint64_t *t_sid = d_s_sid.as<uint64_t>();
-                const uint32_t *t_el = d_s_el.as<uint32_t>(), *t_idx = d_s_idx.as<uint32_t>();
+                const HitRec *t_hits = d_s_hits.as<HitRec>();
                 // trace state and queues: one slot per hit-list entry (at most n)
                 WfState W;
                 WfQueues Q;
@@ -834,10 +830,10 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
                 CK(cudaEventRecord(p1, st));
                 if (n > 0) {
                     if (rq.precision)
-                        out.gpu_launches += launch_trace_mixed(rq.records, S, t_sid, t_el, t_idx,
+                        out.gpu_launches += launch_trace_mixed(rq.records, S, t_hits,
                                                                d_total.as<uint32_t>(), drs, O, W, Q, nullptr, st);
                     else
-                        out.gpu_launches += launch_trace_fp64(rq.records, S, t_sid, t_el, t_idx,
+                        out.gpu_launches += launch_trace_fp64(rq.records, S, t_hits,
                                                               d_total.as<uint32_t>(), drs, O, W, Q, nullptr, st);
                 }
                 CK(cudaEventRecord(p2, st));
@@ -1218,9 +1214,7 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
         CK(ws.offsets.ensure(size_t(nb) * 4));
         CK(ws.scan_parts.ensure(scan_parts(nb) * 4));
         CK(ws.total.ensure(8));
-        CK(ws.s_sid.ensure(n * 8));
-        CK(ws.s_el.ensure(n * 4));
-        CK(ws.s_idx.ensure(n * 4));
+        CK(ws.s_hits.ensure(n * sizeof(HitRec)));
         CK(ws.ecount.ensure(size_t(std::max<uint32_t>(n_elem0, 1)) * 4));
         CK(ws.ecursor.ensure(size_t(std::max<uint32_t>(n_elem0, 1)) * 4));
         CK(ws.etotal.ensure(8));
@@ -1291,16 +1285,14 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
                             ws.scan_parts.as<uint32_t>(), st);
                 launch_list_sort(s0, po, ws.offsets.as<uint32_t>(), ws.total.as<uint32_t>(), drs + p, n_elem0,
                                  ws.ecount.as<uint32_t>(), ws.ecursor.as<uint32_t>(), ws.etotal.as<uint32_t>(),
-                                 ws.s_sid.as<uint64_t>(), ws.s_el.as<uint32_t>(), ws.s_idx.as<uint32_t>(),
+                                 ws.s_hits.as<HitRec>(),
                                  uint32_t(n), st);
                 CK(cudaEventRecord(p1, st));
                 if (rq.precision)
-                    out.gpu_launches += launch_trace_mixed(false, S, ws.s_sid.as<uint64_t>(), ws.s_el.as<uint32_t>(),
-                                                           ws.s_idx.as<uint32_t>(), ws.total.as<uint32_t>(), drs + p,
+                    out.gpu_launches += launch_trace_mixed(false, S, ws.s_hits.as<HitRec>(), ws.total.as<uint32_t>(), drs + p,
                                                            Op[p], W, Q, nullptr, st);
                 else
-                    out.gpu_launches += launch_trace_fp64(false, S, ws.s_sid.as<uint64_t>(), ws.s_el.as<uint32_t>(),
-                                                          ws.s_idx.as<uint32_t>(), ws.total.as<uint32_t>(), drs + p,
+                    out.gpu_launches += launch_trace_fp64(false, S, ws.s_hits.as<HitRec>(), ws.total.as<uint32_t>(), drs + p,
                                                           Op[p], W, Q, nullptr, st);
                 CK(cudaEventRecord(p2, st));
                 launch_advance(ws.total.as<uint32_t>(), nullptr, s0, uint32_t(n), drs + p, st);

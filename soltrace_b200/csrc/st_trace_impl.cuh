@@ -1055,13 +1055,15 @@ __device__ __forceinline__ uint32_t batch_take(const RunState *rs, const uint32_
     return uint32_t(n < left ? n : left);
 }
 
-// one sorted hit: sun-ray index, element, rank; the last numbered one marks the cut-off
+// one sorted hit: sun-ray index, element, rank (one 16-byte store); the last numbered one
+// marks the cut-off
 __device__ __forceinline__ void list_put(uint64_t s0, uint32_t ray, uint32_t e, uint32_t pos, uint32_t rank,
-                                         uint32_t take, RunState *rs, uint64_t *s_sid, uint32_t *s_el,
-                                         uint32_t *s_idx) {
-    s_sid[pos] = s0 + ray;
-    s_el[pos] = e;
-    s_idx[pos] = rank;
+                                         uint32_t take, RunState *rs, HitRec *hits) {
+    HitRec h;
+    h.sid = s0 + ray;
+    h.el = e;
+    h.rank = rank;
+    hits[pos] = h;
     if (rank + 1 == take) rs->cut_sid = s0 + ray;
 }
 
@@ -1075,7 +1077,7 @@ __global__ void __launch_bounds__(256) k_list_hist(const uint32_t *list_count, c
 }
 __global__ void __launch_bounds__(256) k_list_scatter(uint64_t s0, ProbeOut o, const uint32_t *offsets,
                                                       const uint32_t *total, RunState *rs, uint32_t *elem_cursor,
-                                                      uint64_t *s_sid, uint32_t *s_el, uint32_t *s_idx) {
+                                                      HitRec *hits) {
     const uint32_t n = *o.cand_count;
     const uint32_t take = batch_take(rs, total);
     for (uint32_t i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
@@ -1083,8 +1085,7 @@ __global__ void __launch_bounds__(256) k_list_scatter(uint64_t s0, ProbeOut o, c
         if (!h) continue;
         const uint32_t pos = atomicAdd(&elem_cursor[h - 1], 1u);
         const uint32_t ray = o.cand[i];
-        list_put(s0, ray, h - 1, pos, rank_of(rank_load(offsets, o.hit_mask, ray), ray), take, rs, s_sid, s_el,
-                 s_idx);
+        list_put(s0, ray, h - 1, pos, rank_of(rank_load(offsets, o.hit_mask, ray), ray), take, rs, hits);
     }
 }
 
@@ -1126,8 +1127,7 @@ __global__ void __launch_bounds__(kSortBlock) k_list_hist_sh(const uint32_t *lis
 }
 __global__ void __launch_bounds__(kSortBlock) k_list_scatter_sh(uint64_t s0, ProbeOut o, const uint32_t *offsets,
                                                                 const uint32_t *total, RunState *rs, uint32_t n_elem,
-                                                                uint32_t *elem_cursor, uint64_t *s_sid, uint32_t *s_el,
-                                                                uint32_t *s_idx) {
+                                                                uint32_t *elem_cursor, HitRec *hits) {
     __shared__ uint32_t h[kSortBins];
     const uint32_t n = *o.cand_count;
     const uint32_t take = batch_take(rs, total);
@@ -1158,7 +1158,7 @@ __global__ void __launch_bounds__(kSortBlock) k_list_scatter_sh(uint64_t s0, Pro
         for (int u = 0; u < kSortUnroll; ++u) {
             if (!x[u]) continue;
             const uint32_t pos = atomicAdd(&h[x[u] - 1], 1u);
-            list_put(s0, ray[u], x[u] - 1, pos, rank_of(q[u], ray[u]), take, rs, s_sid, s_el, s_idx);
+            list_put(s0, ray[u], x[u] - 1, pos, rank_of(q[u], ray[u]), take, rs, hits);
         }
     }
 }
@@ -1547,7 +1547,7 @@ __device__ __forceinline__ int wf_shade_hit(const SceneDev &S, const TraceOut &O
 // results go to round 0's shade queue and to the search queue of the ray's stage).
 template <int MIXED, int RECORDS, int FLAT>
 __global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kWfShadeMinBlocks) k_wf_first(
-    const __grid_constant__ SceneDev S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx, const uint32_t *total,
+    const __grid_constant__ SceneDev S, const HitRec *hits, const uint32_t *total,
     const RunState *rs, TraceOut O, WfState W, const __grid_constant__ WfQueues Q) {
     __shared__ WfBlockCtr c;
     __shared__ WfPushSh psh;
@@ -1560,7 +1560,6 @@ __global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kW
         take = uint32_t(n < left ? n : left);
         raynum_base = uint32_t(rs->hits_done);
     }
-    if (!hit_idx) n = take;
     const uint32_t stride = gridDim.x * kTraceBlock;
     // whole blocks in the loop (block-wide queue appends)
     const uint32_t n_round = (n + kTraceBlock - 1) / kTraceBlock * kTraceBlock;
@@ -1568,11 +1567,11 @@ __global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kW
         bool live = false;
         WfRay r;
         if (i < n) {
-            const uint32_t idx = hit_idx ? hit_idx[i] : i;
-            live = idx < take;
+            const HitRec hr = hits[i];
+            live = hr.rank < take;
             if (live) {
-                r.sid = hit_sid[i];
-                r.raynum = raynum_base + idx + 1;
+                r.sid = hr.sid;
+                r.raynum = raynum_base + hr.rank + 1;
                 RayRng rng;
                 rng.init(S.seed, r.sid, 0);
                 double xs, ys;
@@ -1581,7 +1580,7 @@ __global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kW
                 r.si = 0;
                 r.hits = 0;
                 r.last_j = -1;
-                r.next_j = int(hit_el[i]);
+                r.next_j = int(hr.el);
                 r.fe0 = -1;
                 r.moved = true;
             }
@@ -1748,7 +1747,7 @@ static void wf_launch_search(const SceneDev &S, const TraceOut &O, const WfState
 }
 
 template <int MIXED, int RECORDS>
-static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t *hit_el, const uint32_t *hit_idx,
+static int wf_launch(const SceneDev &S, const HitRec *hits,
                      const uint32_t *total, const RunState *rs, const TraceOut &O, const WfState &W,
                      const WfQueues &Q, const ReplayIn *replay, cudaStream_t st) {
     // persistent grids: every block the kernels can keep resident on every SM
@@ -1773,13 +1772,13 @@ static int wf_launch(const SceneDev &S, const uint64_t *hit_sid, const uint32_t 
     if (replay)
         k_wf_replay<MIXED, RECORDS><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, O, W, *replay, Q);
     else if (stage_search_kind(S.stages[0]) == kSearchFlat)  // heliostat fields: blocking search fused
-        k_wf_first<MIXED, RECORDS, 2><<<sms * per_sm[5], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs,
+        k_wf_first<MIXED, RECORDS, 2><<<sms * per_sm[5], kTraceBlock, 0, st>>>(S, hits, total, rs,
                                                                                  O, W, Q);
     else if (S.stages[0].flat_only)  // a first stage of flat elements only
-        k_wf_first<MIXED, RECORDS, 1><<<sms * per_sm[4], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs,
+        k_wf_first<MIXED, RECORDS, 1><<<sms * per_sm[4], kTraceBlock, 0, st>>>(S, hits, total, rs,
                                                                                  O, W, Q);
     else
-        k_wf_first<MIXED, RECORDS, 0><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, hit_sid, hit_el, hit_idx, total, rs,
+        k_wf_first<MIXED, RECORDS, 0><<<sms * per_sm[0], kTraceBlock, 0, st>>>(S, hits, total, rs,
                                                                                  O, W, Q);
     for (int r = 0; r < R; ++r) {
         for (int k = 0; k < nq; ++k) {
