@@ -508,7 +508,11 @@ def main():
     else:
         ach, pk = trace_tflops, fm.NOMINAL_FP64_TFLOPS
         hbm_ach = fm.trace_bytes(hits) / (trace_ms / 1e3) / 1e9
-    group = {"k_probe": "probe group (k_sun_candidates, k_sun_resolve, block-count scan, element sort)",
+    clk_summary = clk.summary()
+    clk_mhz = clk_summary.get("sm_mhz") or 1965.0
+    issue_peak = fm.issue_peak_per_s(clk_mhz)
+    group = {"k_probe": "probe group (k_sun_probe_exact or k_sun_candidates + k_sun_resolve, block-count scan, "
+                        "element sort)",
              "k_trace": "trace group (k_wf_first, k_wf_search, k_wf_shade, k_wf_finish)"}[dominant]
     roofline = {"bound": "fp64", "kernel": group, "achieved": ach, "peak": pk, "unit": "TFLOP/s",
                 "scope": "per step: the group's launches of every batch, timed by CUDA events around them",
@@ -519,7 +523,15 @@ def main():
                 "hbm": {"achieved": hbm_ach, "peak": hbm_peak, "unit": "GB/s", "frac": hbm_ach / hbm_peak,
                         "peak_source": "of measured" if "hbm_gbs" in peaks else "of fallback"},
                 "split_ms_per_step": {"k_probe+compact": probe_ms / len(runs), "k_trace": trace_ms / len(runs)},
-                "probe_tflops": probe_tflops, "trace_tflops": trace_tflops}
+                "probe_tflops": probe_tflops, "trace_tflops": trace_tflops,
+                # instruction issue: warp instructions per unit (ncu, flops_model) x units / the
+                # group's device time, against four warp instructions per SM and cycle
+                "issue": {
+                    "unit": "warp instructions/s",
+                    "peak": issue_peak,
+                    "peak_source": f"148 SMs x 4 schedulers x {clk_mhz:.0f} MHz (median SM clock of the timed steps)",
+                    "probe_group_frac": fm.WARP_INSTR_PER_SUN_RAY_PROBE * sun_rays / (probe_ms / 1e3) / issue_peak,
+                    "trace_group_frac": fm.WARP_INSTR_PER_HIT_TRACE * hits / (trace_ms / 1e3) / issue_peak}}
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
@@ -549,7 +561,7 @@ def main():
                                "fp64_trace": runs64[-1]["trace_variant"]},
         "units_per_step": units / len(runs), "sun_rays_per_step": sun_rays / len(runs),
         "receiver_flux_counts": int(flux_sum.sum()),
-        "roofline": roofline, "clocks": clk.summary(), "cpu_baseline": cpu,
+        "roofline": roofline, "clocks": clk_summary, "cpu_baseline": cpu,
         "other_configs": extra,
     }
     print(json.dumps(line), flush=True)

@@ -41,15 +41,25 @@ NOMINAL_FP64_TFLOPS = 148 * 64 * 2 * 1.965e9 / 1e12
 NOMINAL_FP32_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 
 
-# DRAM bytes (read + written) per unit, measured: ncu --set full captures of every main-batch
-# launch of the headline field at 2,000 heliostats and 2e6 hits (the command
-# `python bench.py --hits 2000000 --steps 1 --warmup 1 --no-cpu-baseline --no-extra`),
-# dram__bytes_read.sum + dram__bytes_write.sum summed over each launch group and divided by
-# the units the launches processed (15.32 M sun rays; 1.867 M first-stage hits).  The probe
-# figure is a lower bound at full size (its lists fit in L2 at 2e6 hits); the trace figure is
-# the wavefront's ray state, read and written at every kernel step.
-DRAM_BYTES_PER_SUN_RAY_PROBE = 4.17
-DRAM_BYTES_PER_HIT_TRACE = 368.0
+# DRAM bytes (read + written) and warp instructions issued per unit, measured: ncu --set full
+# captures of the main-batch launches of the headline field at 2,000 heliostats and 2e6 hits
+# (`python bench.py --hits 2000000 --steps 1 --warmup 1 --no-cpu-baseline --no-extra`, mixed
+# precision), dram__bytes_read.sum + dram__bytes_write.sum and smsp__inst_executed.sum summed
+# over each launch group and divided by the units the launches processed (15.32 M sun rays:
+# k_sun_probe_exact, k_sun_resolve_amb, k_scan_parts, k_scan_chunks, k_list_hist_sh,
+# k_list_scatter_sh; 1.867 M first-stage hits: k_wf_first, k_wf_search and k_wf_shade of
+# rounds 0 and 1).  The probe's lists fit in L2 at 2e6 hits, so its DRAM figure is a lower
+# bound at full size; the trace figure is the wavefront's ray state, read and written at
+# every kernel step.
+DRAM_BYTES_PER_SUN_RAY_PROBE = 2.87
+DRAM_BYTES_PER_HIT_TRACE = 365.0
+WARP_INSTR_PER_SUN_RAY_PROBE = 9.44
+WARP_INSTR_PER_HIT_TRACE = 125.5
+
+
+def issue_peak_per_s(sm_mhz: float = 1965.0, sms: int = 148) -> float:
+    """Warp instructions a B200 can issue per second: one per scheduler (four per SM) per cycle."""
+    return sms * 4 * sm_mhz * 1e6
 
 
 def probe_flops(sun_rays: int) -> float:

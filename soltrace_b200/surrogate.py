@@ -414,3 +414,31 @@ def time_fields(net: Mlp, tracer: FieldTracer, target_scale: float, n_suns: int 
     e1.record()
     torch.cuda.synchronize()
     return e0.elapsed_time(e1) / reps
+
+
+def _time_fused_forward(rows: int = 64 * 2000, group: int = 2000, reps: int = 20) -> None:
+    """Times the fused forward of a randomly initialised network on `rows` random inputs summed
+    per `group` rows (the field maps of rows / group suns): device milliseconds per pass and
+    TFLOP/s, with 4 warm-up passes.  `python -m soltrace_b200.surrogate`."""
+    import torch
+
+    from .lib import load
+    net = Mlp(load(), seed=3)
+    x = torch.randn(rows, DIMS[0], device="cuda").to(torch.bfloat16)
+    out = torch.zeros(-(-rows // group), DIMS[-1], dtype=torch.float32, device="cuda")
+    for _ in range(4):
+        net.forward_fused(x, group_rows=group, scale=1.0, clamp=True, out=out)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net.forward_fused(x, group_rows=group, scale=1.0, clamp=True, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    print(f"fused forward, {rows} rows in groups of {group}: {ms:.4f} ms per pass, "
+          f"{fused_flops(DIMS, rows) / (ms / 1e3) / 1e12:.1f} TFLOP/s, error flag {net.error()}")
+
+
+if __name__ == "__main__":
+    _time_fused_forward()
