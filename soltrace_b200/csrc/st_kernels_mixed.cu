@@ -26,7 +26,16 @@ int launch_probe_mixed(const SceneDev &S, uint64_t s0, uint32_t n, const ProbeOu
         if (S.sun.exact_flat && S.stages[0].flat_only && o.amb) {  // flat rectangles: float probe
             cudaMemsetAsync(o.cand_count, 0, sizeof(uint32_t), st);
             cudaMemsetAsync(o.amb_count, 0, sizeof(uint32_t), st);
-            k_sun_probe_exact<1><<<(n + kCandRays - 1) / kCandRays, kProbeBlock, 0, st>>>(S, s0, n, o, rs);
+            // the autotuner's variant: rays per thread (kExactRpt)
+            if (variant == 0)
+                k_sun_probe_exact<1, kExactRpt[0]><<<(n + kExactRpt[0] * kProbeBlock - 1) / (kExactRpt[0] * kProbeBlock),
+                                                     kProbeBlock, 0, st>>>(S, s0, n, o, rs);
+            else if (variant == 2)
+                k_sun_probe_exact<1, kExactRpt[2]><<<(n + kExactRpt[2] * kProbeBlock - 1) / (kExactRpt[2] * kProbeBlock),
+                                                     kProbeBlock, 0, st>>>(S, s0, n, o, rs);
+            else
+                k_sun_probe_exact<1, kExactRpt[1]><<<(n + kExactRpt[1] * kProbeBlock - 1) / (kExactRpt[1] * kProbeBlock),
+                                                     kProbeBlock, 0, st>>>(S, s0, n, o, rs);
             int dev = 0, sms = 148;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

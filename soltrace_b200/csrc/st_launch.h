@@ -31,7 +31,11 @@ __host__ __device__ inline int stage_search_kind(const StageRec &st) {
 }
 constexpr int kWfBruteMinBlocks = 8;      // search kernels of stages tested element by element
 constexpr int kWfFlatSearchMinBlocks = 5;  // search kernels of flat-only stages
-constexpr int kWfFirstFlatMinBlocks = 8;   // first kernel on a flat-only first stage
+constexpr int kWfFirstFlatMinBlocks = 8;   // first kernel on a flat-only first stage (FP64)
+#ifndef ST_FIRST_FLAT_MINB_MIXED
+#define ST_FIRST_FLAT_MINB_MIXED 8
+#endif
+constexpr int kWfFirstFlatMinBlocksMixed = ST_FIRST_FLAT_MINB_MIXED;  // the same in mixed precision
 
 constexpr int kWfClosedShadeMinBlocks = 4; // shade kernel of scenes with closed-form surfaces only
 #ifndef ST_EXACT_PROBE_MINB
@@ -141,7 +145,12 @@ struct ProbeOut {
     uint32_t *hit_mask;
     uint32_t *amb, *amb_count;  // mixed probe of flat rectangles: rays left to the double search
 };
-constexpr size_t hit_mask_words(uint64_t n) { return size_t((n + kCandRays - 1) / kCandRays) * (kCandRays / 32); }
+// hit-mask words for n sun rays, rounded up to whole blocks of the widest probe variant
+// (16 rays per thread): every probe kernel writes the words of its blocks in full
+constexpr int kMaskRays = kProbeBlock * 16;
+constexpr size_t hit_mask_words(uint64_t n) { return size_t((n + kMaskRays - 1) / kMaskRays) * (kMaskRays / 32); }
+// rays per thread of the mixed flat-rectangle probe, per autotuner variant
+constexpr int kExactRpt[kProbeVariants] = {4, 8, 16};
 
 // First-stage probe of sun rays [s0, s0 + n) into `o`.  Returns the number of kernels
 // launched.

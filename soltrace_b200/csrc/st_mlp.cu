@@ -130,6 +130,30 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 64 accumulator columns of the warp's 32 lanes in one load and one wait (the fused kernel's
+// epilogue: a wait per 16 columns would serialise sixteen tensor-memory round trips per layer)
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float v[64]) {
+    uint32_t r[64];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
+        "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, "
+        "%48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(taddr)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // Stage rows [r0, r0 + R) x K [k0, k0 + kBK) of an operand (element (r, k) at src[r lr + k lk],
 // rows < rows_end and k < k_end valid, zero elsewhere) in shared memory as K-major core
 // matrices: core matrix (row group g, K chunk c) at byte ((c R/8) + g) 128, its 8 rows 16 bytes
@@ -532,22 +556,27 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(FusedArgs g) {
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     const uint32_t ta = tmem + (uint32_t(warp * 32) << 16) + uint32_t(b * kWidth);
                     if (l < L - 1) {
-                        for (int c0 = 0; c0 < kWidth; c0 += 16) {
-                            float v[16];
-                            tmem_ld16(ta + uint32_t(c0), v);
-                            uint32_t p[8];
+                        for (int c64 = 0; c64 < kWidth; c64 += 64) {
+                            float w64[64];
+                            tmem_ld64(ta + uint32_t(c64), w64);
 #pragma unroll
-                            for (int i = 0; i < 8; ++i) {
-                                const float a0 = fmaxf(v[2 * i] + __ldg(bias + c0 + 2 * i), 0.f);
-                                const float a1 = fmaxf(v[2 * i + 1] + __ldg(bias + c0 + 2 * i + 1), 0.f);
-                                p[i] = uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(a0))) |
-                                       (uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(a1))) << 16);
+                            for (int q = 0; q < 4; ++q) {
+                                const float *v = w64 + 16 * q;
+                                const int c0 = c64 + 16 * q;
+                                uint32_t p[8];
+#pragma unroll
+                                for (int i = 0; i < 8; ++i) {
+                                    const float a0 = fmaxf(v[2 * i] + __ldg(bias + c0 + 2 * i), 0.f);
+                                    const float a1 = fmaxf(v[2 * i + 1] + __ldg(bias + c0 + 2 * i + 1), 0.f);
+                                    p[i] = uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(a0))) |
+                                           (uint32_t(__bfloat16_as_ushort(__float2bfloat16_rn(a1))) << 16);
+                                }
+                                const int kc = c0 / 8;
+                                *reinterpret_cast<uint4 *>(X + (kc * 16 + r / 8) * 128 + (r % 8) * 16) =
+                                    make_uint4(p[0], p[1], p[2], p[3]);
+                                *reinterpret_cast<uint4 *>(X + ((kc + 1) * 16 + r / 8) * 128 + (r % 8) * 16) =
+                                    make_uint4(p[4], p[5], p[6], p[7]);
                             }
-                            const int kc = c0 / 8;
-                            *reinterpret_cast<uint4 *>(X + (kc * 16 + r / 8) * 128 + (r % 8) * 16) =
-                                make_uint4(p[0], p[1], p[2], p[3]);
-                            *reinterpret_cast<uint4 *>(X + ((kc + 1) * 16 + r / 8) * 128 + (r % 8) * 16) =
-                                make_uint4(p[4], p[5], p[6], p[7]);
                         }
                         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                         mbar_arrive(&acc_free[b]);
@@ -559,9 +588,13 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(FusedArgs g) {
                         const long long grp = (long long)(valid ? row : g.M - 1) / (g.mode == 1 ? g.group_rows : 1);
                         const long long grp0 = __shfl_sync(0xffffffffu, grp, 0);
                         const bool uniform = __all_sync(0xffffffffu, grp0 == grp) && g.mode == 1;
-                        for (int c0 = 0; c0 < kWidth; c0 += 16) {
-                            float v[16];
-                            tmem_ld16(ta + uint32_t(c0), v);
+                        for (int c64 = 0; c64 < kWidth; c64 += 64) {
+                          float w64[64];
+                          tmem_ld64(ta + uint32_t(c64), w64);
+#pragma unroll
+                          for (int q = 0; q < 4; ++q) {
+                            float *v = w64 + 16 * q;
+                            const int c0 = c64 + 16 * q;
 #pragma unroll
                             for (int i = 0; i < 16; ++i) {
                                 float y = (v[i] + __ldg(bias + n0 + c0 + i)) * g.scale;
@@ -597,6 +630,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) k_mlp_fused(FusedArgs g) {
 #pragma unroll
                                 for (int i = 0; i < 16; ++i) atomicAdd(g.out + grp * g.n_out + col + i, v[i]);
                             }
+                          }
                         }
                         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                         mbar_arrive(&acc_free[b]);

@@ -149,14 +149,15 @@ static cudaError_t probe_buffers(Workspace &ws, uint64_t n, ProbeOut &o) {
     return cudaSuccess;
 }
 
-// Autotuner: time every register-budget variant of the probe on the same 2^21 sun rays
-// (indices 0.., outputs discarded into scratch buffers) and keep the fastest for this
-// workspace and precision.  Variants share their arithmetic, so the choice changes
-// timing only.
+// Autotuner: time every variant of the probe (register budgets, or rays per thread of the
+// mixed flat-rectangle probe) on the same 2^24 sun rays (indices 0.., outputs discarded into
+// scratch buffers: enough blocks to fill the GPU at every variant's rays per block, as the
+// 2^26-ray batches do) and keep the fastest for this workspace and precision.  Variants share
+// their arithmetic, so the choice changes timing only.
 static cudaError_t autotune(Workspace &ws, const SceneDev &S0, int precision, uint64_t max_sun, cudaStream_t st,
                             int &launches) {
     Workspace::Tuning &tu = ws.tune[precision ? 1 : 0];
-    const uint64_t n = std::min<uint64_t>(uint64_t(1) << 21, max_sun);
+    const uint64_t n = std::min<uint64_t>(uint64_t(1) << 24, max_sun);
     if (n == 0) return cudaSuccess;
     cudaError_t e;
     ProbeOut po;

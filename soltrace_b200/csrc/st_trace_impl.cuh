@@ -428,6 +428,14 @@ __device__ inline void refract(const OpticRec &op, const double cin[3], const do
 template <int MIXED>
 __device__ inline void error_sample(const SceneDev &S, int dist, double delop, const double axis[3], RayRng &rng,
                                     bool redraw_below, const double nrm[3], double out[3]) {
+    // mixed precision: a Gaussian or pillbox spread of zero (a perfectly specular mirror)
+    // leaves the axis unchanged; its two draws are skipped rather than generated, so the
+    // ray's later draws stay where they are
+    if (MIXED && delop == 0.0 && (dist == 'g' || dist == 'G' || dist == 'p' || dist == 'P')) {
+        rng.k += 2;
+        for (int q = 0; q < 3; ++q) out[q] = axis[q];
+        return;
+    }
     for (unsigned call = 0;; ++call) {
         const double ut = rng.u();
         const double up = rng.u();
@@ -678,29 +686,29 @@ __global__ void __launch_bounds__(kResolveBlock, MINB) k_sun_resolve(const __gri
 // rounding of one depth leave the ray undecided: it goes to a list that k_sun_resolve_amb
 // searches in double, so the element found is the FP64 probe's.  Output as k_sun_resolve
 // leaves it: hitting rays listed with their element, one hit-mask bit per ray, hits per
-// kProbeBlock rays.  kCandPerThread sun rays per thread at kProbeBlock apart, kCandRays per
-// block.
-template <int MIXED>
+// kProbeBlock rays.  RPT sun rays per thread at kProbeBlock apart (4, 8 or 16: the autotuner's
+// variants), RPT x kProbeBlock per block.
+template <int MIXED, int RPT>
 __global__ void __launch_bounds__(kProbeBlock, kExactProbeMinBlocks) k_sun_probe_exact(const __grid_constant__ SceneDev S, uint64_t s0,
                                                                   uint32_t n, ProbeOut o, const RunState *rs) {
     const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (rs->reached) {  // the requested hits are numbered: this batch is surplus
-        if (threadIdx.x < kCandPerThread && blockIdx.x * kCandPerThread + threadIdx.x < nb)
-            o.block_counts[blockIdx.x * kCandPerThread + threadIdx.x] = 0;
-        if (o.hit_mask && threadIdx.x < kCandRays / 32) o.hit_mask[blockIdx.x * (kCandRays / 32) + threadIdx.x] = 0;
+        if (threadIdx.x < RPT && blockIdx.x * RPT + threadIdx.x < nb)
+            o.block_counts[blockIdx.x * RPT + threadIdx.x] = 0;
+        if (o.hit_mask && threadIdx.x < (RPT * kProbeBlock) / 32) o.hit_mask[blockIdx.x * ((RPT * kProbeBlock) / 32) + threadIdx.x] = 0;
         return;
     }
     const SunDev &sun = S.sun;
     // per ray of the block its result, per warp and ray group the hit ballot
     constexpr uint32_t kUndecided = 0xffffffffu;
-    __shared__ uint32_t hsh[kCandPerThread][kProbeBlock];
-    __shared__ unsigned wb[kCandPerThread][kProbeBlock / 32];
+    __shared__ uint32_t hsh[RPT][kProbeBlock];
+    __shared__ unsigned wb[RPT][kProbeBlock / 32];
     __shared__ uint32_t wn[kProbeBlock / 32], base;
     // pass 1, float only: element + 1, 0 for a miss, kUndecided for the double-precision search
 #pragma unroll 1
-    for (int m = 0; m < kCandPerThread; ++m) {
-        const uint32_t i = blockIdx.x * kCandRays + m * kProbeBlock + threadIdx.x;
+    for (int m = 0; m < RPT; ++m) {
+        const uint32_t i = blockIdx.x * (RPT * kProbeBlock) + m * kProbeBlock + threadIdx.x;
         uint32_t h = 0;
         if (i < n) {
             RayRng rng;
@@ -754,8 +762,8 @@ __global__ void __launch_bounds__(kProbeBlock, kExactProbeMinBlocks) k_sun_probe
     // pass 2: undecided rays (a few per million) to the double-precision list; ballots, mask
     uint32_t mine = 0;
 #pragma unroll 1
-    for (int m = 0; m < kCandPerThread; ++m) {
-        const uint32_t i = blockIdx.x * kCandRays + m * kProbeBlock + threadIdx.x;
+    for (int m = 0; m < RPT; ++m) {
+        const uint32_t i = blockIdx.x * (RPT * kProbeBlock) + m * kProbeBlock + threadIdx.x;
         uint32_t h = hsh[m][threadIdx.x];
         if (h == kUndecided) {
             o.amb[atomicAdd(o.amb_count, 1u)] = i;
@@ -765,7 +773,7 @@ __global__ void __launch_bounds__(kProbeBlock, kExactProbeMinBlocks) k_sun_probe
         if (o.hit_elem && i < n) o.hit_elem[i] = h;
         const unsigned bal = __ballot_sync(0xffffffffu, h != 0);
         if (lane == 0) {
-            if (o.hit_mask) o.hit_mask[(blockIdx.x * kCandRays + m * kProbeBlock) / 32 + w] = bal;
+            if (o.hit_mask) o.hit_mask[(blockIdx.x * (RPT * kProbeBlock) + m * kProbeBlock) / 32 + w] = bal;
             wb[m][w] = bal;
         }
         mine += __popc(bal);
@@ -773,10 +781,10 @@ __global__ void __launch_bounds__(kProbeBlock, kExactProbeMinBlocks) k_sun_probe
     // one reservation in the list per block: warp counts, their prefix, one atomic
     if (lane == 0) wn[w] = mine;
     __syncthreads();
-    if (threadIdx.x < kCandPerThread && blockIdx.x * kCandPerThread + threadIdx.x < nb) {
+    if (threadIdx.x < RPT && blockIdx.x * RPT + threadIdx.x < nb) {
         uint32_t c = 0;
         for (int k = 0; k < kProbeBlock / 32; ++k) c += __popc(wb[threadIdx.x][k]);
-        o.block_counts[blockIdx.x * kCandPerThread + threadIdx.x] = c;
+        o.block_counts[blockIdx.x * RPT + threadIdx.x] = c;
     }
     if (threadIdx.x == 0) {
         uint32_t t = 0;
@@ -790,11 +798,11 @@ __global__ void __launch_bounds__(kProbeBlock, kExactProbeMinBlocks) k_sun_probe
     __syncthreads();
     uint32_t at = base + wn[w];
     const unsigned lt = (1u << lane) - 1u;
-    for (int m = 0; m < kCandPerThread; ++m) {
+    for (int m = 0; m < RPT; ++m) {
         const unsigned bal = wb[m][w];
         if ((bal >> lane) & 1u) {
             const uint32_t pos = at + __popc(bal & lt);
-            o.cand[pos] = blockIdx.x * kCandRays + m * kProbeBlock + threadIdx.x;
+            o.cand[pos] = blockIdx.x * (RPT * kProbeBlock) + m * kProbeBlock + threadIdx.x;
             if (o.cand_el) o.cand_el[pos] = hsh[m][threadIdx.x];
         }
         at += __popc(bal);
@@ -1546,7 +1554,8 @@ __device__ __forceinline__ int wf_shade_hit(const SceneDev &S, const TraceOut &O
 // kSearchFlat, and the rays it reflects are searched for blocking in this kernel (their
 // results go to round 0's shade queue and to the search queue of the ray's stage).
 template <int MIXED, int RECORDS, int FLAT>
-__global__ void __launch_bounds__(kTraceBlock, FLAT ? kWfFirstFlatMinBlocks : kWfShadeMinBlocks) k_wf_first(
+__global__ void __launch_bounds__(kTraceBlock, FLAT ? (MIXED ? kWfFirstFlatMinBlocksMixed : kWfFirstFlatMinBlocks)
+                                                    : kWfShadeMinBlocks) k_wf_first(
     const __grid_constant__ SceneDev S, const HitRec *hits, const uint32_t *total,
     const RunState *rs, TraceOut O, WfState W, const __grid_constant__ WfQueues Q) {
     __shared__ WfBlockCtr c;
