@@ -1078,36 +1078,50 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
     CK(upload(ws.bvh, hs.bvh, st, h2d));
     CK(upload(ws.bvh_items, hs.bvh_items, st, h2d));
     CK(upload(ws.inv_cdf, hs.inv_cdf, st, h2d));
-    // every position's tables, concatenated
-    std::vector<int> cells;
-    std::vector<float4> disc, par, xa, xb, xc;
-    std::vector<ElemRec> pelems;
+    // every position's tables, laid end to end on the device: sized first, then each position's
+    // arrays copied straight from its own vectors (no host-side concatenation)
     std::vector<size_t> off_cells(K), off_disc(K), off_elems(K);
     bool all_exact = true;
     for (const SunPosition &sp : pos)
         if (!sp.sun.exact_flat || sp.cell_xa.size() != sp.cell_disc.size() || sp.cell_xa.empty()) all_exact = false;
+    size_t n_cells = 0, n_disc = 0, n_elems = 0;
     for (size_t p = 0; p < K; ++p) {
         const SunPosition &sp = pos[p];
-        off_cells[p] = cells.size();
-        cells.insert(cells.end(), sp.cell_start.begin(), sp.cell_start.end());
-        off_disc[p] = disc.size();
-        disc.insert(disc.end(), sp.cell_disc.begin(), sp.cell_disc.end());
-        par.insert(par.end(), sp.cell_par.begin(), sp.cell_par.end());
-        if (all_exact) {
-            xa.insert(xa.end(), sp.cell_xa.begin(), sp.cell_xa.end());
-            xb.insert(xb.end(), sp.cell_xb.begin(), sp.cell_xb.end());
-            xc.insert(xc.end(), sp.cell_xc.begin(), sp.cell_xc.end());
-        }
-        off_elems[p] = sp.elems.empty() ? size_t(-1) : pelems.size();
-        pelems.insert(pelems.end(), sp.elems.begin(), sp.elems.end());
+        off_cells[p] = n_cells;
+        n_cells += sp.cell_start.size();
+        off_disc[p] = n_disc;
+        n_disc += sp.cell_disc.size();
+        off_elems[p] = sp.elems.empty() ? size_t(-1) : n_elems;
+        n_elems += sp.elems.size();
     }
-    CK(upload(ws.pos_cells, cells, st, h2d));
-    CK(upload(ws.pos_disc, disc, st, h2d));
-    CK(upload(ws.pos_par, par, st, h2d));
-    CK(upload(ws.pos_xa, xa, st, h2d));
-    CK(upload(ws.pos_xb, xb, st, h2d));
-    CK(upload(ws.pos_xc, xc, st, h2d));
-    CK(upload(ws.pos_elems, pelems, st, h2d));
+    CK(ws.pos_cells.ensure(std::max<size_t>(n_cells * sizeof(int), 16)));
+    CK(ws.pos_disc.ensure(std::max<size_t>(n_disc * sizeof(float4), 16)));
+    CK(ws.pos_par.ensure(std::max<size_t>(n_disc * sizeof(float4), 16)));
+    if (all_exact) {
+        CK(ws.pos_xa.ensure(std::max<size_t>(n_disc * sizeof(float4), 16)));
+        CK(ws.pos_xb.ensure(std::max<size_t>(n_disc * sizeof(float4), 16)));
+        CK(ws.pos_xc.ensure(std::max<size_t>(n_disc * sizeof(float4), 16)));
+    }
+    CK(ws.pos_elems.ensure(std::max<size_t>(n_elems * sizeof(ElemRec), 16)));
+    auto put = [&](DevBuf &dst, size_t off_elems_of_t, const void *src, size_t bytes) -> cudaError_t {
+        if (!bytes) return cudaSuccess;
+        h2d += bytes;
+        return cudaMemcpyAsync(static_cast<char *>(dst.p) + off_elems_of_t, src, bytes, cudaMemcpyHostToDevice, st);
+    };
+    for (size_t p = 0; p < K; ++p) {
+        const SunPosition &sp = pos[p];
+        CK(put(ws.pos_cells, off_cells[p] * sizeof(int), sp.cell_start.data(), sp.cell_start.size() * sizeof(int)));
+        const size_t od = off_disc[p] * sizeof(float4), nd = sp.cell_disc.size() * sizeof(float4);
+        CK(put(ws.pos_disc, od, sp.cell_disc.data(), nd));
+        CK(put(ws.pos_par, od, sp.cell_par.data(), sp.cell_par.size() * sizeof(float4)));
+        if (all_exact) {
+            CK(put(ws.pos_xa, od, sp.cell_xa.data(), nd));
+            CK(put(ws.pos_xb, od, sp.cell_xb.data(), nd));
+            CK(put(ws.pos_xc, od, sp.cell_xc.data(), nd));
+        }
+        if (!sp.elems.empty())
+            CK(put(ws.pos_elems, off_elems[p] * sizeof(ElemRec), sp.elems.data(), sp.elems.size() * sizeof(ElemRec)));
+    }
 
     SceneDev S0 = hs.dev;
     S0.elems = ws.elems.as<ElemRec>();
