@@ -333,7 +333,8 @@ def surrogate_line(api) -> dict:
     tracer = S.FieldTracer(api)
     try:
         net, scale, t_data, t_train = S.fit(tracer, N_TRAIN_TRACES, 10_000_000, N_TRAIN_STEPS, batch=N_TRAIN_BATCH)
-        peaks, l1 = S.judge(net, tracer, scale, 16, 10_000_000)
+        noise = []
+        peaks, l1 = S.judge(net, tracer, scale, 16, 10_000_000, noise=noise)
         untrained = S.Mlp(api, seed=77)
         peaks0, l10 = S.judge(untrained, tracer, scale, 4, 10_000_000)
         ms = S.time_fields(net, tracer, scale, n_suns=64)
@@ -356,6 +357,7 @@ def surrogate_line(api) -> dict:
                         "heliostats in one fused tcgen05 pass vs the trace of one sun at 1e7 hits",
             "speedup": 64 * per_trace / ms, "surrogate_ms_64_suns": ms, "trace_ms_per_sun_1e7": per_trace,
             "peak_error_max": max(peaks), "peak_error_mean": float(np.mean(peaks)),
+            "trace_repeat_peak_error_max": max(noise), "trace_repeat_peak_error_mean": float(np.mean(noise)),
             "map_l1_error_mean": float(np.mean(l1)), "untrained_peak_error_mean": float(np.mean(peaks0)),
             "untrained_map_l1_error_mean": float(np.mean(l10)), "train_traces": N_TRAIN_TRACES,
             "train_samples": N_TRAIN_TRACES * 2000, "train_steps": N_TRAIN_STEPS, "train_batch": N_TRAIN_BATCH,

@@ -370,11 +370,14 @@ def fit(tracer: FieldTracer, n_traces: int, hits: int, steps: int, seed: int = 1
     return net, scale, t1 - t0, time.perf_counter() - t1
 
 
-def judge(net: Mlp, tracer: FieldTracer, target_scale: float, n: int, hits: int, seed: int = 999):
+def judge(net: Mlp, tracer: FieldTracer, target_scale: float, n: int, hits: int, seed: int = 999,
+          noise: list = None):
     """Field maps predicted for n held-out random situations (half of them with every aim
     offset 0) against traces of the same situations at `hits` hits: per situation the
     relative peak error |peak(pred) - peak(trace)| / peak(trace) and the relative L1 map
-    error sum |pred - trace| / sum trace."""
+    error sum |pred - trace| / sum trace.  With `noise` (a list), each situation is traced a
+    second time with another seed and the peak error of that repeat against the first trace
+    (the judging trace's own Monte-Carlo noise in the same measure) is appended to it."""
     rng = np.random.default_rng(seed)
     peaks, l1 = [], []
     for i in range(n):
@@ -386,6 +389,9 @@ def judge(net: Mlp, tracer: FieldTracer, target_scale: float, n: int, hits: int,
         pred = pred.reshape(IMG, IMG).double().cpu().numpy()
         peaks.append(peak_error(pred, whole))
         l1.append(float(np.abs(pred - whole).sum() / max(whole.sum(), 1e-30)))
+        if noise is not None:
+            _, again = tracer.trace(sun, off, sig, hits, 7000 + i)
+            noise.append(peak_error(again, whole))
     return peaks, l1
 
 
