@@ -324,7 +324,7 @@ N_TRAIN_TRACES, N_TRAIN_STEPS, N_TRAIN_BATCH = 1000, 12000, 16384
 def surrogate_line(api) -> dict:
     """C5: the BF16 flux surrogate (6 layers, width 256, 32 x 32 receiver image per heliostat)
     trained on the device from 2e6 traced samples (1,000 traces of the headline field at 1e7
-    hits, each giving 2,000 per-heliostat images), judged on 16 held-out situations traced at
+    hits, each giving 2,000 per-heliostat images), compared on 16 held-out situations traced at
     1e7 hits, and timed predicting the field maps of 64 sun positions x 2,000 heliostats in one
     fused pass against the plain trace of one position at 1e7 hits."""
     import torch
@@ -334,9 +334,9 @@ def surrogate_line(api) -> dict:
     try:
         net, scale, t_data, t_train = S.fit(tracer, N_TRAIN_TRACES, 10_000_000, N_TRAIN_STEPS, batch=N_TRAIN_BATCH)
         noise = []
-        peaks, l1 = S.judge(net, tracer, scale, 16, 10_000_000, noise=noise)
+        peaks, l1 = S.evaluate(net, tracer, scale, 16, 10_000_000, noise=noise)
         untrained = S.Mlp(api, seed=77)
-        peaks0, l10 = S.judge(untrained, tracer, scale, 4, 10_000_000)
+        peaks0, l10 = S.evaluate(untrained, tracer, scale, 4, 10_000_000)
         ms = S.time_fields(net, tracer, scale, n_suns=64)
         rng = np.random.default_rng(5)
         trace_ms = []

@@ -8,8 +8,8 @@ the mean-squared-error loss against the target images.  Backward: dZ = dA * (A >
 dW = dZ^T X, db = sum over rows of dZ, dX = dZ W, with the activations and incoming
 gradients rounded to bfloat16 where the device stores them in bfloat16.
 
-This network has no counterpart in the reference (SolTrace traces every ray); its judge is
-the plain trace.  Nothing in the product imports this file.
+This network has no counterpart in the reference (SolTrace traces every ray); its error is
+measured against the plain trace.  Nothing in the product imports this file.
 """
 from __future__ import annotations
 

@@ -3,7 +3,7 @@
 //
 // The surrogate maps one heliostat's inputs (sun vector, field position, aim offset, slope
 // error) to the flux image it puts on the receiver; the plain trace (st_sim_run with a
-// per-source flux map) makes its training data and judges it.  It has no counterpart in the
+// per-source flux map) makes its training data and measures its error.  It has no counterpart in the
 // reference, which traces every ray.
 //
 // One GEMM kernel does every layer's work, forward and backward:

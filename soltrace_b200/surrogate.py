@@ -5,7 +5,7 @@ position (2, in km), aim offset on the receiver (2, m), slope-error sigma (1, mr
 flux image it puts on the receiver (32 x 32 bins over the cylinder: angle x height, kW per
 bin at 1000 W/m2 DNI).  Summing the heliostats' images gives the field's receiver flux map,
 so an aim strategy can be evaluated -- and improved by gradient steps on the aim offsets --
-in one batched network pass instead of a trace.  The plain trace stays the judge: training
+in one batched network pass instead of a trace.  The plain trace stays the reference: training
 images come from st_sim_run with a per-source flux map (every heliostat's image in one run),
 and every surrogate answer can be checked against a trace of the same configuration.
 
@@ -370,7 +370,7 @@ def fit(tracer: FieldTracer, n_traces: int, hits: int, steps: int, seed: int = 1
     return net, scale, t1 - t0, time.perf_counter() - t1
 
 
-def judge(net: Mlp, tracer: FieldTracer, target_scale: float, n: int, hits: int, seed: int = 999,
+def evaluate(net: Mlp, tracer: FieldTracer, target_scale: float, n: int, hits: int, seed: int = 999,
           noise: list = None):
     """Field maps predicted for n held-out random situations (half of them with every aim
     offset 0) against traces of the same situations at `hits` hits: per situation the

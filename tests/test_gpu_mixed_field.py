@@ -1,6 +1,6 @@
 """Mixed precision on the headline heliostat field, against the oracle.
 
-* Deterministic mode: explicit rays fired at the 2,000-heliostat field
+* Deterministic mode (positions within 1e-5 m): explicit rays fired at the 2,000-heliostat field
   from 1 km away, errors off, traced through the blocking search to the receiver 100 m to
   1 km further on.  Every record's element, stage and ray number must equal the FP64
   oracle's, and positions must agree within 1e-5 m (directions within 1e-8).

@@ -34,8 +34,8 @@ def test_source_images_add_up_to_the_receiver_map(tracer):
 def test_trained_surrogate_beats_untrained(tracer, product):
     from soltrace_b200 import surrogate as S
     net, scale, _, _ = S.fit(tracer, 40, 5_000_000, 800)
-    peaks, l1 = S.judge(net, tracer, scale, 4, 5_000_000)
-    peaks0, l10 = S.judge(S.Mlp(product, seed=77), tracer, scale, 2, 5_000_000)
+    peaks, l1 = S.evaluate(net, tracer, scale, 4, 5_000_000)
+    peaks0, l10 = S.evaluate(S.Mlp(product, seed=77), tracer, scale, 2, 5_000_000)
     assert net.error() == 0
     assert np.mean(l1) < 0.15 and np.mean(l1) < 0.25 * np.mean(l10), (l1, l10)
     assert np.mean(peaks) < 0.08, peaks
