@@ -353,7 +353,7 @@ def surrogate_line(api) -> dict:
     flops = S.fused_flops(S.DIMS, 64 * 2000)
     tflops = flops / (ms / 1e3) / 1e12
     per_trace = float(np.median(trace_ms))
-    return {"workload": "C5 BF16 MLP flux surrogate (8 -> 5 x 256 -> 1024), field maps of 64 suns x 2,000 "
+    return {"workload": "C5 BF16 MLP flux surrogate (16 -> 5 x 256 -> 1024), field maps of 64 suns x 2,000 "
                         "heliostats in one fused tcgen05 pass vs the trace of one sun at 1e7 hits",
             "speedup": 64 * per_trace / ms, "surrogate_ms_64_suns": ms, "trace_ms_per_sun_1e7": per_trace,
             "peak_error_max": max(peaks), "peak_error_mean": float(np.mean(peaks)),
