@@ -17,18 +17,25 @@ extern "C" {
 #endif
 
 /* Arithmetic of the per-ray work.
- *   ST_B200_FP64  (default): every ray computation in double precision.
- *   ST_B200_MIXED: element-local intersection, interaction and error sampling in
- *                  float; global/stage/element transforms, the torus quartic, the
- *                  Newton refinement of file-defined surfaces and all counters in
- *                  double/64-bit integers. */
+ *   ST_B200_FP64  (default): every ray computation in double precision, rounded as the
+ *                  reference's x86-64 build rounds it (no fused multiply-add).
+ *   ST_B200_MIXED: aperture tests, property tables, Fresnel coefficients, error sampling
+ *                  and flux binning in float; the first-stage probe of flat rectangles
+ *                  decides hits in float and defers to double within float rounding (the
+ *                  hits are the FP64 probe's); transforms, closed-form roots, the torus
+ *                  quartic, Newton refinement, reflection and refraction directions and
+ *                  all counters in double / 64-bit integers (positions of explicit rays
+ *                  agree with FP64 within 1e-5 m on km paths). */
 #define ST_B200_FP64 0
 #define ST_B200_MIXED 1
 int st_b200_set_precision(st_context_t pcxt, int mode);
 
 /* 1 (default): build the per-intersection records that st_locations & co. read
- * back, in the reference's order.  0: keep only counters and flux maps (the
- * records are then never materialised in device or host memory). */
+ * back, in the reference's order (put in that order on the device; the context keeps
+ * them in page-locked host memory until its next run).  A run with records holds at
+ * most 2^31 of them, and its stages times its ray numbers stay below 2^31.  0: keep
+ * only counters and flux maps (the records are then never materialised in device or
+ * host memory). */
 int st_b200_set_records(st_context_t pcxt, int on);
 
 /* CUDA device ordinal used by st_sim_run (default 0). */
