@@ -37,7 +37,10 @@ constexpr int kWfFirstFlatMinBlocks = 8;   // first kernel on a flat-only first 
 #endif
 constexpr int kWfFirstFlatMinBlocksMixed = ST_FIRST_FLAT_MINB_MIXED;  // the same in mixed precision
 
-constexpr int kWfClosedShadeMinBlocks = 4; // shade kernel of scenes with closed-form surfaces only
+// shade kernel of scenes with closed-form surfaces only: FP64 (5 blocks per SM measured faster
+// than 4 and no slower than 6) and mixed precision (4; 5 and 6 no faster)
+constexpr int kWfClosedShadeMinBlocks = 5;
+constexpr int kWfClosedShadeMinBlocksMixed = 4;
 #ifndef ST_EXACT_PROBE_MINB
 #define ST_EXACT_PROBE_MINB 8
 #endif

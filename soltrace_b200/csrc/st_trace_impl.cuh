@@ -1691,7 +1691,8 @@ __global__ void __launch_bounds__(kTraceBlock, SearchBounds<KIND>::min_blocks) k
 // Shade kernel over round r's shade queue: survivors go to the next round's search queues.
 // CLOSED: every stage has closed-form surfaces only.
 template <int MIXED, int RECORDS, int CLOSED>
-__global__ void __launch_bounds__(kTraceBlock, CLOSED ? kWfClosedShadeMinBlocks : kWfShadeMinBlocks) k_wf_shade(const __grid_constant__ SceneDev S, TraceOut O,
+__global__ void __launch_bounds__(kTraceBlock, CLOSED ? (MIXED ? kWfClosedShadeMinBlocksMixed : kWfClosedShadeMinBlocks)
+                                                      : kWfShadeMinBlocks) k_wf_shade(const __grid_constant__ SceneDev S, TraceOut O,
                                                                              WfState W, const __grid_constant__ WfQueues Q,
                                                                              int r) {
     __shared__ WfBlockCtr c;
