@@ -199,3 +199,25 @@ def test_per_heliostat_counts(product):
     np.testing.assert_array_equal(first, np.bincount(firsts - 1, minlength=120))
     assert int(delivered.sum()) == int(np.sum((rec["stage"] == 2) & (rec["element"] < 0)))
     assert st["ray_hits"] == 50000 and st["sun_rays"] >= 50000
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_sun_ray_cap_fails_like_the_oracle(product, oracle, prec):
+    """A run that needs more sun rays than st_sim_params' maximum returns -1 with the
+    reference's message (raytrace.cpp:600-602; the oracle's message is pinned to the
+    reference's in test_oracle.py), and the context runs again once the cap is raised."""
+    tight = scenes.dish_scene(1000)
+    tight.raymax = 500
+    want = run_scene(oracle, tight, 1)
+    assert want[0] == -1
+    ctx = product.st_create_context()
+    try:
+        scenes.push(product, ctx, tight)
+        product.st_b200_set_precision(ctx, prec)
+        assert product.run(ctx, 1) == -1
+        assert want[3][-1] in product.messages(ctx), (product.messages(ctx), want[3])
+        product.st_sim_params(ctx, 1000, 1_000_000, 0)
+        assert product.run(ctx, 1) > 0, product.messages(ctx)
+        assert product.stats(ctx)["ray_hits"] == 1000
+    finally:
+        product.st_free_context(ctx)
