@@ -318,7 +318,9 @@ def config_lines(api, args) -> dict:
     return out
 
 
-N_TRAIN_TRACES, N_TRAIN_STEPS, N_TRAIN_BATCH = 1000, 12000, 16384
+# 20,000 Adam steps with the rate decayed 2e-3 -> 6e-5: on the same data, 16 held-out peak
+# errors of max 2.1 % (mean 1.0 %) against 3.1 % (1.3 %) for 12,000 steps decayed 2e-3 -> 2e-4
+N_TRAIN_TRACES, N_TRAIN_STEPS, N_TRAIN_BATCH, N_TRAIN_LR_FINAL = 1000, 20000, 16384, 0.03
 
 
 def surrogate_line(api) -> dict:
@@ -332,7 +334,8 @@ def surrogate_line(api) -> dict:
     from soltrace_b200 import surrogate as S
     tracer = S.FieldTracer(api)
     try:
-        net, scale, t_data, t_train = S.fit(tracer, N_TRAIN_TRACES, 10_000_000, N_TRAIN_STEPS, batch=N_TRAIN_BATCH)
+        net, scale, t_data, t_train = S.fit(tracer, N_TRAIN_TRACES, 10_000_000, N_TRAIN_STEPS, batch=N_TRAIN_BATCH,
+                                            lr_final=N_TRAIN_LR_FINAL)
         noise = []
         peaks, l1 = S.evaluate(net, tracer, scale, 16, 10_000_000, noise=noise)
         untrained = S.Mlp(api, seed=77)
@@ -466,6 +469,8 @@ def main():
 
     # FP64 device trace of the same steps: throughput and the flux-map L2 error
     n64 = max(1, min(args.steps, 2))
+    for k in range(max(1, min(args.warmup, 3))):  # untimed, as for the mixed steps
+        step(0, seed0 + k)
     runs64 = [step(0, seed0 + 100 + k) for k in range(n64)]
     units64 = sum(r["ray_stage_units"] for r in runs64)
     dev64 = sum(r["kernel_ms"] for r in runs64)

@@ -310,10 +310,11 @@ def make_dataset(tracer: FieldTracer, n_traces: int, hits: int, seed: int = 0):
     return torch.cat(xs), torch.cat(ts)
 
 
-def train(net: Mlp, x, t, steps: int, batch: int = 8192, lr: float = 1e-3, seed: int = 0, target_scale: float = None):
-    """Adam on random minibatches, the learning rate decayed by 10 over the run.  Targets are
-    divided by target_scale (default: their 99.9th percentile) so the network sees O(1)
-    values; returns (scale, loss history)."""
+def train(net: Mlp, x, t, steps: int, batch: int = 8192, lr: float = 1e-3, seed: int = 0, target_scale: float = None,
+          lr_final: float = 0.1):
+    """Adam on random minibatches, the learning rate decayed exponentially to lr * lr_final
+    over the run.  Targets are divided by target_scale (default: their 99.9th percentile) so
+    the network sees O(1) values; returns (scale, loss history)."""
     import torch
     if target_scale is None:
         target_scale = float(torch.quantile(t.flatten()[:: max(1, t.numel() // 4_000_000)].float(), 0.999).item())
@@ -323,7 +324,7 @@ def train(net: Mlp, x, t, steps: int, batch: int = 8192, lr: float = 1e-3, seed:
     hist = []
     for k in range(steps):
         idx = torch.randint(0, x.shape[0], (batch,), device="cuda", generator=g)
-        step_lr = lr * (0.1 ** (k / max(steps - 1, 1)))
+        step_lr = lr * (lr_final ** (k / max(steps - 1, 1)))
         loss = net.train_step(xb[idx], t[idx] / target_scale, lr=step_lr)
         if k % 50 == 0 or k == steps - 1:
             hist.append(float(loss.item()))
@@ -384,7 +385,7 @@ def optimise_aims(net: Mlp, tracer: "FieldTracer", sun, offsets, sigma: float, t
 # Fitting and judging against the trace
 # ------------------------------------------------------------------------------------
 def fit(tracer: FieldTracer, n_traces: int, hits: int, steps: int, seed: int = 1, dims=DIMS, batch: int = 8192,
-        lr: float = 2e-3):
+        lr: float = 2e-3, lr_final: float = 0.1):
     """A network trained on n_traces random situations traced at `hits` first-stage hits each:
     (net, target_scale, seconds spent tracing, seconds spent training)."""
     import time
@@ -395,7 +396,7 @@ def fit(tracer: FieldTracer, n_traces: int, hits: int, steps: int, seed: int = 1
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     net = Mlp(tracer.api, dims=dims, seed=seed)
-    scale, _ = train(net, x, t, steps=steps, batch=batch, lr=lr)
+    scale, _ = train(net, x, t, steps=steps, batch=batch, lr=lr, lr_final=lr_final)
     torch.cuda.synchronize()
     return net, scale, t1 - t0, time.perf_counter() - t1
 
