@@ -222,7 +222,7 @@ def reference_positions(scene_list, seconds: float, seed: int, label: str):
 
 
 def config_lines(api, args) -> dict:
-    """The other BASELINE configurations, each timed beside the reference on the host cores:
+    """The other benchmark configurations, each timed beside the reference on the host cores:
     C1 dish (FP64, 1e6 hits, 50 x 50 absorber map), C2 trough (FP64 and mixed, 1e7 hits,
     72 x 120 absorber-tube map), C4 batched annual beam-down trace (512 sun positions, tracking
     field of 10,000 heliostats, 64 x 64 ground map, one st_b200_sim_run_batch call), the
