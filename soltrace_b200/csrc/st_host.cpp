@@ -1740,10 +1740,10 @@ bool build_position(const Context *cx, const HostScene &hs, const double sun_xyz
     out.cell_xb.swap(h.cell_xb);
     out.cell_xc.swap(h.cell_xc);
     if (target) {
-        out.elems = hs.elems;
         const StageRec &sr = hs.dev.stages[0];
+        out.rot.resize(size_t(sr.n_elem) * 9);
         for (int k = 0; k < sr.n_elem; ++k)
-            for (int q = 0; q < 9; ++q) out.elems[size_t(sr.first_elem + k)].R[q] = st0.elems[size_t(k)].R[q];
+            for (int q = 0; q < 9; ++q) out.rot[size_t(k) * 9 + q] = st0.elems[size_t(k)].R[q];
     }
     return true;
 }

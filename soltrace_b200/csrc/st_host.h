@@ -100,7 +100,8 @@ struct SunPosition {
     SunDev sun;                       // device pointers are filled by gpu_run_batch
     std::vector<int> cell_start;
     std::vector<float4> cell_disc, cell_par, cell_xa, cell_xb, cell_xc;
-    std::vector<ElemRec> elems;       // empty: the scene's elements
+    std::vector<double> rot;          // tracking: the first stage's re-aimed rotations, 9 per element
+                                      // (empty: the scene's elements as they are)
     uint64_t n_hits = 0;
     uint32_t seed = 0;
 };

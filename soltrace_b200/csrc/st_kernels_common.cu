@@ -124,6 +124,16 @@ static uint32_t rec_blocks(unsigned long long n) {
 void launch_rec_count(const RecOrder &o, cudaStream_t st) { k_rec_count<<<rec_blocks(o.n), 256, 0, st>>>(o); }
 void launch_rec_scatter(const RecOrder &o, cudaStream_t st) { k_rec_scatter<<<rec_blocks(o.n), 256, 0, st>>>(o); }
 
+__global__ void __launch_bounds__(256) k_set_rotations(ElemRec *el, uint32_t n, const double *rot) {
+    const uint32_t i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) el[i].R[q] = rot[size_t(i) * 9 + q];
+}
+void launch_set_rotations(ElemRec *el, uint32_t n, const double *rot, cudaStream_t st) {
+    if (n) k_set_rotations<<<(n + 255) / 256, 256, 0, st>>>(el, n, rot);
+}
+
 void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uint32_t *counts,
                     const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st) {
     const uint32_t nb = (n + kProbeBlock - 1) / kProbeBlock;

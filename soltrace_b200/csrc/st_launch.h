@@ -222,6 +222,9 @@ struct RecOrder {
 };
 void launch_rec_count(const RecOrder &o, cudaStream_t st);
 void launch_rec_scatter(const RecOrder &o, cudaStream_t st);
+// batched runs with tracking: element e of `el` (n elements) takes the stage -> element
+// rotation rot[9e .. 9e + 8]
+void launch_set_rotations(ElemRec *el, uint32_t n, const double *rot, cudaStream_t st);
 
 void launch_compact(uint64_t s0, uint32_t n, const uint32_t *hit_elem, const uint32_t *counts,
                     const uint32_t *offsets, uint64_t *hit_sid, uint32_t *hit_el, cudaStream_t st);

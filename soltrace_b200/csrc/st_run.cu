@@ -99,7 +99,7 @@ struct Workspace {
     size_t rec_host_bytes = 0;
     bool rec_host_pinned = false;
     // batched runs: per-position sun tables, element copies, run states, counters, accumulators
-    DevBuf pos_cells, pos_disc, pos_par, pos_xa, pos_xb, pos_xc, pos_elems, pos_rs, pos_ctr, pos_acc;
+    DevBuf pos_cells, pos_disc, pos_par, pos_xa, pos_xb, pos_xc, pos_elems, pos_rot, pos_rs, pos_ctr, pos_acc;
     DevBuf cell_xa, cell_xb, cell_xc;  // exact flat footprints of the sun-plane grid
     std::vector<cudaEvent_t> events;
     // autotuned kernel variants per precision (FP64, mixed), chosen on the first run
@@ -1080,19 +1080,26 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
     CK(upload(ws.inv_cdf, hs.inv_cdf, st, h2d));
     // every position's tables, laid end to end on the device: sized first, then each position's
     // arrays copied straight from its own vectors (no host-side concatenation)
-    std::vector<size_t> off_cells(K), off_disc(K), off_elems(K);
+    std::vector<size_t> off_cells(K), off_disc(K), off_elems(K), off_rot(K);
     bool all_exact = true;
     for (const SunPosition &sp : pos)
         if (!sp.sun.exact_flat || sp.cell_xa.size() != sp.cell_disc.size() || sp.cell_xa.empty()) all_exact = false;
-    size_t n_cells = 0, n_disc = 0, n_elems = 0;
+    const size_t n_elem_all = hs.elems.size(), n_first = size_t(hs.dev.stages[0].n_elem);
+    size_t n_cells = 0, n_disc = 0, n_elems = 0, n_rot = 0;
     for (size_t p = 0; p < K; ++p) {
         const SunPosition &sp = pos[p];
+        if (!sp.rot.empty() && sp.rot.size() != n_first * 9) {
+            out.error = "sun position " + std::to_string(p) + ": rotations do not match the first stage";
+            return false;
+        }
         off_cells[p] = n_cells;
         n_cells += sp.cell_start.size();
         off_disc[p] = n_disc;
         n_disc += sp.cell_disc.size();
-        off_elems[p] = sp.elems.empty() ? size_t(-1) : n_elems;
-        n_elems += sp.elems.size();
+        off_elems[p] = sp.rot.empty() ? size_t(-1) : n_elems;  // a re-aimed copy of the element table
+        n_elems += sp.rot.empty() ? 0 : n_elem_all;
+        off_rot[p] = n_rot;
+        n_rot += sp.rot.size();
     }
     CK(ws.pos_cells.ensure(std::max<size_t>(n_cells * sizeof(int), 16)));
     CK(ws.pos_disc.ensure(std::max<size_t>(n_disc * sizeof(float4), 16)));
@@ -1103,6 +1110,7 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
         CK(ws.pos_xc.ensure(std::max<size_t>(n_disc * sizeof(float4), 16)));
     }
     CK(ws.pos_elems.ensure(std::max<size_t>(n_elems * sizeof(ElemRec), 16)));
+    CK(ws.pos_rot.ensure(std::max<size_t>(n_rot * sizeof(double), 16)));
     auto put = [&](DevBuf &dst, size_t off_elems_of_t, const void *src, size_t bytes) -> cudaError_t {
         if (!bytes) return cudaSuccess;
         h2d += bytes;
@@ -1119,8 +1127,16 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
             CK(put(ws.pos_xb, od, sp.cell_xb.data(), nd));
             CK(put(ws.pos_xc, od, sp.cell_xc.data(), nd));
         }
-        if (!sp.elems.empty())
-            CK(put(ws.pos_elems, off_elems[p] * sizeof(ElemRec), sp.elems.data(), sp.elems.size() * sizeof(ElemRec)));
+        if (!sp.rot.empty()) {
+            // the scene's element table (already on the device) copied, then the re-aimed
+            // rotations of the first stage written over it: 72 bytes per heliostat cross PCIe
+            // instead of the whole element record
+            ElemRec *el = ws.pos_elems.as<ElemRec>() + off_elems[p];
+            CK(put(ws.pos_rot, off_rot[p] * sizeof(double), sp.rot.data(), sp.rot.size() * sizeof(double)));
+            CK(cudaMemcpyAsync(el, ws.elems.p, n_elem_all * sizeof(ElemRec), cudaMemcpyDeviceToDevice, st));
+            launch_set_rotations(el + hs.dev.stages[0].first_elem, uint32_t(n_first), ws.pos_rot.as<double>() + off_rot[p], st);
+            ++out.gpu_launches;
+        }
     }
 
     SceneDev S0 = hs.dev;
