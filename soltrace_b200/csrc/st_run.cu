@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <thread>
 
 #include "st_host.h"
 #include "st_launch.h"
@@ -95,6 +96,8 @@ struct Workspace {
     DevBuf ecount, ecursor, etotal, s_hits;  // the batch's hits sorted by first-stage element (HitRec)
     // record ordering: key counts / slots, scan partials, per-stage counts, merge runs, columns
     DevBuf rec_key, rec_parts, rec_parts2, rec_stage, rec_runs, rec_cols, rec_bad;
+    void *pos_host = nullptr;  // batched runs: the positions' tables gathered in page-locked memory
+    size_t pos_host_bytes = 0;
     void *rec_host = nullptr;  // the ordered records' columns in host memory (pinned when possible)
     size_t rec_host_bytes = 0;
     bool rec_host_pinned = false;
@@ -110,6 +113,7 @@ struct Workspace {
     DevBuf tune_rs;
     ~Workspace() {
         if (device >= 0) cudaSetDevice(device);
+        if (pos_host) cudaFreeHost(pos_host);
         if (rec_host) {
             if (rec_host_pinned)
                 cudaFreeHost(rec_host);
@@ -1116,23 +1120,83 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
         h2d += bytes;
         return cudaMemcpyAsync(static_cast<char *>(dst.p) + off_elems_of_t, src, bytes, cudaMemcpyHostToDevice, st);
     };
+    // The positions' tables are gathered on all host cores into page-locked memory laid out as
+    // on the device (one region per array, positions end to end), then copied with one DMA per
+    // array at page-locked speed; when page-locked memory cannot be had, each position's
+    // arrays are copied from its own vectors instead.
+    const size_t nx = all_exact ? 3 : 0;
+    const size_t b_cells = n_cells * sizeof(int), b_disc = n_disc * sizeof(float4), b_rot = n_rot * sizeof(double);
+    const size_t b_all = b_cells + (2 + nx) * b_disc + b_rot;
+    CK(cudaStreamSynchronize(st));  // no copy out of the staging area is still in flight
+    if (ws.pos_host_bytes < b_all) {
+        if (ws.pos_host) cudaFreeHost(ws.pos_host);
+        ws.pos_host = nullptr;
+        ws.pos_host_bytes = 0;
+        const size_t want = b_all + b_all / 4;
+        if (cudaMallocHost(&ws.pos_host, want) == cudaSuccess) {
+            ws.pos_host_bytes = want;
+        } else {
+            ws.pos_host = nullptr;
+            cudaGetLastError();  // clear the failed allocation's error; the vectors are copied instead
+        }
+    }
+    const bool staged = ws.pos_host != nullptr && b_all > 0;
+    if (staged) {
+        char *r_cells = static_cast<char *>(ws.pos_host), *r_disc = r_cells + b_cells, *r_par = r_disc + b_disc;
+        char *r_xa = r_par + b_disc, *r_xb = r_xa + (nx ? b_disc : 0), *r_xc = r_xb + (nx ? b_disc : 0);
+        char *r_rot = r_xc + (nx ? b_disc : 0);
+        auto cp = [](char *dst, const void *src, size_t bytes) {
+            if (bytes) memcpy(dst, src, bytes);
+        };
+        auto gather = [&](size_t p) {
+            const SunPosition &sp = pos[p];
+            const size_t od = off_disc[p] * sizeof(float4), nd = sp.cell_disc.size() * sizeof(float4);
+            cp(r_cells + off_cells[p] * sizeof(int), sp.cell_start.data(), sp.cell_start.size() * sizeof(int));
+            cp(r_disc + od, sp.cell_disc.data(), nd);
+            cp(r_par + od, sp.cell_par.data(), sp.cell_par.size() * sizeof(float4));
+            if (nx) {
+                cp(r_xa + od, sp.cell_xa.data(), nd);
+                cp(r_xb + od, sp.cell_xb.data(), nd);
+                cp(r_xc + od, sp.cell_xc.data(), nd);
+            }
+            cp(r_rot + off_rot[p] * sizeof(double), sp.rot.data(), sp.rot.size() * sizeof(double));
+        };
+        const size_t nth = std::max<size_t>(1, std::min<size_t>(K, std::thread::hardware_concurrency()));
+        std::vector<std::thread> th;
+        for (size_t t = 0; t < nth; ++t)
+            th.emplace_back([&gather, t, nth, K]() {
+                for (size_t p = t; p < K; p += nth) gather(p);
+            });
+        for (auto &x : th) x.join();
+        CK(put(ws.pos_cells, 0, r_cells, b_cells));
+        CK(put(ws.pos_disc, 0, r_disc, b_disc));
+        CK(put(ws.pos_par, 0, r_par, b_disc));
+        if (nx) {
+            CK(put(ws.pos_xa, 0, r_xa, b_disc));
+            CK(put(ws.pos_xb, 0, r_xb, b_disc));
+            CK(put(ws.pos_xc, 0, r_xc, b_disc));
+        }
+        CK(put(ws.pos_rot, 0, r_rot, b_rot));
+    }
     for (size_t p = 0; p < K; ++p) {
         const SunPosition &sp = pos[p];
-        CK(put(ws.pos_cells, off_cells[p] * sizeof(int), sp.cell_start.data(), sp.cell_start.size() * sizeof(int)));
-        const size_t od = off_disc[p] * sizeof(float4), nd = sp.cell_disc.size() * sizeof(float4);
-        CK(put(ws.pos_disc, od, sp.cell_disc.data(), nd));
-        CK(put(ws.pos_par, od, sp.cell_par.data(), sp.cell_par.size() * sizeof(float4)));
-        if (all_exact) {
-            CK(put(ws.pos_xa, od, sp.cell_xa.data(), nd));
-            CK(put(ws.pos_xb, od, sp.cell_xb.data(), nd));
-            CK(put(ws.pos_xc, od, sp.cell_xc.data(), nd));
+        if (!staged) {
+            CK(put(ws.pos_cells, off_cells[p] * sizeof(int), sp.cell_start.data(), sp.cell_start.size() * sizeof(int)));
+            const size_t od = off_disc[p] * sizeof(float4), nd = sp.cell_disc.size() * sizeof(float4);
+            CK(put(ws.pos_disc, od, sp.cell_disc.data(), nd));
+            CK(put(ws.pos_par, od, sp.cell_par.data(), sp.cell_par.size() * sizeof(float4)));
+            if (all_exact) {
+                CK(put(ws.pos_xa, od, sp.cell_xa.data(), nd));
+                CK(put(ws.pos_xb, od, sp.cell_xb.data(), nd));
+                CK(put(ws.pos_xc, od, sp.cell_xc.data(), nd));
+            }
+            CK(put(ws.pos_rot, off_rot[p] * sizeof(double), sp.rot.data(), sp.rot.size() * sizeof(double)));
         }
         if (!sp.rot.empty()) {
             // the scene's element table (already on the device) copied, then the re-aimed
             // rotations of the first stage written over it: 72 bytes per heliostat cross PCIe
             // instead of the whole element record
             ElemRec *el = ws.pos_elems.as<ElemRec>() + off_elems[p];
-            CK(put(ws.pos_rot, off_rot[p] * sizeof(double), sp.rot.data(), sp.rot.size() * sizeof(double)));
             CK(cudaMemcpyAsync(el, ws.elems.p, n_elem_all * sizeof(ElemRec), cudaMemcpyDeviceToDevice, st));
             launch_set_rotations(el + hs.dev.stages[0].first_elem, uint32_t(n_first), ws.pos_rot.as<double>() + off_rot[p], st);
             ++out.gpu_launches;
