@@ -285,9 +285,9 @@ def config_lines(api, args) -> dict:
     api.st_b200_set_precision(ctx, 1)
     api.st_b200_add_flux_map(ctx, *scenes.GROUND_MAP)
     tgt = scenes.beam_down_target()
-    # warm-up: one full chunk (64 positions spread over the year, a tenth of their hits), so the
-    # timed call finds its device buffers and page-locked staging area already sized
-    api.run_batch(ctx, 100, suns[::8], hits[::8] // 10, tgt)
+    # warm-up: two full chunks (128 positions spread over the year, a tenth of their hits), so
+    # the timed call finds its device buffers and both page-locked staging areas already sized
+    api.run_batch(ctx, 100, suns[::4], hits[::4] // 10, tgt)
     t0 = time.perf_counter()
     rc = api.run_batch(ctx, 100, suns, hits, tgt)
     wall = time.perf_counter() - t0

@@ -193,8 +193,9 @@ int st_b200_set_ranks(st_context_t pcxt, int rank, int nranks, st_b200_allgather
  * stage aimed for sun k).  Precision and flux maps (st_b200_add_flux_map, kept per position)
  * come from the context; records are not built.  The host reads the positions' progress
  * once per wave (a few times per call), not once per position.  Positions go to the device
- * in chunks of 64 through a page-locked staging area that the context keeps (sized for its
- * largest chunk) until st_free_context.  Returns 1, or -1 with the reason in st_message(). */
+ * in chunks of 64 through two page-locked staging areas that the context keeps (each sized
+ * for its largest chunk: a chunk is staged while the previous one runs) until
+ * st_free_context.  Returns 1, or -1 with the reason in st_message(). */
 int st_b200_sim_run_batch(st_context_t pcxt, unsigned int seed, int n_positions, const double *sun_xyz,
                           const st_uint_t *hits, const double *track_target);
 /* Results of the last batched run.  position >= 0: that position's SunRayCount, hits, stage

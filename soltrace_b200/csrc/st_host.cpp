@@ -1802,6 +1802,10 @@ int run_batch(Context *cx, unsigned seed, int n_pos, const double *sun_xyz, cons
         return true;
     };
     if (!cx->ws) cx->ws = workspace_create();
+    if (!workspace_bind(*cx->ws, rq.device)) {
+        cx->log("st_b200_sim_run_batch: cannot use CUDA device %d", rq.device);
+        return -1;
+    }
     double host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     BatchResult tot;
     std::vector<SunPosition> cur, nxt;
@@ -1811,15 +1815,20 @@ int run_batch(Context *cx, unsigned seed, int n_pos, const double *sun_xyz, cons
         cx->log("st_b200_sim_run_batch: %s", err.c_str());
         return -1;
     }
+    int slot = 0;  // the staging area holding `cur`; the next chunk is staged in the other
+    stage_positions(*cx->ws, slot, cur, rq.device);
     host_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb).count();
     for (size_t a = 0; a < np; a += kBatchChunk) {
         const size_t b = std::min(np, a + kBatchChunk);
         bool next_ok = true;
         std::thread builder;
         if (b < np)
-            builder = std::thread([&]() { next_ok = build_chunk(b, std::min(np, b + kBatchChunk), nxt, err_next); });
+            builder = std::thread([&]() {
+                next_ok = build_chunk(b, std::min(np, b + kBatchChunk), nxt, err_next);
+                if (next_ok) stage_positions(*cx->ws, slot ^ 1, nxt, rq.device);
+            });
         BatchResult br;
-        const bool ran = gpu_run_batch(hs, cur, rq, br, *cx->ws);
+        const bool ran = gpu_run_batch(hs, cur, rq, br, *cx->ws, slot);
         if (builder.joinable()) builder.join();
         if (!ran) {
             cx->log("%s", br.error.c_str());
@@ -1843,6 +1852,7 @@ int run_batch(Context *cx, unsigned seed, int n_pos, const double *sun_xyz, cons
         tot.probe_variant = br.probe_variant;
         cur.swap(nxt);
         nxt.clear();
+        slot ^= 1;
     }
     BatchResult &br = tot;
     cx->batch.swap(br.pos);

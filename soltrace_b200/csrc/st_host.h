@@ -131,8 +131,18 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
 // K sun positions over one scene in one launch sequence: every position's sun-ray batches
 // are queued without a host round trip, the host reading the positions' progress once per
 // wave.  rq supplies precision, device, flux maps and the sun-ray cap per position.
+// `slot`: the staging area (0 or 1) that stage_positions filled with `pos`, -1 for none.
 bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, const RunRequest &rq, BatchResult &out,
-                   Workspace &ws);
+                   Workspace &ws, int slot);
+// Binds a workspace to a device (a workspace bound to another is started afresh) and gives it
+// its stream; called before positions are staged into it.
+bool workspace_bind(Workspace &ws, int device);
+// Gathers the positions' sun-plane tables and tracking rotations, on all host cores, into the
+// workspace's page-locked staging area `slot` (0 or 1), laid out as gpu_run_batch copies them
+// to the device, so that a chunk is staged while the device runs the previous one.  false
+// (nothing staged; gpu_run_batch then copies from the vectors) when page-locked memory cannot
+// be had or the workspace is not bound to `device`.
+bool stage_positions(Workspace &ws, int slot, const std::vector<SunPosition> &pos, int device);
 
 // st_host.cpp: set up and flatten the scene of a context; append a message to it
 bool prepare_scene(void *ctx, HostScene &hs);

@@ -96,8 +96,12 @@ struct Workspace {
     DevBuf ecount, ecursor, etotal, s_hits;  // the batch's hits sorted by first-stage element (HitRec)
     // record ordering: key counts / slots, scan partials, per-stage counts, merge runs, columns
     DevBuf rec_key, rec_parts, rec_parts2, rec_stage, rec_runs, rec_cols, rec_bad;
-    void *pos_host = nullptr;  // batched runs: the positions' tables gathered in page-locked memory
-    size_t pos_host_bytes = 0;
+    // batched runs: two page-locked staging areas, the positions' tables of a chunk gathered
+    // in one while the device runs the chunk staged in the other
+    void *pos_host[2] = {nullptr, nullptr};
+    size_t pos_host_bytes[2] = {0, 0};
+    size_t pos_staged_bytes[2] = {0, 0}, pos_staged_k[2] = {0, 0};  // what each area holds
+    bool pos_dma_pending[2] = {false, false};  // a copy out of the area may still be running
     void *rec_host = nullptr;  // the ordered records' columns in host memory (pinned when possible)
     size_t rec_host_bytes = 0;
     bool rec_host_pinned = false;
@@ -113,7 +117,8 @@ struct Workspace {
     DevBuf tune_rs;
     ~Workspace() {
         if (device >= 0) cudaSetDevice(device);
-        if (pos_host) cudaFreeHost(pos_host);
+        for (int k = 0; k < 2; ++k)
+            if (pos_host[k]) cudaFreeHost(pos_host[k]);
         if (rec_host) {
             if (rec_host_pinned)
                 cudaFreeHost(rec_host);
@@ -1044,8 +1049,112 @@ bool gpu_run(const HostScene &hs, const RunRequest &rq, RunResult &out, Workspac
 // in waves: a wave queues, for every position still short of its hits, the sun rays its hit
 // rate (measured by the previous wave; the first wave probes 2^20 rays) says it needs, with
 // no host round trip inside the wave; the host then reads all positions' run states at once.
+namespace {
+// Where a chunk's positions sit in the device tables (and in a staging area laid out the
+// same way: one region per array, positions end to end).
+struct PosLayout {
+    std::vector<size_t> off_cells, off_disc, off_rot;
+    size_t n_cells = 0, n_disc = 0, n_rot = 0;
+    bool all_exact = true;
+    size_t b_cells = 0, b_disc = 0, b_rot = 0, nx = 0, b_all = 0;
+    explicit PosLayout(const std::vector<SunPosition> &pos) : off_cells(pos.size()), off_disc(pos.size()),
+                                                              off_rot(pos.size()) {
+        for (const SunPosition &sp : pos)
+            if (!sp.sun.exact_flat || sp.cell_xa.size() != sp.cell_disc.size() || sp.cell_xa.empty()) all_exact = false;
+        for (size_t p = 0; p < pos.size(); ++p) {
+            off_cells[p] = n_cells;
+            n_cells += pos[p].cell_start.size();
+            off_disc[p] = n_disc;
+            n_disc += pos[p].cell_disc.size();
+            off_rot[p] = n_rot;
+            n_rot += pos[p].rot.size();
+        }
+        nx = all_exact ? 3 : 0;
+        b_cells = n_cells * sizeof(int);
+        b_disc = n_disc * sizeof(float4);
+        b_rot = n_rot * sizeof(double);
+        b_all = b_cells + (2 + nx) * b_disc + b_rot;
+    }
+    // region starts in a staging area: cells, disc, par, xa, xb, xc, rot
+    void regions(char *base, char *r[7]) const {
+        r[0] = base;
+        r[1] = r[0] + b_cells;
+        r[2] = r[1] + b_disc;
+        r[3] = r[2] + b_disc;
+        r[4] = r[3] + (nx ? b_disc : 0);
+        r[5] = r[4] + (nx ? b_disc : 0);
+        r[6] = r[5] + (nx ? b_disc : 0);
+    }
+};
+}  // namespace
+
+bool workspace_bind(Workspace &ws, int device) {
+    if (cudaSetDevice(device) != cudaSuccess) return false;
+    if (ws.device != device) {  // a workspace serves one device: start afresh on another
+        ws.~Workspace();
+        new (&ws) Workspace();
+        ws.device = device;
+    }
+    return ws.stream || cudaStreamCreateWithFlags(&ws.stream, cudaStreamNonBlocking) == cudaSuccess;
+}
+
+bool stage_positions(Workspace &ws, int slot, const std::vector<SunPosition> &pos, int device) {
+    if (slot < 0 || slot > 1) return false;
+    ws.pos_staged_bytes[slot] = ws.pos_staged_k[slot] = 0;
+    const PosLayout L(pos);
+    // only into a workspace already bound to the device (workspace_bind), which the batch
+    // run will not start afresh
+    if (L.b_all == 0 || ws.device != device || cudaSetDevice(device) != cudaSuccess) return false;
+    if (ws.pos_dma_pending[slot] && ws.stream) {  // a run that failed may have left its copy running
+        cudaStreamSynchronize(ws.stream);
+        cudaGetLastError();
+        ws.pos_dma_pending[slot] = false;
+    }
+    if (ws.pos_host_bytes[slot] < L.b_all) {
+        if (ws.pos_host[slot]) cudaFreeHost(ws.pos_host[slot]);
+        ws.pos_host[slot] = nullptr;
+        ws.pos_host_bytes[slot] = 0;
+        const size_t want = L.b_all + L.b_all / 4;
+        if (cudaMallocHost(&ws.pos_host[slot], want) != cudaSuccess) {
+            ws.pos_host[slot] = nullptr;
+            cudaGetLastError();  // the vectors are copied instead
+            return false;
+        }
+        ws.pos_host_bytes[slot] = want;
+    }
+    char *r[7];
+    L.regions(static_cast<char *>(ws.pos_host[slot]), r);
+    auto cp = [](char *dst, const void *src, size_t bytes) {
+        if (bytes) memcpy(dst, src, bytes);
+    };
+    auto gather = [&](size_t p) {
+        const SunPosition &sp = pos[p];
+        const size_t od = L.off_disc[p] * sizeof(float4), nd = sp.cell_disc.size() * sizeof(float4);
+        cp(r[0] + L.off_cells[p] * sizeof(int), sp.cell_start.data(), sp.cell_start.size() * sizeof(int));
+        cp(r[1] + od, sp.cell_disc.data(), nd);
+        cp(r[2] + od, sp.cell_par.data(), sp.cell_par.size() * sizeof(float4));
+        if (L.nx) {
+            cp(r[3] + od, sp.cell_xa.data(), nd);
+            cp(r[4] + od, sp.cell_xb.data(), nd);
+            cp(r[5] + od, sp.cell_xc.data(), nd);
+        }
+        cp(r[6] + L.off_rot[p] * sizeof(double), sp.rot.data(), sp.rot.size() * sizeof(double));
+    };
+    const size_t K = pos.size();
+    const size_t nth = std::max<size_t>(1, std::min<size_t>(K, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (size_t t = 0; t < nth; ++t)
+        th.emplace_back([&gather, t, nth, K]() {
+            for (size_t p = t; p < K; p += nth) gather(p);
+        });
+    for (auto &x : th) x.join();
+    ws.pos_staged_bytes[slot] = L.b_all;
+    ws.pos_staged_k[slot] = K;
+    return true;
+}
+
 bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, const RunRequest &rq, BatchResult &out,
-                   Workspace &ws) {
+                   Workspace &ws, int slot) {
     const auto t_setup = std::chrono::steady_clock::now();
     const size_t K = pos.size();
     int ndev = 0;
@@ -1120,63 +1229,25 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
         h2d += bytes;
         return cudaMemcpyAsync(static_cast<char *>(dst.p) + off_elems_of_t, src, bytes, cudaMemcpyHostToDevice, st);
     };
-    // The positions' tables are gathered on all host cores into page-locked memory laid out as
-    // on the device (one region per array, positions end to end), then copied with one DMA per
-    // array at page-locked speed; when page-locked memory cannot be had, each position's
-    // arrays are copied from its own vectors instead.
-    const size_t nx = all_exact ? 3 : 0;
-    const size_t b_cells = n_cells * sizeof(int), b_disc = n_disc * sizeof(float4), b_rot = n_rot * sizeof(double);
-    const size_t b_all = b_cells + (2 + nx) * b_disc + b_rot;
-    CK(cudaStreamSynchronize(st));  // no copy out of the staging area is still in flight
-    if (ws.pos_host_bytes < b_all) {
-        if (ws.pos_host) cudaFreeHost(ws.pos_host);
-        ws.pos_host = nullptr;
-        ws.pos_host_bytes = 0;
-        const size_t want = b_all + b_all / 4;
-        if (cudaMallocHost(&ws.pos_host, want) == cudaSuccess) {
-            ws.pos_host_bytes = want;
-        } else {
-            ws.pos_host = nullptr;
-            cudaGetLastError();  // clear the failed allocation's error; the vectors are copied instead
-        }
-    }
-    const bool staged = ws.pos_host != nullptr && b_all > 0;
+    // The positions' tables, staged by stage_positions in page-locked memory laid out as on the
+    // device, go over with one copy per array; otherwise each position's arrays are copied from
+    // its own vectors.
+    const PosLayout L(pos);
+    const bool staged = slot >= 0 && slot <= 1 && ws.pos_host[slot] && ws.pos_staged_k[slot] == K &&
+                        ws.pos_staged_bytes[slot] == L.b_all && L.b_all > 0 && L.all_exact == all_exact;
     if (staged) {
-        char *r_cells = static_cast<char *>(ws.pos_host), *r_disc = r_cells + b_cells, *r_par = r_disc + b_disc;
-        char *r_xa = r_par + b_disc, *r_xb = r_xa + (nx ? b_disc : 0), *r_xc = r_xb + (nx ? b_disc : 0);
-        char *r_rot = r_xc + (nx ? b_disc : 0);
-        auto cp = [](char *dst, const void *src, size_t bytes) {
-            if (bytes) memcpy(dst, src, bytes);
-        };
-        auto gather = [&](size_t p) {
-            const SunPosition &sp = pos[p];
-            const size_t od = off_disc[p] * sizeof(float4), nd = sp.cell_disc.size() * sizeof(float4);
-            cp(r_cells + off_cells[p] * sizeof(int), sp.cell_start.data(), sp.cell_start.size() * sizeof(int));
-            cp(r_disc + od, sp.cell_disc.data(), nd);
-            cp(r_par + od, sp.cell_par.data(), sp.cell_par.size() * sizeof(float4));
-            if (nx) {
-                cp(r_xa + od, sp.cell_xa.data(), nd);
-                cp(r_xb + od, sp.cell_xb.data(), nd);
-                cp(r_xc + od, sp.cell_xc.data(), nd);
-            }
-            cp(r_rot + off_rot[p] * sizeof(double), sp.rot.data(), sp.rot.size() * sizeof(double));
-        };
-        const size_t nth = std::max<size_t>(1, std::min<size_t>(K, std::thread::hardware_concurrency()));
-        std::vector<std::thread> th;
-        for (size_t t = 0; t < nth; ++t)
-            th.emplace_back([&gather, t, nth, K]() {
-                for (size_t p = t; p < K; p += nth) gather(p);
-            });
-        for (auto &x : th) x.join();
-        CK(put(ws.pos_cells, 0, r_cells, b_cells));
-        CK(put(ws.pos_disc, 0, r_disc, b_disc));
-        CK(put(ws.pos_par, 0, r_par, b_disc));
-        if (nx) {
-            CK(put(ws.pos_xa, 0, r_xa, b_disc));
-            CK(put(ws.pos_xb, 0, r_xb, b_disc));
-            CK(put(ws.pos_xc, 0, r_xc, b_disc));
+        char *r[7];
+        L.regions(static_cast<char *>(ws.pos_host[slot]), r);
+        ws.pos_dma_pending[slot] = true;
+        CK(put(ws.pos_cells, 0, r[0], L.b_cells));
+        CK(put(ws.pos_disc, 0, r[1], L.b_disc));
+        CK(put(ws.pos_par, 0, r[2], L.b_disc));
+        if (L.nx) {
+            CK(put(ws.pos_xa, 0, r[3], L.b_disc));
+            CK(put(ws.pos_xb, 0, r[4], L.b_disc));
+            CK(put(ws.pos_xc, 0, r[5], L.b_disc));
         }
-        CK(put(ws.pos_rot, 0, r_rot, b_rot));
+        CK(put(ws.pos_rot, 0, r[6], L.b_rot));
     }
     for (size_t p = 0; p < K; ++p) {
         const SunPosition &sp = pos[p];
@@ -1434,6 +1505,7 @@ bool gpu_run_batch(const HostScene &hs, const std::vector<SunPosition> &pos, con
     CK(cudaMemcpyAsync(accv.data(), ws.pos_acc.p, K * acc_n * 8, cudaMemcpyDeviceToHost, st));
     out.d2h_bytes += K * (sizeof(RunCounters) + acc_n * 8);
     CK(cudaStreamSynchronize(st));
+    if (slot >= 0 && slot <= 1) ws.pos_dma_pending[slot] = false;
     out.pos.assign(K, PositionResult());
     for (size_t p = 0; p < K; ++p) {
         PositionResult &r = out.pos[p];

@@ -102,3 +102,40 @@ def test_batch_zero_budget_and_repeat(product):
         np.testing.assert_array_equal(out[0][2], out[1][2])
     finally:
         product.st_free_context(ctx)
+
+
+def test_batch_over_several_chunks_equals_separate_calls(product):
+    """150 positions go to the device in three chunks, each staged (page-locked, on the host
+    cores) while the device runs the previous one; every position must equal the same position
+    run in a call of its own chunk-sized slice (seed offset so that it keeps its streams)."""
+    n = 150
+    suns, _, _ = scenes.annual_suns(n, seed=5)
+    hits = [1500 + 37 * (k % 11) for k in range(n)]
+    seed = 70
+    sc = scenes.beam_down_scene(N_HELIO, raycount=1000)
+    target = scenes.beam_down_target()
+
+    def run(ctx, a, b):
+        assert product.run_batch(ctx, seed + a, suns[a:b], hits[a:b], target) == 1, product.messages(ctx)
+        return [(product.batch_stats(ctx, k), product.batch_flux(ctx, 0, k, GM[3], GM[4]),
+                 product.batch_absorbed(ctx, k, 1, N_HELIO)) for k in range(b - a)]
+
+    ctxs = []
+    try:
+        for _ in range(2):
+            ctx = product.st_create_context()
+            ctxs.append(ctx)
+            scenes.push(product, ctx, sc)
+            product.st_b200_set_precision(ctx, 1)
+            product.st_b200_add_flux_map(ctx, *GM)
+        whole = run(ctxs[0], 0, n)
+        parts = run(ctxs[1], 0, 50) + run(ctxs[1], 50, 100) + run(ctxs[1], 100, n)
+        for k in range(n):
+            (bw, fw, aw), (bp, fp, ap) = whole[k], parts[k]
+            for key in ("sun_rays", "ray_hits", "ray_stage_units", "intersections"):
+                assert bw[key] == bp[key], (k, key)
+            np.testing.assert_array_equal(fw, fp)
+            np.testing.assert_array_equal(aw, ap)
+    finally:
+        for ctx in ctxs:
+            product.st_free_context(ctx)
