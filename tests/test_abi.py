@@ -130,6 +130,9 @@ def test_run_without_gpu_fails_loudly(product):
     scenes.push(product, ctx, scenes.dish_scene(100))
     assert product.run(ctx, 1) == -1
     assert any("CUDA" in m for m in product.messages(ctx))
+    # the batched entry point too, before it stages anything
+    assert product.run_batch(ctx, 1, np.array([[0.0, 0.0, 100.0], [0.0, 50.0, 100.0]]), [10, 10]) == -1
+    assert "CUDA" in product.messages(ctx)[-1]
     product.st_free_context(ctx)
 
 
