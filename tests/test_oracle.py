@@ -94,3 +94,19 @@ def test_oracle_philox_stream_is_per_ray(oracle):
         mb = (rb["stage"] == s) & (rb["raynum"] <= 200)
         for k in ("x", "y", "z", "element", "raynum"):
             np.testing.assert_array_equal(np.sort(ra[k][ma]), np.sort(rb[k][mb]))
+
+
+@pytest.mark.parametrize("sun_elev_az", [None, (30.0, 120.0)])
+def test_oracle_matches_reference_on_beam_down(oracle, reference, sun_elev_az):
+    """The batched study's geometry (heliostats aimed at the upper focus of a convex
+    hyperboloid secondary with an absorbing torus lip, ground receiver under the lower focus),
+    at 300 heliostats: records bit for bit, with rays on the lip and on the ground."""
+    sun = None if sun_elev_az is None else scenes.sun_vector(*sun_elev_az)
+    sc = scenes.beam_down_scene(300, raycount=3000, sun_xyz=sun)
+    a = run_scene(reference, sc, 5)
+    b = run_scene(oracle, sc, 5, lambda x, c: x.st_oracle_set_rng(c, 0))
+    assert a[0] == b[0] > 0 and a[2] == b[2]
+    assert records_digest(a[1]) == records_digest(b[1])
+    rec = a[1]
+    assert np.sum((rec["stage"] == 2) & (np.abs(rec["element"]) == 2)) > 0  # the torus lip
+    assert np.sum((rec["stage"] == 3) & (rec["element"] < 0)) > 0           # absorbed on the ground
