@@ -36,6 +36,8 @@ def _bench_scenes():
         "bench_dish": scenes.dish_scene(20000),
         "bench_trough": scenes.trough_scene(20000),
         "bench_field300": scenes.field_scene(300, 20000, dynamic_group=False),
+        # the batched study's geometry: hyperboloid secondary, torus lip, ground receiver
+        "bench_beam_down300": scenes.beam_down_scene(300, raycount=3000),
     }
 
 
@@ -57,6 +59,19 @@ def test_fp64_matches_oracle_ray_by_ray(product, oracle, zoo_scenes, name):
     # device and the host library; the Newton iteration on it then stops a step earlier or
     # later within its 1e-6 relative tolerance
     tol = 1e-7 if name == "fe_surface" else 1e-9
+    if name == "bench_beam_down300":
+        # The torus lip's quartic has coefficients built from pow(x, 4) terms of the ray's
+        # start relative to the tube; with the start metres from a 0.5 m tube those terms
+        # cancel, so a last-bit difference between the device's pow and the host library's
+        # moves the root by up to a few micrometres (4.1e-6 m measured on 76 of the 128 lip
+        # records).  Every record's element, stage and ray number is still identical, and
+        # every record off the lip is held to 1e-9 m.
+        lip = (a[1]["stage"] == 2) & (np.abs(a[1]["element"]) == 2)
+        assert lip.any()
+        sub = lambda r, m: {k: v[m] for k, v in r.items()}  # noqa: E731
+        assert_same_records(a[1], b[1], pos_tol=1e-5, dir_tol=1e-9)
+        assert_same_records(sub(a[1], ~lip), sub(b[1], ~lip), pos_tol=tol, rel_tol=2e-12, dir_tol=tol)
+        return
     assert_same_records(a[1], b[1], pos_tol=tol, rel_tol=2e-12, dir_tol=tol)
 
 
