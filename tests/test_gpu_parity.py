@@ -60,12 +60,12 @@ def test_fp64_matches_oracle_ray_by_ray(product, oracle, zoo_scenes, name):
     # later within its 1e-6 relative tolerance
     tol = 1e-7 if name == "fe_surface" else 1e-9
     if name == "bench_beam_down300":
-        # The torus lip's quartic has coefficients built from pow(x, 4) terms of the ray's
-        # start relative to the tube; with the start metres from a 0.5 m tube those terms
-        # cancel, so a last-bit difference between the device's pow and the host library's
-        # moves the root by up to a few micrometres (4.1e-6 m measured on 76 of the 128 lip
-        # records).  Every record's element, stage and ray number is still identical, and
-        # every record off the lip is held to 1e-9 m.
+        # The torus lip's quartic has coefficients built from pow(x, 4) terms, whose last bit
+        # can differ between the device's pow and the host library's; the resolvent cubic's
+        # bisection stops at a bracket width of 1e-6, so a flipped sign test moves the root
+        # by up to about that much (4.1e-6 m measured on 76 of the 128 lip records, rays
+        # starting tens of metres from the 0.5 m tube).  Every record's element, stage and
+        # ray number is still identical, and every record off the lip is held to 1e-9 m.
         lip = (a[1]["stage"] == 2) & (np.abs(a[1]["element"]) == 2)
         assert lip.any()
         sub = lambda r, m: {k: v[m] for k, v in r.items()}  # noqa: E731
