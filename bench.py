@@ -316,7 +316,10 @@ def config_lines(api, args) -> dict:
             except Exception as ex:  # noqa: BLE001
                 line["reference"] = {"unavailable": str(ex)}
     out["C1_dish"], out["C2_trough"], out["C4_batch"] = c1, c2, c4
-    out["C5_surrogate"] = surrogate_line(api)
+    try:  # a failure here keeps the lines above
+        out["C5_surrogate"] = surrogate_line(api)
+    except Exception as ex:  # noqa: BLE001
+        out["C5_surrogate"] = {"error": str(ex)}
     return out
 
 
