@@ -2243,18 +2243,22 @@ int st_sun_xyz(st_context_t p, double x, double y, double z) {
     return 1;
 }
 // solar position formula of stapi.cpp:485-527 (x west, y zenith, z north)
+// Degrees to radians as the reference writes it, v * pi / 180 evaluated left to right (not
+// v * (pi / 180)), so that the sun vector agrees with the reference's bit for bit.
+static inline double rad(double v) { return v * kPi / 180; }
+static inline double rad_l(double v) { return kPi / 180 * v; }  // the reference's M_PI / 180 * v
 int st_sun_position(st_context_t, double lat, double day, double hour, double *x, double *y, double *z) {
-    const double d2r = kPi / 180;
     const double decl = 180 / kPi * asin(0.39795 * cos(0.98563 * kPi / 180 * (day - 173)));
     const double ha = 15 * (hour - 12);
-    const double el = 180 / kPi * asin(sin(decl * d2r) * sin(lat * d2r) + cos(decl * d2r) * cos(ha * d2r) * cos(lat * d2r));
+    const double el = 180 / kPi * asin(sin(rad(decl)) * sin(rad(lat)) + cos(rad(decl)) * cos(rad(ha)) * cos(rad(lat)));
     double az = 180 / kPi *
-                acos((sin(d2r * decl) * cos(d2r * lat) - cos(d2r * decl) * sin(d2r * lat) * cos(d2r * ha)) / cos(d2r * el) +
+                acos((sin(rad_l(decl)) * cos(rad_l(lat)) - cos(rad_l(decl)) * sin(rad_l(lat)) * cos(rad_l(ha))) /
+                         cos(rad_l(el)) +
                      0.0000000001);
-    if (sin(ha * d2r) > 0.0) az = 360 - az;
-    if (x) *x = -sin(az * d2r) * cos(el * d2r);
-    if (y) *y = sin(el * d2r);
-    if (z) *z = cos(az * d2r) * cos(el * d2r);
+    if (sin(rad(ha)) > 0.0) az = 360 - az;
+    if (x) *x = -sin(rad(az)) * cos(rad(el));
+    if (y) *y = sin(rad(el));
+    if (z) *z = cos(rad(az)) * cos(rad(el));
     return 1;
 }
 int st_sun_userdata(st_context_t p, st_uint_t n, double angle[], double intensity[]) {
