@@ -34,3 +34,13 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["config"]["heliostats"] == 120 and d["config"]["hits_per_step_per_gpu"] == 20000
+
+
+def test_reference_arm_other_ranks_exit_without_work():
+    """Under torchrun only rank 0 times the reference; the other ranks print nothing and exit 0."""
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1",
+           "--warmup", "0", "--cpu-seconds", "2", "--hits", "20000", "--helios", "120"]
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=300, env=env)
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert not [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
